@@ -1,0 +1,203 @@
+/*
+ * mf.h -- C ABI of libmf, the B200 (sm_100a) implementation of the
+ * Mille-feuille tiled sparse solver path.
+ *
+ * Plain C types only.  Device pointers are CUDA global-memory addresses on
+ * the current device; `stream` is a cudaStream_t passed as void* (NULL =
+ * the legacy default stream).  Every call returns an mf_status; a failing
+ * call leaves a message for mf_last_error().  No call aborts the process.
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   mf_matrix_create        Tile_create              src/csr2block.h:267
+ *                           + host preprocessing      src/main-cg.cu:1231-1454
+ *   mf_matrix_destroy       Tile_destroy             src/format.h:88
+ *   mf_matrix_export        the Tile_matrix fields   src/format.h:14-86
+ *   mf_encode_column_index  encode                   src/encode.h:29
+ *   mf_spmv                 stir_spmv_cuda_kernel_newcsr  src/Mille-feuille-cg.h:97
+ *                           / blockspmv_cpu          src/blockspmv_cpu.h:2
+ *   mf_cg_solve             persistent CG kernels    src/Mille-feuille-cg.h:168,352,1109
+ *                           mixed persistent CG      src/main-cg-mixed.cu:99,998
+ *   mf_read_matrix_market   read_Dmatrix_32          src/biio2.0/src/biio.h:153
+ * The reference's own solve entry points (cg_solve_*, bicgstab*) keep their
+ * signatures in Mille-feuille-cg.h / Mille-feuille-bicg.h beside this file.
+ */
+#ifndef MF_H
+#define MF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum mf_status {
+    MF_OK = 0,
+    MF_ERR_INVALID_ARG = 1,  /* bad size, null pointer, index out of range */
+    MF_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    MF_ERR_NO_MEMORY = 3,    /* device or host allocation failed */
+    MF_ERR_TIMEOUT = 4,      /* a bounded grid-wide wait expired inside a kernel */
+    MF_ERR_BREAKDOWN = 5,    /* solver breakdown (zero or non-finite denominator) */
+    MF_ERR_NOT_CONVERGED = 6,/* maxiter reached before the tolerance */
+    MF_ERR_IO = 7,           /* file could not be read or parsed */
+    MF_ERR_UNSUPPORTED = 8,  /* valid input this build does not handle */
+    MF_ERR_NO_DEVICE = 9     /* no CUDA device / unsupported architecture */
+} mf_status;
+
+/* Text of the last error raised on the calling thread ("" if none). */
+const char *mf_last_error(void);
+/* Library version string. */
+const char *mf_version(void);
+
+/* ---------------------------------------------------------------------- */
+/* Tiled matrix                                                            */
+/* ---------------------------------------------------------------------- */
+
+/* Device-resident 16x16 tiled matrix: the reference's tile-CSR arrays,
+ * bit-exact, plus the derived schedules and the per-class payloads. */
+typedef struct mf_matrix_s *mf_matrix;
+
+/* Static (value-range) precision classes of a tile.  The codes follow the
+ * reference's class codes (src/main-cg-mixed.cu:236-322). */
+enum {
+    MF_CLASS_FP64 = 0,
+    MF_CLASS_BYPASS = 1,
+    MF_CLASS_INT8 = 2,
+    MF_CLASS_FP16 = 3,
+    MF_CLASS_FP32 = 4
+};
+
+typedef struct mf_matrix_info {
+    int rows;           /* rowA: tiled rows */
+    int cols;           /* colA */
+    int nnz;            /* entries in the first `rows` rows (= csrsize) */
+    int tilem, tilen, tilenum, csrsize, csrptrlen;
+    int nonzero_rows;   /* cnt_non_new: entries of the non-empty-row lists */
+    int rowblkblock;    /* entries of the blockspmv_cpu schedule */
+    int class_tiles[5]; /* tiles per static class, indexed by MF_CLASS_* */
+    int max_tile_nnz;
+    size_t device_bytes;
+} mf_matrix_info;
+
+/*
+ * Builds the tiled matrix from CSR rows [0, rowA) on the GPU.
+ * rowptr has rowA+1 entries (rowptr[0] may be nonzero), column indices must
+ * lie in [0, colA).  val_low may be NULL (then (float)val is used).
+ * on_device = 0: the four arrays are host memory (copied in), 1: device.
+ * Tiles with more than 256 entries (only possible with duplicate entries)
+ * are rejected with MF_ERR_UNSUPPORTED: the reference's u8 in-tile row
+ * pointers cannot describe them.
+ */
+mf_status mf_matrix_create(int rowA, int colA, const int *rowptr, const int *colidx,
+                           const double *val, const float *val_low, int on_device,
+                           void *stream, mf_matrix *out);
+mf_status mf_matrix_destroy(mf_matrix m);
+mf_status mf_matrix_get_info(mf_matrix m, mf_matrix_info *info);
+
+/*
+ * Copies one array of the tiled matrix to host memory.  Names (and element
+ * types) follow the reference: tile_ptr, tile_columnidx, tile_nnz, blknnz,
+ * csr_offset, csrptr_offset, ptroffset1, ptroffset2 (int32); blknnznnz,
+ * Tile_csr_Col, Blockcsr_Ptr, csr_compressedIdx, blockrowid_new,
+ * blockcsr_ptr_new (u8); Blockcsr_Val (f64); Blockcsr_Val_Low (f32);
+ * nonzero_row_new, tile_rowidx, block_signal (int32); rowblkblock_rowidx
+ * (u32), rowblkblock_colstart, rowblkblock_colstop (int32);
+ * tile_class (u8, MF_CLASS_*); payload_f16 (u16 bits); payload_i8 (i8).
+ * `bytes` must equal the array's size; mf_matrix_array_bytes tells it.
+ */
+mf_status mf_matrix_array_bytes(mf_matrix m, const char *name, size_t *bytes);
+mf_status mf_matrix_export(mf_matrix m, const char *name, void *host_dst, size_t bytes);
+
+/* Packs the in-tile column indices two per byte into csr_compressedIdx,
+ * as the reference's encode() over the whole array (src/encode.h:29). */
+mf_status mf_encode_column_index(mf_matrix m, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* SpMV and solvers                                                        */
+/* ---------------------------------------------------------------------- */
+
+/* y = A x in FP64 (device pointers; x has tilen*16 entries readable, y has
+ * rows entries).  Row sums follow blockspmv_cpu's order: per tile a
+ * sequential sum over the row's entries, tiles added in column order. */
+mf_status mf_spmv(mf_matrix m, const double *x, double *y, void *stream);
+
+typedef enum mf_policy {
+    MF_POLICY_FP64 = 0,    /* plain FP64 tiles and vectors */
+    MF_POLICY_STATIC = 1,  /* value-range tile classes, FP32 accumulate,
+                              FP64 reliable-update refinement */
+    MF_POLICY_RULE = 2,    /* STATIC + the partial-convergence rule per segment */
+    MF_POLICY_LEARNED = 3  /* STATIC + the learned per-tile policy */
+} mf_policy;
+
+typedef struct mf_solve_opts {
+    int maxiter;          /* iteration cap */
+    double tol;           /* stop when ||r||/||b|| <= tol; tol < 0 runs
+                             exactly maxiter iterations (the reference's
+                             fixed-count behaviour) */
+    int policy;           /* mf_policy */
+    double refine_delta;  /* reliable update when ||r|| fell by this factor
+                             since the last FP64 residual (mixed policies) */
+    double wait_budget_s; /* bound on every grid-wide wait inside a kernel */
+    int record_history;   /* keep ||r_k||/||b|| per iteration (see report) */
+} mf_solve_opts;
+
+typedef struct mf_solve_report {
+    int iterations;        /* Krylov iterations taken */
+    int status;            /* mf_status of the solve */
+    int refinements;       /* FP64 true-residual recomputations */
+    double relres;         /* recurrence residual ||r||/||b|| at exit */
+    double relres_true;    /* FP64 ||b - A x|| / ||b|| recomputed at exit */
+    double kernel_ms;      /* device time of the solve kernels */
+    long long bytes_moved; /* algorithmic bytes of the solve */
+    int grid_ctas;         /* CTAs of the persistent launch */
+} mf_solve_report;
+
+/* Fills opts with the defaults (maxiter 20000, tol 1e-10, FP64 policy). */
+void mf_solve_opts_default(mf_solve_opts *opts);
+
+/* Solves A x = b with one persistent cooperative CG kernel (device
+ * pointers, x0 = 0).  `history` (may be NULL) receives maxiter+1 doubles
+ * when opts->record_history is set. */
+mf_status mf_cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts *opts,
+                      mf_solve_report *report, double *history, void *stream);
+
+/* Same, with b and x in host memory: copies in, solves, copies out. */
+mf_status mf_cg_solve_host(mf_matrix m, const double *b_host, double *x_host,
+                           const mf_solve_opts *opts, mf_solve_report *report);
+
+/* ---------------------------------------------------------------------- */
+/* Matrix Market input and synthetic matrices                              */
+/* ---------------------------------------------------------------------- */
+
+/* Reads a Matrix Market coordinate file into host CSR arrays allocated
+ * with malloc (free with mf_free_host).  Entry order follows the
+ * reference reader: rows in file order, the mirrored entry of a symmetric
+ * file placed right after its original (mmio_highlevel.h:151-321). */
+mf_status mf_read_matrix_market(const char *path, int *m, int *n, int *nnz, int **rowptr,
+                                int **colidx, double **val, int *is_symmetric);
+void mf_free_host(void *p);
+
+/*
+ * Seeded synthetic matrices (host CSR, malloc'd; free with mf_free_host).
+ * They stand in for the paper's SuiteSparse inputs.  No reference
+ * counterpart: the generator is this library's own.  Randomness is the
+ * counter-based SplitMix64 stream u(seed, stream, i) in [0, 1).
+ */
+double mf_rng_u01(uint64_t seed, uint64_t stream, uint64_t i);
+double mf_rng_normal(uint64_t seed, uint64_t stream, uint64_t m);
+mf_status mf_synth_xstar(uint64_t seed, int n, double *out);
+mf_status mf_synth_laplace2d(int nx, int ny, int *n, int *nnz, int **rowptr, int **colidx, double **val);
+mf_status mf_synth_poisson3d_scaled(int g, uint64_t seed, int *n, int *nnz, int **rowptr, int **colidx,
+                                    double **val);
+mf_status mf_synth_convdiff3d(int g, double peclet, double vx, double vy, double vz, int *n, int *nnz,
+                              int **rowptr, int **colidx, double **val);
+int mf_synth_random_spd_size(uint64_t seed);
+mf_status mf_synth_random_spd(int n, uint64_t seed, int *n_out, int *nnz, int **rowptr, int **colidx,
+                              double **val);
+mf_status mf_synth_aniso3d(int g, uint64_t seed, double log_sigma, double corr_len, double aniso, int *n,
+                           int *nnz, int **rowptr, int **colidx, double **val);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MF_H */

@@ -1,0 +1,253 @@
+"""Python bindings (ctypes) for libmf, the B200 (sm_100a) Mille-feuille
+tiled sparse solver library.  The product is the C ABI in include/mf.h; this
+module only marshals numpy arrays to it for tests, benchmarks and scripts.
+
+Load it with ``load_package()`` from ``__graft_entry__`` (the directory name
+is not a Python identifier).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "lib" / "libmf.so"
+
+MF_OK = 0
+STATUS_NAMES = {
+    0: "MF_OK", 1: "MF_ERR_INVALID_ARG", 2: "MF_ERR_CUDA", 3: "MF_ERR_NO_MEMORY", 4: "MF_ERR_TIMEOUT",
+    5: "MF_ERR_BREAKDOWN", 6: "MF_ERR_NOT_CONVERGED", 7: "MF_ERR_IO", 8: "MF_ERR_UNSUPPORTED",
+    9: "MF_ERR_NO_DEVICE",
+}
+POLICY = {"fp64": 0, "static": 1, "rule": 2, "learned": 3}
+CLASS_NAMES = {0: "fp64", 1: "bypass", 2: "int8", 3: "fp16", 4: "fp32"}
+
+
+class MfError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class MatrixInfo(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("rows", "cols", "nnz", "tilem", "tilen", "tilenum", "csrsize",
+                                       "csrptrlen", "nonzero_rows", "rowblkblock")] + [
+        ("class_tiles", C.c_int * 5), ("max_tile_nnz", C.c_int), ("device_bytes", C.c_size_t)]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("maxiter", C.c_int), ("tol", C.c_double), ("policy", C.c_int), ("refine_delta", C.c_double),
+                ("wait_budget_s", C.c_double), ("record_history", C.c_int)]
+
+
+class SolveReport(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("refinements", C.c_int), ("relres", C.c_double),
+                ("relres_true", C.c_double), ("kernel_ms", C.c_double), ("bytes_moved", C.c_longlong),
+                ("grid_ctas", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+ARRAY_DTYPES = {
+    "tile_ptr": np.int32, "tile_columnidx": np.int32, "tile_nnz": np.int32, "blknnz": np.int32,
+    "csr_offset": np.int32, "csrptr_offset": np.int32, "ptroffset1": np.int32, "ptroffset2": np.int32,
+    "blknnznnz": np.uint8, "Blockcsr_Val": np.float64, "Blockcsr_Val_Low": np.float32, "Tile_csr_Col": np.uint8,
+    "Blockcsr_Ptr": np.uint8, "csr_compressedIdx": np.uint8, "nonzero_row_new": np.int32, "tile_rowidx": np.int32,
+    "block_signal": np.int32, "blockrowid_new": np.uint8, "blockcsr_ptr_new": np.uint8,
+    "rowblkblock_rowidx": np.uint32, "rowblkblock_colstart": np.int32, "rowblkblock_colstop": np.int32,
+    "tile_class": np.uint8, "payload_f16": np.uint16, "payload_i8": np.int8,
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded libmf (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"libmf not built: {LIB_PATH} missing (run __graft_entry__.build())")
+        L = C.CDLL(str(LIB_PATH))
+        vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)
+        L.mf_last_error.restype = C.c_char_p
+        L.mf_version.restype = C.c_char_p
+        L.mf_matrix_create.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_int, vp, C.POINTER(vp)]
+        L.mf_matrix_destroy.argtypes = [vp]
+        L.mf_matrix_get_info.argtypes = [vp, C.POINTER(MatrixInfo)]
+        L.mf_matrix_array_bytes.argtypes = [vp, C.c_char_p, C.POINTER(C.c_size_t)]
+        L.mf_matrix_export.argtypes = [vp, C.c_char_p, vp, C.c_size_t]
+        L.mf_encode_column_index.argtypes = [vp, vp]
+        L.mf_spmv.argtypes = [vp, vp, vp, vp]
+        L.mf_solve_opts_default.argtypes = [C.POINTER(SolveOpts)]
+        L.mf_solve_opts_default.restype = None
+        L.mf_cg_solve.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport), vp, vp]
+        L.mf_cg_solve_host.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]
+        L.mf_read_matrix_market.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
+        L.mf_free_host.argtypes = [vp]
+        L.mf_free_host.restype = None
+        L.mf_rng_u01.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
+        L.mf_rng_u01.restype = C.c_double
+        L.mf_rng_normal.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
+        L.mf_rng_normal.restype = C.c_double
+        L.mf_synth_xstar.argtypes = [C.c_uint64, C.c_int, vp]
+        L.mf_synth_random_spd_size.argtypes = [C.c_uint64]
+        L.mf_synth_random_spd_size.restype = C.c_int
+        gen = [ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp)]
+        L.mf_synth_laplace2d.argtypes = [C.c_int, C.c_int] + gen
+        L.mf_synth_poisson3d_scaled.argtypes = [C.c_int, C.c_uint64] + gen
+        L.mf_synth_convdiff3d.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double] + gen
+        L.mf_synth_random_spd.argtypes = [C.c_int, C.c_uint64] + gen
+        L.mf_synth_aniso3d.argtypes = [C.c_int, C.c_uint64, C.c_double, C.c_double, C.c_double] + gen
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != MF_OK:
+        raise MfError(status, lib().mf_last_error().decode(errors="replace"))
+
+
+class HostCsr:
+    """CSR matrix in numpy arrays (int32 indices, float64 values)."""
+
+    def __init__(self, n_rows, n_cols, rowptr, colidx, val):
+        self.n_rows, self.n_cols = int(n_rows), int(n_cols)
+        self.rowptr = np.ascontiguousarray(rowptr, np.int32)
+        self.colidx = np.ascontiguousarray(colidx, np.int32)
+        self.val = np.ascontiguousarray(val, np.float64)
+
+    @property
+    def nnz(self):
+        return int(self.rowptr[-1])
+
+    def truncated(self, rows):
+        rp = self.rowptr[: rows + 1].copy()
+        return HostCsr(rows, self.n_cols, rp, self.colidx[: rp[-1]].copy(), self.val[: rp[-1]].copy())
+
+    def matvec(self, x):
+        import scipy.sparse as sp
+
+        A = sp.csr_matrix((self.val, self.colidx, self.rowptr), shape=(self.n_rows, self.n_cols))
+        return A @ x
+
+
+def _take_csr(n, nnz, rp, ci, v, n_cols=None):
+    L = lib()
+    out = HostCsr(n, n if n_cols is None else n_cols,
+                  np.ctypeslib.as_array(rp, shape=(n + 1,)).copy(),
+                  np.ctypeslib.as_array(ci, shape=(max(nnz, 1),))[:nnz].copy(),
+                  np.ctypeslib.as_array(v, shape=(max(nnz, 1),))[:nnz].copy())
+    for p in (rp, ci, v):
+        L.mf_free_host(C.cast(p, C.c_void_p))
+    return out
+
+
+def _gen(fn, *args):
+    n, nnz = C.c_int(), C.c_int()
+    rp, ci = C.POINTER(C.c_int)(), C.POINTER(C.c_int)()
+    v = C.POINTER(C.c_double)()
+    check(fn(*args, C.byref(n), C.byref(nnz), C.byref(rp), C.byref(ci), C.byref(v)))
+    return _take_csr(n.value, nnz.value, rp, ci, v)
+
+
+def synth_laplace2d(nx, ny):
+    return _gen(lib().mf_synth_laplace2d, nx, ny)
+
+
+def synth_poisson3d_scaled(g, seed):
+    return _gen(lib().mf_synth_poisson3d_scaled, g, seed)
+
+
+def synth_convdiff3d(g, peclet=10.0, v=(1.0, 0.5, 0.25)):
+    return _gen(lib().mf_synth_convdiff3d, g, peclet, v[0], v[1], v[2])
+
+
+def synth_random_spd(seed, n=0):
+    return _gen(lib().mf_synth_random_spd, n, seed)
+
+
+def synth_aniso3d(g, seed, log_sigma=2.0, corr_len=8.0, aniso=100.0):
+    return _gen(lib().mf_synth_aniso3d, g, seed, log_sigma, corr_len, aniso)
+
+
+def synth_xstar(seed, n):
+    out = np.zeros(n, np.float64)
+    check(lib().mf_synth_xstar(seed, n, out.ctypes.data))
+    return out
+
+
+def read_matrix_market(path):
+    L = lib()
+    m, n, nnz, sym = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    rp, ci = C.POINTER(C.c_int)(), C.POINTER(C.c_int)()
+    v = C.POINTER(C.c_double)()
+    check(L.mf_read_matrix_market(str(path).encode(), C.byref(m), C.byref(n), C.byref(nnz), C.byref(rp),
+                                  C.byref(ci), C.byref(v), C.byref(sym)))
+    return _take_csr(m.value, nnz.value, rp, ci, v, n_cols=n.value)
+
+
+def solve_opts(**kw):
+    o = SolveOpts()
+    lib().mf_solve_opts_default(C.byref(o))
+    for k, val in kw.items():
+        if k == "policy" and isinstance(val, str):
+            val = POLICY[val]
+        setattr(o, k, val)
+    return o
+
+
+class Matrix:
+    """A device-resident tiled matrix (mf_matrix handle)."""
+
+    def __init__(self, csr: HostCsr, rows=None, cols=None, val_low=None):
+        L = lib()
+        rows = csr.n_rows if rows is None else rows
+        cols = csr.n_cols if cols is None else cols
+        h = C.c_void_p()
+        self._keep = (csr, None if val_low is None else np.ascontiguousarray(val_low, np.float32))
+        vl = None if val_low is None else self._keep[1].ctypes.data
+        check(L.mf_matrix_create(rows, cols, csr.rowptr.ctypes.data, csr.colidx.ctypes.data, csr.val.ctypes.data,
+                                 vl, 0, None, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mf_matrix_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> MatrixInfo:
+        inf = MatrixInfo()
+        check(lib().mf_matrix_get_info(self.h, C.byref(inf)))
+        return inf
+
+    def export(self, name):
+        L = lib()
+        nb = C.c_size_t()
+        check(L.mf_matrix_array_bytes(self.h, name.encode(), C.byref(nb)))
+        dt = np.dtype(ARRAY_DTYPES[name])
+        out = np.zeros(nb.value // dt.itemsize, dt)
+        check(L.mf_matrix_export(self.h, name.encode(), out.ctypes.data if out.size else None, nb.value))
+        return out
+
+    def encode_column_index(self):
+        check(lib().mf_encode_column_index(self.h, None))
+
+    def solve_host(self, b, **opts):
+        """CG with host b/x through mf_cg_solve_host; returns (x, report)."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.info().rows, np.float64)
+        rep = SolveReport()
+        o = solve_opts(**opts)
+        st = lib().mf_cg_solve_host(self.h, b.ctypes.data, x.ctypes.data, C.byref(o), C.byref(rep))
+        if st not in (MF_OK, 6):
+            check(st)
+        return x, rep

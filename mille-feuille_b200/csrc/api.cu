@@ -1,0 +1,327 @@
+// api.cu -- the C ABI (include/mf.h): handles, status codes, host/device
+// entry points.  No call aborts; every CUDA error becomes an mf_status.
+#include <cstdarg>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "mf_internal.h"
+
+namespace mf {
+
+static thread_local char g_err[1024] = "";
+
+void set_last_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+mf_status ensure_work(mf_matrix m, size_t bytes)
+{
+    if (m->work_bytes >= bytes) return MF_OK;
+    if (m->work) cudaFree(m->work);
+    m->work = nullptr;
+    m->work_bytes = 0;
+    MF_CUDA(cudaMalloc(&m->work, bytes));
+    m->work_bytes = bytes;
+    return MF_OK;
+}
+
+mf_status cg_solve_fp64(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,
+                        double *history, cudaStream_t s);
+
+static mf_status check_device()
+{
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        set_last_error("no CUDA device: %s", cudaGetErrorString(e));
+        return MF_ERR_NO_DEVICE;
+    }
+    int dev = 0, major = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (major != 10) {
+        set_last_error("libmf is built for sm_100a (B200); device has compute capability %d.x", major);
+        return MF_ERR_NO_DEVICE;
+    }
+    return MF_OK;
+}
+
+}  // namespace mf
+
+using namespace mf;
+
+extern "C" {
+
+const char *mf_last_error(void) { return g_err; }
+const char *mf_version(void) { return "mille-feuille-b200 0.1 (sm_100a)"; }
+
+void mf_free_host(void *p) { free(p); }
+
+mf_status mf_matrix_create(int rowA, int colA, const int *rowptr, const int *colidx, const double *val,
+                           const float *val_low, int on_device, void *stream, mf_matrix *out)
+{
+    g_err[0] = 0;
+    if (!out || !rowptr || rowA < 0 || colA < 0 || (rowA > 0 && (!colidx || !val))) {
+        set_last_error("mf_matrix_create: invalid arguments");
+        return MF_ERR_INVALID_ARG;
+    }
+    *out = nullptr;
+    MF_TRY(check_device());
+    cudaStream_t s = (cudaStream_t)stream;
+    const int *d_rp = rowptr, *d_ci = colidx;
+    const double *d_v = val;
+    const float *d_vl = val_low;
+    void *tmp = nullptr;
+    if (!on_device) {
+        const int rp0 = rowptr[0];
+        const long long nnz_end = rowptr[rowA];
+        if (nnz_end < rp0) {
+            set_last_error("rowptr[rowA] < rowptr[0]");
+            return MF_ERR_INVALID_ARG;
+        }
+        size_t b_rp = sizeof(int) * (rowA + 1), b_ci = sizeof(int) * nnz_end, b_v = sizeof(double) * nnz_end,
+               b_vl = val_low ? sizeof(float) * nnz_end : 0;
+        MF_CUDA(cudaMalloc(&tmp, b_rp + b_ci + b_v + b_vl + 64));
+        char *c = (char *)tmp;
+        double *dv = (double *)c;
+        int *dci = (int *)(c + b_v);
+        int *drp = (int *)(c + b_v + b_ci);
+        float *dvl = val_low ? (float *)(c + b_v + b_ci + b_rp + ((4 - (b_rp & 3)) & 3)) : nullptr;
+        cudaError_t e = cudaMemcpyAsync(drp, rowptr, b_rp, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && nnz_end > 0) e = cudaMemcpyAsync(dci, colidx, b_ci, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && nnz_end > 0) e = cudaMemcpyAsync(dv, val, b_v, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && val_low && nnz_end > 0) e = cudaMemcpyAsync(dvl, val_low, b_vl, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) {
+            cudaFree(tmp);
+            set_last_error("H2D copy: %s", cudaGetErrorString(e));
+            return MF_ERR_CUDA;
+        }
+        d_rp = drp;
+        d_ci = dci;
+        d_v = dv;
+        d_vl = dvl;
+    }
+    mf_matrix m = new mf_matrix_s();
+    memset(&m->v, 0, sizeof(m->v));
+    cudaGetDevice(&m->device);
+    mf_status st = build_tiles(m, rowA, colA, d_rp, d_ci, d_v, d_vl, s);
+    if (tmp) {
+        cudaStreamSynchronize(s);
+        cudaFree(tmp);
+    }
+    if (st != MF_OK) {
+        mf_matrix_destroy(m);
+        return st;
+    }
+    *out = m;
+    return MF_OK;
+}
+
+mf_status mf_matrix_destroy(mf_matrix m)
+{
+    if (!m) return MF_OK;
+    void *bufs[] = {m->d_tile_ptr, m->d_tile_columnidx, m->d_tile_nnz, m->d_csrptr_offset, m->d_blknnznnz, m->d_val,
+                    m->d_val_low, m->d_col, m->d_ptr, m->d_cidx, m->d_f16, m->d_i8, m->d_class, m->d_nonzero_row_new,
+                    m->d_tile_rowidx, m->d_block_signal, m->d_blockrowid_new, m->d_blockcsr_ptr_new, m->d_rbb_rowidx,
+                    m->d_rbb_colstart, m->d_rbb_colstop, m->d_part, m->work};
+    for (void *p : bufs)
+        if (p) cudaFree(p);
+    delete m;
+    return MF_OK;
+}
+
+mf_status mf_matrix_get_info(mf_matrix m, mf_matrix_info *info)
+{
+    if (!m || !info) return MF_ERR_INVALID_ARG;
+    memset(info, 0, sizeof(*info));
+    info->rows = m->v.rows;
+    info->cols = m->v.cols;
+    info->nnz = m->v.nnz;
+    info->tilem = m->v.tilem;
+    info->tilen = m->v.tilen;
+    info->tilenum = m->v.tilenum;
+    info->csrsize = m->v.nnz;
+    info->csrptrlen = m->v.csrptrlen;
+    info->nonzero_rows = m->nonzero_rows;
+    info->rowblkblock = m->rowblkblock;
+    for (int c = 0; c < 5; c++) info->class_tiles[c] = m->class_tiles[c];
+    info->max_tile_nnz = m->max_tile_nnz;
+    info->device_bytes = m->device_bytes;
+    return MF_OK;
+}
+
+static bool array_desc(mf_matrix m, const char *name, const void **ptr, size_t *bytes)
+{
+    const size_t T = m->v.tilenum, nnz = m->v.nnz, tilem = m->v.tilem;
+    struct D {
+        const char *n;
+        const void *p;
+        size_t b;
+    } tab[] = {
+        {"tile_ptr", m->d_tile_ptr, 4 * (tilem + 1)},
+        {"tile_columnidx", m->d_tile_columnidx, 4 * T},
+        {"tile_nnz", m->d_tile_nnz, 4 * (T + 1)},
+        {"blknnz", m->d_tile_nnz, 4 * (T + 1)},
+        {"csr_offset", m->d_tile_nnz, 4 * (T + 1)},
+        {"ptroffset1", m->d_tile_nnz, 4 * T},
+        {"csrptr_offset", m->d_csrptr_offset, 4 * (T + 1)},
+        {"ptroffset2", m->d_csrptr_offset, 4 * T},
+        {"blknnznnz", m->d_blknnznnz, T + 1},
+        {"Blockcsr_Val", m->d_val, 8 * nnz},
+        {"Blockcsr_Val_Low", m->d_val_low, 4 * nnz},
+        {"Tile_csr_Col", m->d_col, nnz},
+        {"Blockcsr_Ptr", m->d_ptr, (size_t)m->v.csrptrlen},
+        {"csr_compressedIdx", m->d_cidx, (nnz + 1) / 2},
+        {"nonzero_row_new", m->d_nonzero_row_new, 4 * (T + 1)},
+        {"tile_rowidx", m->d_tile_rowidx, 4 * T},
+        {"block_signal", m->d_block_signal, 4 * (tilem + 1)},
+        {"blockrowid_new", m->d_blockrowid_new, (size_t)m->nonzero_rows + 1},
+        {"blockcsr_ptr_new", m->d_blockcsr_ptr_new, (size_t)m->nonzero_rows + 1},
+        {"rowblkblock_rowidx", m->d_rbb_rowidx, 4 * (size_t)m->rowblkblock},
+        {"rowblkblock_colstart", m->d_rbb_colstart, 4 * (size_t)m->rowblkblock},
+        {"rowblkblock_colstop", m->d_rbb_colstop, 4 * (size_t)m->rowblkblock},
+        {"tile_class", m->d_class, T},
+        {"payload_f16", m->d_f16, 2 * nnz},
+        {"payload_i8", m->d_i8, nnz},
+    };
+    for (auto &d : tab)
+        if (!strcmp(d.n, name)) {
+            *ptr = d.p;
+            *bytes = d.b;
+            return true;
+        }
+    return false;
+}
+
+mf_status mf_matrix_array_bytes(mf_matrix m, const char *name, size_t *bytes)
+{
+    const void *p;
+    if (!m || !name || !bytes || !array_desc(m, name, &p, bytes)) {
+        set_last_error("unknown array name");
+        return MF_ERR_INVALID_ARG;
+    }
+    return MF_OK;
+}
+
+mf_status mf_matrix_export(mf_matrix m, const char *name, void *host_dst, size_t bytes)
+{
+    const void *p;
+    size_t b;
+    if (!m || !name || !array_desc(m, name, &p, &b)) {
+        set_last_error("unknown array name");
+        return MF_ERR_INVALID_ARG;
+    }
+    if (bytes != b || (b > 0 && !host_dst)) {
+        set_last_error("export %s: expected %zu bytes, got %zu", name, b, bytes);
+        return MF_ERR_INVALID_ARG;
+    }
+    if (b == 0) return MF_OK;
+    MF_CUDA(cudaMemcpy(host_dst, p, b, cudaMemcpyDeviceToHost));
+    return MF_OK;
+}
+
+static __global__ void k_encode(int n, const unsigned char *__restrict__ col, unsigned char *__restrict__ out)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < (n + 1) / 2; p += gridDim.x * blockDim.x) {
+        unsigned char hi = col[2 * p];
+        unsigned char lo = (2 * p + 1 < n) ? col[2 * p + 1] : 0;
+        out[p] = (unsigned char)((hi << 4) + lo);
+    }
+}
+
+mf_status mf_encode_column_index(mf_matrix m, void *stream)
+{
+    if (!m) return MF_ERR_INVALID_ARG;
+    const int n = m->v.nnz;
+    if (n == 0) return MF_OK;
+    int grid = ceil_div((n + 1) / 2, 256);
+    if (grid > 148 * 16) grid = 148 * 16;
+    k_encode<<<grid, 256, 0, (cudaStream_t)stream>>>(n, m->d_col, m->d_cidx);
+    MF_CUDA(cudaGetLastError());
+    return MF_OK;
+}
+
+mf_status mf_spmv(mf_matrix m, const double *x, double *y, void *stream)
+{
+    if (!m || (m->v.rows > 0 && (!x || !y))) return MF_ERR_INVALID_ARG;
+    return spmv_fp64(m->v, x, y, (cudaStream_t)stream);
+}
+
+void mf_solve_opts_default(mf_solve_opts *o)
+{
+    if (!o) return;
+    o->maxiter = 20000;
+    o->tol = 1e-10;
+    o->policy = MF_POLICY_FP64;
+    o->refine_delta = 0.1;
+    o->wait_budget_s = 5.0;
+    o->record_history = 0;
+}
+
+mf_status mf_cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts *opts, mf_solve_report *report,
+                      double *history, void *stream)
+{
+    g_err[0] = 0;
+    if (!m || !b || !x) {
+        set_last_error("mf_cg_solve: null argument");
+        return MF_ERR_INVALID_ARG;
+    }
+    mf_solve_opts o;
+    mf_solve_opts_default(&o);
+    if (opts) o = *opts;
+    if (o.maxiter < 0 || o.wait_budget_s <= 0) {
+        set_last_error("mf_cg_solve: maxiter < 0 or wait budget <= 0");
+        return MF_ERR_INVALID_ARG;
+    }
+    if (m->v.rows != m->v.cols) {
+        set_last_error("mf_cg_solve: matrix is %d x %d, a square system is required", m->v.rows, m->v.cols);
+        return MF_ERR_INVALID_ARG;
+    }
+    mf_solve_report rep;
+    memset(&rep, 0, sizeof(rep));
+    mf_status st;
+    if (m->v.rows == 0) {
+        st = MF_OK;
+    } else if (o.policy == MF_POLICY_FP64) {
+        st = cg_solve_fp64(m, b, x, o, rep, history, (cudaStream_t)stream);
+    } else {
+        set_last_error("policy %d not available in this build", o.policy);
+        st = MF_ERR_UNSUPPORTED;
+    }
+    rep.status = st;
+    if (report) *report = rep;
+    return st;
+}
+
+mf_status mf_cg_solve_host(mf_matrix m, const double *b_host, double *x_host, const mf_solve_opts *opts,
+                           mf_solve_report *report)
+{
+    if (!m || !b_host || !x_host) return MF_ERR_INVALID_ARG;
+    const size_t n = m->v.rows;
+    double *d = nullptr;
+    MF_CUDA(cudaMalloc(&d, sizeof(double) * (2 * n + 2)));
+    double *db = d, *dx = d + n + 1;
+    cudaStream_t s = 0;
+    cudaError_t e = cudaMemcpyAsync(db, b_host, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        set_last_error("H2D: %s", cudaGetErrorString(e));
+        return MF_ERR_CUDA;
+    }
+    mf_status st = mf_cg_solve(m, db, dx, opts, report, nullptr, s);
+    e = cudaMemcpyAsync(x_host, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        set_last_error("D2H: %s", cudaGetErrorString(e));
+        return MF_ERR_CUDA;
+    }
+    return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,124 @@
+// mf_common.cuh -- shared device/host helpers for the sm_100a kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "mf.h"
+
+#define MF_TILE 16
+
+namespace mf {
+
+// ---------------------------------------------------------------------------
+// Host-side error handling: every CUDA call is checked and turned into an
+// mf_status; nothing aborts the process.
+// ---------------------------------------------------------------------------
+void set_last_error(const char *fmt, ...);
+
+#define MF_CUDA(expr)                                                                     \
+    do {                                                                                  \
+        cudaError_t _e = (expr);                                                          \
+        if (_e != cudaSuccess) {                                                          \
+            ::mf::set_last_error("%s:%d %s: %s", __FILE__, __LINE__, #expr,               \
+                                 cudaGetErrorString(_e));                                 \
+            return (_e == cudaErrorMemoryAllocation) ? MF_ERR_NO_MEMORY : MF_ERR_CUDA;    \
+        }                                                                                 \
+    } while (0)
+
+#define MF_TRY(expr)                                                                      \
+    do {                                                                                  \
+        mf_status _s = (expr);                                                            \
+        if (_s != MF_OK) return _s;                                                       \
+    } while (0)
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ int ld_volatile_i32(const int *p)
+{
+    return *(const volatile int *)p;
+}
+
+// Status word codes written by kernels (device side mirror of mf_status).
+enum : int { DEV_OK = 0, DEV_TIMEOUT = MF_ERR_TIMEOUT, DEV_BREAKDOWN = MF_ERR_BREAKDOWN };
+
+// Grid-wide barrier for a cooperative launch.  Every CTA calls it with the
+// same running `epoch`; the counter is reset to 0 before the launch.  The
+// spin is bounded by `budget_ns`: on expiry the status word is set to
+// DEV_TIMEOUT and the call returns false (the caller then leaves the kernel).
+__device__ __forceinline__ bool grid_barrier(unsigned long long *counter, unsigned long long target,
+                                             int *status, unsigned long long budget_ns)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        __threadfence();
+        atomicAdd(counter, 1ull);
+        unsigned long long t0 = globaltimer_ns();
+        unsigned spins = 0;
+        while (ld_acquire_u64(counter) < target) {
+            if (((++spins) & 63u) == 0u) {
+                if (ld_volatile_i32(status) != DEV_OK) { ok = 0; break; }
+                if (globaltimer_ns() - t0 > budget_ns) {
+                    atomicCAS(status, DEV_OK, DEV_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        if (ld_volatile_i32(status) != DEV_OK) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Deterministic CTA reduction of one double per thread: warp butterfly, then
+// the warp results summed in warp order.  All threads get the result.
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double *s_warp)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) s_warp[w] = v;
+    __syncthreads();
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < NT / 32; i++) s += s_warp[i];
+    return s;
+}
+
+// Deterministic sum of `count` per-CTA partials (same order in every CTA):
+// lane l sums entries l, l+32, ... sequentially, then a butterfly.
+__device__ __forceinline__ double warp_sum_partials(const double *part, int count)
+{
+    const int lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int i = lane; i < count; i += 32) s += __ldcg(part + i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
+}  // namespace mf

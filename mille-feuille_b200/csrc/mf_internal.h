@@ -1,0 +1,71 @@
+// mf_internal.h -- internal (C++) view of the device-resident tiled matrix.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "mf.h"
+#include "mf_common.cuh"
+
+// Flat, trivially-copyable view passed to kernels.
+struct MfTiles {
+    int rows, cols, nnz;
+    int tilem, tilen, tilenum, csrptrlen;
+    int rows_multiple_of_16;            // 1 when every tile has 16 row pointers
+    const int *tile_ptr;                // [tilem+1]
+    const int *tile_columnidx;          // [tilenum]
+    const int *tile_nnz;                // [tilenum+1] scanned (= blknnz = csr_offset)
+    const int *csrptr_offset;           // [tilenum+1]
+    const double *val;                  // [nnz] Blockcsr_Val
+    const float *val_low;               // [nnz] Blockcsr_Val_Low
+    const unsigned char *col;           // [nnz] Tile_csr_Col
+    const unsigned char *ptr;           // [csrptrlen] Blockcsr_Ptr
+    const uint16_t *val_f16;            // [nnz] fp16 payload bits
+    const int8_t *val_i8;               // [nnz] int8 payload
+    const unsigned char *tile_class;    // [tilenum] static class
+};
+
+struct mf_matrix_s {
+    MfTiles v;                 // device pointers (views into the buffers below)
+    int device;
+    int max_tile_nnz;
+    int class_tiles[5];
+    int nonzero_rows;          // cnt_non_new
+    int rowblkblock;
+    size_t device_bytes;
+
+    // owned device buffers
+    int *d_tile_ptr = nullptr, *d_tile_columnidx = nullptr, *d_tile_nnz = nullptr;
+    int *d_csrptr_offset = nullptr;
+    unsigned char *d_blknnznnz = nullptr;
+    double *d_val = nullptr;
+    float *d_val_low = nullptr;
+    unsigned char *d_col = nullptr, *d_ptr = nullptr, *d_cidx = nullptr;
+    uint16_t *d_f16 = nullptr;
+    int8_t *d_i8 = nullptr;
+    unsigned char *d_class = nullptr;
+    // derived reference arrays (src/main-cg.cu:1231-1288, blockspmv_cpu.h:35-83)
+    int *d_nonzero_row_new = nullptr, *d_tile_rowidx = nullptr, *d_block_signal = nullptr;
+    unsigned char *d_blockrowid_new = nullptr, *d_blockcsr_ptr_new = nullptr;
+    unsigned int *d_rbb_rowidx = nullptr;
+    int *d_rbb_colstart = nullptr, *d_rbb_colstop = nullptr;
+    // strip partitions for the persistent kernels, cached per CTA count
+    int part_ctas = 0;
+    int *d_part = nullptr;     // [part_ctas+1] strip boundaries
+    // cached per-matrix solver workspace
+    void *work = nullptr;
+    size_t work_bytes = 0;
+};
+
+namespace mf {
+// scan.cu
+mf_status exclusive_scan_i32(const int *in, int *out, int n, cudaStream_t s, int *total_host);
+// tile_build.cu
+mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, const int *d_colidx,
+                      const double *d_val, const float *d_val_low, cudaStream_t s);
+mf_status strip_partition(mf_matrix m, int ctas, cudaStream_t s);
+// spmv.cu
+mf_status spmv_fp64(const MfTiles &A, const double *x, double *y, cudaStream_t s);
+// workspace
+mf_status ensure_work(mf_matrix m, size_t bytes);
+}  // namespace mf

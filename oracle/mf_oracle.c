@@ -1,0 +1,512 @@
+/*
+ * mf_oracle.c -- CPU oracle (test infrastructure only; see mf_oracle.h).
+ *
+ * Plain C restatement of the reference's CPU algorithms.  Each function
+ * names the reference file:line it follows.  Sums are written as separate
+ * multiply and add statements and the file is compiled with
+ * -ffp-contract=off so that no fused multiply-add changes a rounding.
+ */
+#include "mf_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define TILE 16
+
+static int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+/* ---- Tile_create: src/csr2block.h:267-422 (steps 1-4 at 6-265) ---------- */
+
+typedef struct { int jc; int src; } orc_pair;
+
+static int pair_cmp(const void *a, const void *b)
+{
+    const orc_pair *x = (const orc_pair *)a, *y = (const orc_pair *)b;
+    if (x->jc != y->jc) return x->jc < y->jc ? -1 : 1;
+    return (x->src > y->src) - (x->src < y->src);
+}
+
+void orc_tiles_free(orc_tiles *t)
+{
+    free(t->tile_ptr); free(t->tile_columnidx); free(t->tile_nnz); free(t->blknnz);
+    free(t->blknnznnz); free(t->csr_offset); free(t->csrptr_offset); free(t->Blockcsr_Val);
+    free(t->Blockcsr_Val_Low); free(t->Tile_csr_Col); free(t->Blockcsr_Ptr);
+    memset(t, 0, sizeof(*t));
+}
+
+/* Returns 0 on success, -1 on an out-of-range column index. */
+int orc_tile_create(int rowA, int colA, const int *rowptr, const int *colidx,
+                    const double *val, const float *val_low, orc_tiles *out)
+{
+    memset(out, 0, sizeof(*out));
+    int tilem = ceil_div(rowA, TILE), tilen = ceil_div(colA, TILE);
+    out->tilem = tilem; out->tilen = tilen;
+    int nnz_used = rowA > 0 ? rowptr[rowA] - rowptr[0] : 0;
+    for (int k = rowptr[0]; k < rowptr[0] + nnz_used; k++)
+        if (colidx[k] < 0 || colidx[k] >= colA) return -1;
+
+    /* step 1 (csr2block.h:6-41): distinct tile columns per tile-row */
+    out->tile_ptr = (int *)calloc(tilem + 1, sizeof(int));
+    int maxrow = 0;
+    for (int bi = 0; bi < tilem; bi++) {
+        int s = bi * TILE, e = (bi == tilem - 1) ? rowA : (bi + 1) * TILE;
+        if (rowptr[e] - rowptr[s] > maxrow) maxrow = rowptr[e] - rowptr[s];
+    }
+    orc_pair *pairs = (orc_pair *)malloc((size_t)(maxrow > 0 ? maxrow : 1) * sizeof(orc_pair));
+    for (int bi = 0; bi < tilem; bi++) {
+        int s = bi * TILE, e = (bi == tilem - 1) ? rowA : (bi + 1) * TILE;
+        int m = 0;
+        for (int k = rowptr[s]; k < rowptr[e]; k++) { pairs[m].jc = colidx[k] / TILE; pairs[m].src = k; m++; }
+        qsort(pairs, m, sizeof(orc_pair), pair_cmp);
+        int cnt = 0;
+        for (int q = 0; q < m; q++) if (q == 0 || pairs[q].jc != pairs[q - 1].jc) cnt++;
+        out->tile_ptr[bi] = cnt;
+    }
+    /* exclusive scan (utils.h:34-49) */
+    {
+        int run = 0;
+        for (int bi = 0; bi <= tilem; bi++) { int v = out->tile_ptr[bi]; out->tile_ptr[bi] = run; run += v; }
+    }
+    int T = out->tile_ptr[tilem];
+    out->tilenum = T;
+
+    /* step 2 (csr2block.h:43-107): tile columns, per-tile nnz, per-row u8 counts */
+    out->tile_columnidx = (int *)calloc(T > 0 ? T : 1, sizeof(int));
+    out->tile_nnz = (int *)calloc(T + 1, sizeof(int));
+    unsigned char *row_cnt = (unsigned char *)calloc((size_t)(T > 0 ? T : 1) * TILE, 1);
+    for (int bi = 0; bi < tilem; bi++) {
+        int s = bi * TILE, e = (bi == tilem - 1) ? rowA : (bi + 1) * TILE;
+        int m = 0;
+        for (int k = rowptr[s]; k < rowptr[e]; k++) { pairs[m].jc = colidx[k] / TILE; pairs[m].src = k; m++; }
+        qsort(pairs, m, sizeof(orc_pair), pair_cmp);
+        int t = out->tile_ptr[bi] - 1;
+        for (int q = 0; q < m; q++) {
+            if (q == 0 || pairs[q].jc != pairs[q - 1].jc) { t++; out->tile_columnidx[t] = pairs[q].jc; }
+            out->tile_nnz[t]++;
+        }
+        for (int r = s; r < e; r++)
+            for (int k = rowptr[r]; k < rowptr[r + 1]; k++) {
+                int jc = colidx[k] / TILE;
+                /* locate tile of jc in this tile-row (linear, as step 4 does) */
+                for (int tt = out->tile_ptr[bi]; tt < out->tile_ptr[bi + 1]; tt++)
+                    if (out->tile_columnidx[tt] == jc) { row_cnt[(size_t)tt * TILE + (r - s)]++; break; }
+            }
+    }
+    {
+        int run = 0;
+        for (int i = 0; i <= T; i++) { int v = out->tile_nnz[i]; out->tile_nnz[i] = run; run += v; }
+    }
+
+    /* step 3 (csr2block.h:109-150) + scans (csr2block.h:346-376) */
+    out->blknnz = (int *)calloc(T + 1, sizeof(int));
+    out->blknnznnz = (unsigned char *)calloc(T + 1, 1);
+    out->csr_offset = (int *)calloc(T + 1, sizeof(int));
+    out->csrptr_offset = (int *)calloc(T + 1, sizeof(int));
+    int csrsize = 0, csrptrlen = 0;
+    for (int bi = 0; bi < tilem; bi++) {
+        int rowlen = (bi == tilem - 1) ? rowA - (tilem - 1) * TILE : TILE;
+        for (int t = out->tile_ptr[bi]; t < out->tile_ptr[bi + 1]; t++) {
+            int nz = out->tile_nnz[t + 1] - out->tile_nnz[t];
+            out->blknnz[t] = nz; out->csr_offset[t] = nz; out->csrptr_offset[t] = rowlen;
+            csrsize += nz; csrptrlen += rowlen;
+        }
+    }
+    for (int i = 0; i <= T; i++) out->blknnznnz[i] = (unsigned char)out->blknnz[i];
+    {
+        int r1 = 0, r2 = 0, r3 = 0;
+        for (int i = 0; i <= T; i++) {
+            int a = out->blknnz[i], b = out->csr_offset[i], c = out->csrptr_offset[i];
+            out->blknnz[i] = r1; out->csr_offset[i] = r2; out->csrptr_offset[i] = r3;
+            r1 += a; r2 += b; r3 += c;
+        }
+    }
+    out->csrsize = csrsize; out->csrptrlen = csrptrlen;
+
+    /* step 4 (csr2block.h:152-265): scatter in CSR order, u8 row pointers */
+    out->Blockcsr_Val = (double *)calloc(csrsize > 0 ? csrsize : 1, sizeof(double));
+    out->Blockcsr_Val_Low = (float *)calloc(csrsize > 0 ? csrsize : 1, sizeof(float));
+    out->Tile_csr_Col = (unsigned char *)calloc(csrsize > 0 ? csrsize : 1, 1);
+    out->Blockcsr_Ptr = (unsigned char *)calloc(csrptrlen > 0 ? csrptrlen : 1, 1);
+    int *fill = (int *)calloc(T > 0 ? T : 1, sizeof(int));
+    for (int bi = 0; bi < tilem; bi++) {
+        int s = bi * TILE, e = (bi == tilem - 1) ? rowA : (bi + 1) * TILE;
+        int rowlen = e - s;
+        for (int k = rowptr[s]; k < rowptr[e]; k++) {
+            int jc = colidx[k] / TILE;
+            for (int t = out->tile_ptr[bi]; t < out->tile_ptr[bi + 1]; t++) {
+                if (out->tile_columnidx[t] != jc) continue;
+                int dst = out->csr_offset[t] + fill[t]++;
+                out->Blockcsr_Val[dst] = val[k];
+                out->Blockcsr_Val_Low[dst] = val_low ? val_low[k] : (float)val[k];
+                out->Tile_csr_Col[dst] = (unsigned char)(colidx[k] - jc * TILE);
+                break;
+            }
+        }
+        for (int t = out->tile_ptr[bi]; t < out->tile_ptr[bi + 1]; t++) {
+            /* exclusive_scan_char over rowlen entries (utils.h:50-65) */
+            unsigned char run = 0;
+            for (int r = 0; r < rowlen; r++) {
+                unsigned char v = row_cnt[(size_t)t * TILE + r];
+                out->Blockcsr_Ptr[out->csrptr_offset[t] + r] = run;
+                run = (unsigned char)(run + v);
+            }
+        }
+    }
+    free(fill); free(row_cnt); free(pairs);
+    return 0;
+}
+
+/* ---- encode / decode: src/encode.h:29-72 -------------------------------- */
+
+void orc_encode(const unsigned char *str, unsigned char *res, int str_len, int offset)
+{
+    int pairs = str_len / 2;
+    for (int p = 0; p < pairs; p++)
+        res[offset + p] = (unsigned char)((str[2 * p] << 4) + str[2 * p + 1]);
+    if (str_len % 2) res[offset + pairs] = (unsigned char)(str[str_len - 1] << 4);
+}
+
+void orc_decode(const unsigned char *str, unsigned char *res, int res_len)
+{
+    for (int i = 0; i + 1 < res_len; i += 2) {
+        res[i] = (unsigned char)((str[i / 2] & 240) >> 4);
+        res[i + 1] = (unsigned char)(str[i / 2] & 15);
+    }
+    if (res_len % 2) res[res_len - 1] = (unsigned char)(str[res_len / 2] >> 4);
+}
+
+/* ---- blockspmv_cpu: src/blockspmv_cpu.h:2-112 --------------------------- */
+
+#define PREFETCH_TH 4
+
+int orc_rowblkblock_count(const orc_tiles *t)
+{
+    int c = 0;
+    for (int bi = 0; bi < t->tilem; bi++) {
+        int k = t->tile_ptr[bi + 1] - t->tile_ptr[bi];
+        c += (k <= PREFETCH_TH) ? 1 : ceil_div(k, PREFETCH_TH);
+    }
+    return c;
+}
+
+void orc_blockspmv(const orc_tiles *t, int rowA, int colA, const unsigned char *cidx,
+                   int *ptroffset1, int *ptroffset2, unsigned int *rowidx, int *colstart,
+                   int *colstop, const double *x, double *y)
+{
+    (void)colA;
+    int e = 0;
+    for (int bi = 0; bi < t->tilem; bi++) {
+        int k = t->tile_ptr[bi + 1] - t->tile_ptr[bi];
+        if (k <= PREFETCH_TH) { rowidx[e] = (unsigned)bi; colstart[e] = 0; colstop[e] = 0; e++; continue; }
+        int parts = ceil_div(k, PREFETCH_TH);
+        int len = ceil_div(k, parts);
+        for (int p = 0; p < parts; p++) {
+            rowidx[e] = (unsigned)bi | 0x80000000u;
+            colstart[e] = t->tile_ptr[bi] + p * len;
+            colstop[e] = (p == parts - 1) ? t->tile_ptr[bi] + k : t->tile_ptr[bi] + (p + 1) * len;
+            e++;
+        }
+    }
+    int valoff = 0, ptroff = 0;
+    for (int bi = 0; bi < t->tilem; bi++) {
+        int rowlen = (bi == t->tilem - 1) ? rowA - (t->tilem - 1) * TILE : TILE;
+        for (int r = 0; r < TILE; r++) y[bi * TILE + r] = 0;
+        for (int tt = t->tile_ptr[bi]; tt < t->tile_ptr[bi + 1]; tt++) {
+            int xo = t->tile_columnidx[tt] * TILE;
+            ptroffset1[tt] = valoff; ptroffset2[tt] = ptroff;
+            int nz = t->blknnz[tt + 1] - t->blknnz[tt];
+            for (int r = 0; r < rowlen; r++) {
+                double sum = 0;
+                int stop = (r == rowlen - 1) ? nz : t->Blockcsr_Ptr[ptroff + r + 1];
+                for (int k = t->Blockcsr_Ptr[ptroff + r]; k < stop; k++) {
+                    int g = valoff + k;
+                    int c = (g % 2 == 0) ? (cidx[g / 2] & 240) >> 4 : (cidx[g / 2] & 15);
+                    double prod = x[xo + c] * t->Blockcsr_Val[g];
+                    sum = sum + prod;
+                }
+                y[bi * TILE + r] = y[bi * TILE + r] + sum;
+            }
+            valoff += nz; ptroff += rowlen;
+        }
+    }
+}
+
+void orc_tiled_spmv(const orc_tiles *t, int rowA, const double *x, double *y)
+{
+    for (int bi = 0; bi < t->tilem; bi++) {
+        int rowlen = (bi == t->tilem - 1) ? rowA - (t->tilem - 1) * TILE : TILE;
+        for (int r = 0; r < rowlen; r++) y[bi * TILE + r] = 0;
+        for (int tt = t->tile_ptr[bi]; tt < t->tile_ptr[bi + 1]; tt++) {
+            int xo = t->tile_columnidx[tt] * TILE;
+            int off = t->tile_nnz[tt], nz = t->tile_nnz[tt + 1] - off, po = t->csrptr_offset[tt];
+            for (int r = 0; r < rowlen; r++) {
+                double sum = 0;
+                int stop = (r == rowlen - 1) ? nz : t->Blockcsr_Ptr[po + r + 1];
+                for (int k = t->Blockcsr_Ptr[po + r]; k < stop; k++) {
+                    double prod = x[xo + t->Tile_csr_Col[off + k]] * t->Blockcsr_Val[off + k];
+                    sum = sum + prod;
+                }
+                y[bi * TILE + r] = y[bi * TILE + r] + sum;
+            }
+        }
+    }
+}
+
+/* ---- non-empty-row compaction: src/main-cg.cu:1231-1288 ----------------- */
+
+static int row_stop(const orc_tiles *t, int tt, int r, int rowlen)
+{
+    int po = t->csrptr_offset[tt];
+    return (r == rowlen - 1) ? (t->blknnz[tt + 1] - t->blknnz[tt]) : t->Blockcsr_Ptr[po + r + 1];
+}
+
+int orc_nonzero_rows_count(const orc_tiles *t, int rowA)
+{
+    int c = 0;
+    for (int bi = 0; bi < t->tilem; bi++) {
+        int rowlen = (bi == t->tilem - 1) ? rowA - (t->tilem - 1) * TILE : TILE;
+        for (int tt = t->tile_ptr[bi]; tt < t->tile_ptr[bi + 1]; tt++) {
+            c += 1;
+            for (int r = 0; r < rowlen; r++)
+                if (row_stop(t, tt, r, rowlen) != t->Blockcsr_Ptr[t->csrptr_offset[tt] + r]) c++;
+        }
+    }
+    return c;
+}
+
+void orc_nonzero_rows(const orc_tiles *t, int rowA, int *nzr, int *tile_rowidx,
+                      unsigned char *rowid, unsigned char *ptrnew, int *block_signal)
+{
+    int T = t->tilenum, run = 0;
+    for (int bi = 0; bi < t->tilem; bi++) {
+        int rowlen = (bi == t->tilem - 1) ? rowA - (t->tilem - 1) * TILE : TILE;
+        block_signal[bi] = t->tile_ptr[bi + 1] - t->tile_ptr[bi];
+        for (int tt = t->tile_ptr[bi]; tt < t->tile_ptr[bi + 1]; tt++) {
+            tile_rowidx[tt] = bi;
+            nzr[tt] = run;
+            rowid[run] = 0; ptrnew[run] = 0; run++;
+            for (int r = 0; r < rowlen; r++) {
+                int stop = row_stop(t, tt, r, rowlen);
+                if (stop != t->Blockcsr_Ptr[t->csrptr_offset[tt] + r]) {
+                    rowid[run] = (unsigned char)r; ptrnew[run] = (unsigned char)stop; run++;
+                }
+            }
+        }
+    }
+    nzr[T] = run;
+    rowid[run] = 0; ptrnew[run] = 0;
+    block_signal[t->tilem] = 0;
+}
+
+/* ---- nnz load balancer (cg_solve_inc): src/main-cg.cu:1290-1454 ---------- */
+
+static int balance_count(const int *nz, int T, int budget)
+{
+    int i = 0, j = T - 1, cnt = 0, index = 1;
+    while (i < j) {
+        if (nz[i] + cnt < budget) { cnt += nz[i]; i++; } else { i++; index++; cnt = 0; }
+        if (nz[j] + cnt < budget) { cnt += nz[j]; j--; } else { j--; index++; cnt = 0; }
+    }
+    return index;
+}
+
+/* Returns 0 on success; -1 where the reference would loop forever (no
+ * budget in its list gives fewer than 6912 warps) or return early. */
+int orc_balance(const orc_tiles *t, int nnzR, int *index_out, int *budget_out,
+                int *bptr, int *row_new, int *idx_new, int *vew32, int *vt32)
+{
+    int T = t->tilenum;
+    int *nz = (int *)malloc((size_t)(T + 1) * sizeof(int));
+    int *row = (int *)malloc((size_t)(T + 1) * sizeof(int));
+    for (int bi = 0; bi < t->tilem; bi++)
+        for (int tt = t->tile_ptr[bi]; tt < t->tile_ptr[bi + 1]; tt++) {
+            nz[tt] = t->blknnz[tt + 1] - t->blknnz[tt]; row[tt] = bi;
+        }
+    int list[12] = {16, 32, 64, 96, 128, 256, 512, 1024, 2048, 4096, nnzR / 6912, 0};
+    int budget = -1, index = 0;
+    for (int k = 0; k < 12; k++) {
+        index = balance_count(nz, T, list[k]);
+        if (index < 6912) { budget = list[k]; break; }
+    }
+    if (budget < 0) { free(nz); free(row); return -1; }
+    *vew32 = 0; *vt32 = 0;
+    if (index < t->tilem) {
+        int vew16 = ceil_div(t->tilem, index);
+        int tilem32 = ceil_div(t->tilem, 2);
+        *vew32 = vew16 * 2;
+        *vt32 = (tilem32 / *vew32 / 8) * 8;
+    }
+    for (int q = 0; q <= index; q++) bptr[q] = 0;
+    for (int q = 0; q <= T; q++) { row_new[q] = 0; idx_new[q] = 0; }
+    int i = 0, j = T - 1, cnt = 0, step = 0;
+    index = 1;
+    while (i < j) {
+        if (nz[i] + cnt < budget) { cnt += nz[i]; idx_new[step] = i; row_new[step] = row[i]; i++; step++; }
+        else { idx_new[step] = i; row_new[step] = row[i]; i++; step++; bptr[index] = step; index++; cnt = 0; }
+        if (nz[j] + cnt < budget) { cnt += nz[j]; idx_new[step] = j; row_new[step] = row[j]; j--; step++; }
+        else { idx_new[step] = j; row_new[step] = row[j]; j--; step++; bptr[index] = step; index++; cnt = 0; }
+        if (i == j) { idx_new[step] = j; row_new[step] = row[j]; step++; bptr[index] = step; }
+        if (i > j) { idx_new[step] = j; row_new[step] = row[j]; bptr[index] = step; }
+    }
+    *index_out = index; *budget_out = budget;
+    free(nz); free(row);
+    return 0;
+}
+
+/* ---- payload casts: src/main-cg-mixed.cu:2325-2342 ---------------------- */
+
+/* IEEE-754 binary32 -> binary16, round to nearest even (the rounding that
+ * the reference's (half)(float)v conversion performs). */
+uint16_t orc_f32_to_f16_bits(float f)
+{
+    uint32_t x; memcpy(&x, &f, 4);
+    uint32_t sign = (x >> 16) & 0x8000u;
+    uint32_t ex = (x >> 23) & 0xffu, man = x & 0x7fffffu;
+    if (ex == 0xffu) return (uint16_t)(sign | 0x7c00u | (man ? 0x200u | (man >> 13) : 0u));
+    int e = (int)ex - 127 + 15;
+    if (e >= 31) return (uint16_t)(sign | 0x7c00u);
+    if (e <= 0) {
+        if (e < -10) return (uint16_t)sign;
+        uint32_t m = man | 0x800000u;
+        int shift = 14 - e;
+        uint32_t q = m >> shift, rem = m & ((1u << shift) - 1u), half = 1u << (shift - 1);
+        if (rem > half || (rem == half && (q & 1u))) q++;
+        return (uint16_t)(sign | q);
+    }
+    uint32_t q = man >> 13, rem = man & 0x1fffu;
+    uint32_t h = sign | ((uint32_t)e << 10) | q;
+    if (rem > 0x1000u || (rem == 0x1000u && (q & 1u))) h++;
+    return (uint16_t)h;
+}
+
+float orc_f16_bits_to_f32(uint16_t h)
+{
+    uint32_t sign = (uint32_t)(h & 0x8000u) << 16, ex = (h >> 10) & 0x1fu, man = h & 0x3ffu, x;
+    if (ex == 0) {
+        if (man == 0) x = sign;
+        else { float v = (float)man * 0x1p-24f; memcpy(&x, &v, 4); x |= sign; }
+    } else if (ex == 31) x = sign | 0x7f800000u | (man << 13);
+    else x = sign | ((ex - 15 + 127) << 23) | (man << 13);
+    float f; memcpy(&f, &x, 4); return f;
+}
+
+void orc_payload_casts(const double *v, int n, float *f32, uint16_t *f16, int8_t *i8)
+{
+    for (int i = 0; i < n; i++) {
+        float f = (float)v[i];
+        if (f32) f32[i] = f;
+        if (f16) f16[i] = orc_f32_to_f16_bits(f);
+        if (i8) {
+            /* (int8_t)v as compiled for x86-64: truncate toward zero to a
+             * 32-bit integer, keep the low byte (two's complement). */
+            double tv = trunc(v[i]);
+            int32_t w = (tv >= 2147483648.0 || tv < -2147483648.0 || tv != tv) ? INT32_MIN : (int32_t)tv;
+            i8[i] = (int8_t)(uint8_t)(uint32_t)w;
+        }
+    }
+}
+
+/* Race-free restatement of the per-segment rule of
+ * src/main-cg-mixed.cu:415-460: the most precise class demanded by any
+ * element of the segment wins, i.e. the class follows the largest |dp|.
+ * Codes follow the reference: 0 fp64, 4 fp32, 3 fp16, 2 int8, 1 bypass. */
+int orc_rule_class(double v)
+{
+    if (v > 1e-5) return 0;
+    if (v > 1e-6) return 4;
+    if (v > 1e-7) return 3;
+    if (v > 1e-8) return 2;
+    return 1;
+}
+
+/* ---- FP64 solvers (textbook order) --------------------------------------- */
+
+void orc_csr_spmv(int n, const int *rp, const int *ci, const double *v, const double *x, double *y)
+{
+    for (int i = 0; i < n; i++) {
+        double s = 0;
+        for (int k = rp[i]; k < rp[i + 1]; k++) { double p = v[k] * x[ci[k]]; s = s + p; }
+        y[i] = s;
+    }
+}
+
+static double dot(int n, const double *a, const double *b)
+{
+    double s = 0;
+    for (int i = 0; i < n; i++) { double p = a[i] * b[i]; s = s + p; }
+    return s;
+}
+
+double orc_true_relres(int n, const int *rp, const int *ci, const double *v, const double *b, const double *x)
+{
+    double *ax = (double *)malloc((size_t)n * sizeof(double));
+    orc_csr_spmv(n, rp, ci, v, x, ax);
+    double rr = 0, bb = 0;
+    for (int i = 0; i < n; i++) { double d = b[i] - ax[i]; rr += d * d; bb += b[i] * b[i]; }
+    free(ax);
+    return bb > 0 ? sqrt(rr) / sqrt(bb) : sqrt(rr);
+}
+
+/* Unpreconditioned CG (the algorithm of src/Mille-feuille-cg.h:168-350),
+ * x0 = 0, stopping when ||r||/||b|| <= tol (the reference's stopping test
+ * is commented out at Mille-feuille-cg.h:232; tol = 0 runs maxiter).
+ * Returns the iteration count; hist (optional) gets ||r_k||/||b||. */
+int orc_cg(int n, const int *rp, const int *ci, const double *v, const double *b, double *x,
+           int maxiter, double tol, double *relres_out, double *hist)
+{
+    double *r = (double *)malloc((size_t)n * sizeof(double));
+    double *p = (double *)malloc((size_t)n * sizeof(double));
+    double *q = (double *)malloc((size_t)n * sizeof(double));
+    for (int i = 0; i < n; i++) { x[i] = 0; r[i] = b[i]; p[i] = b[i]; }
+    double bb = dot(n, b, b), rho = bb;
+    double nb = sqrt(bb) > 0 ? sqrt(bb) : 1.0;
+    int it = 0;
+    if (hist) hist[0] = sqrt(rho) / nb;
+    while (it < maxiter && sqrt(rho) / nb > tol) {
+        orc_csr_spmv(n, rp, ci, v, p, q);
+        double pq = dot(n, p, q);
+        double alpha = rho / pq;
+        for (int i = 0; i < n; i++) { x[i] = x[i] + alpha * p[i]; r[i] = r[i] - alpha * q[i]; }
+        double rho_new = dot(n, r, r);
+        double beta = rho_new / rho;
+        rho = rho_new;
+        for (int i = 0; i < n; i++) p[i] = r[i] + beta * p[i];
+        it++;
+        if (hist) hist[it] = sqrt(rho) / nb;
+    }
+    if (relres_out) *relres_out = sqrt(rho) / nb;
+    free(r); free(p); free(q);
+    return it;
+}
+
+/* Unpreconditioned BiCGSTAB (the algorithm of
+ * src/Mille-feuille-bicg.h:202-474 with r_hat = r0), x0 = 0. */
+int orc_bicgstab(int n, const int *rp, const int *ci, const double *v, const double *b, double *x,
+                 int maxiter, double tol, double *relres_out)
+{
+    size_t sz = (size_t)n * sizeof(double);
+    double *r = malloc(sz), *rh = malloc(sz), *p = malloc(sz), *vv = malloc(sz);
+    double *s = malloc(sz), *t = malloc(sz);
+    for (int i = 0; i < n; i++) { x[i] = 0; r[i] = b[i]; rh[i] = b[i]; p[i] = b[i]; }
+    double nb = sqrt(dot(n, b, b)); if (nb == 0) nb = 1;
+    double rho = dot(n, rh, r), rr = dot(n, r, r);
+    int it = 0;
+    while (it < maxiter && sqrt(rr) / nb > tol) {
+        orc_csr_spmv(n, rp, ci, v, p, vv);
+        double alpha = rho / dot(n, rh, vv);
+        for (int i = 0; i < n; i++) s[i] = r[i] - alpha * vv[i];
+        orc_csr_spmv(n, rp, ci, v, s, t);
+        double tt = dot(n, t, t);
+        double omega = tt != 0 ? dot(n, t, s) / tt : 0.0;
+        for (int i = 0; i < n; i++) { x[i] = x[i] + alpha * p[i] + omega * s[i]; r[i] = s[i] - omega * t[i]; }
+        double rho_new = dot(n, rh, r);
+        double beta = (rho_new / rho) * (alpha / omega);
+        rho = rho_new;
+        for (int i = 0; i < n; i++) p[i] = r[i] + beta * (p[i] - omega * vv[i]);
+        rr = dot(n, r, r);
+        it++;
+    }
+    if (relres_out) *relres_out = sqrt(rr) / nb;
+    free(r); free(rh); free(p); free(vv); free(s); free(t);
+    return it;
+}

@@ -1,0 +1,91 @@
+"""Persistent CG on the GPU against the FP64 CPU oracle (needs a B200)."""
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_csr(A):
+    return ol.Csr(A.n_rows, A.n_cols, A.rowptr, A.colidx, A.val)
+
+
+def test_cg_config1_laplace2d_128(mf):
+    """Configuration 1: 2D 5-point Laplacian 128x128, x* ~ U[-1,1] seed 0,
+    stop at 1e-10.  Iterations within 2% of the FP64 oracle, true residual
+    below the tolerance, solution equal to the oracle's to 1e-8."""
+    A = mf.synth_laplace2d(128, 128)
+    xs = mf.synth_xstar(0, A.n_rows)
+    b = A.matvec(xs)
+    M = mf.Matrix(A)
+    x, rep = M.solve_host(b, tol=1e-10, maxiter=5000)
+    it_o, x_o, rr_o = ol.oracle_cg(_oracle_csr(A), b, 5000, 1e-10)
+    assert rep.status == 0
+    assert rep.relres <= 1e-10
+    assert rep.relres_true <= 2e-10
+    assert abs(rep.iterations - it_o) <= max(2, it_o // 50)
+    assert np.max(np.abs(x - x_o)) <= 1e-8
+    assert np.max(np.abs(x - xs)) <= 1e-6
+    M.close()
+
+
+@pytest.mark.parametrize("name,make,seed", [
+    ("poisson3d_24", lambda mf: mf.synth_poisson3d_scaled(24, 1), 1),
+    ("randspd_3000", lambda mf: mf.synth_random_spd(107, 3000), 107),
+    ("ragged_rows", lambda mf: mf.synth_laplace2d(37, 29), 0),
+])
+def test_cg_matches_oracle(mf, name, make, seed):
+    A = make(mf)
+    xs = mf.synth_xstar(seed, A.n_rows)
+    b = A.matvec(xs)
+    M = mf.Matrix(A)
+    x, rep = M.solve_host(b, tol=1e-10, maxiter=20000)
+    it_o, x_o, rr_o = ol.oracle_cg(_oracle_csr(A), b, 20000, 1e-10)
+    assert rep.status == 0, rep.as_dict()
+    assert rep.relres_true <= 1e-9
+    assert abs(rep.iterations - it_o) <= max(3, it_o // 20), (rep.iterations, it_o)
+    assert ol.oracle_true_relres(_oracle_csr(A), b, x) <= 1e-9
+    M.close()
+
+
+def test_cg_fixed_iterations_like_reference(mf):
+    """tol < 0 runs exactly maxiter iterations (the reference's persistent CG
+    runs a fixed 100, src/Mille-feuille-cg.h:232-233)."""
+    A = mf.synth_laplace2d(64, 64)
+    b = A.matvec(np.ones(A.n_rows))
+    M = mf.Matrix(A)
+    x, rep = M.solve_host(b, tol=-1.0, maxiter=100)
+    it_o, x_o, _ = ol.oracle_cg(_oracle_csr(A), b, 100, -1.0)
+    assert rep.iterations == 100 == it_o
+    assert np.max(np.abs(x - x_o)) <= 1e-10 * max(1.0, np.max(np.abs(x_o)))
+    M.close()
+
+
+def test_cg_deterministic_runs(mf):
+    A = mf.synth_poisson3d_scaled(16, 1)
+    b = A.matvec(mf.synth_xstar(1, A.n_rows))
+    M = mf.Matrix(A)
+    x1, r1 = M.solve_host(b, tol=1e-10, maxiter=5000)
+    x2, r2 = M.solve_host(b, tol=1e-10, maxiter=5000)
+    assert r1.iterations == r2.iterations
+    assert np.array_equal(x1, x2)
+    M.close()
+
+
+def test_cg_not_converged_status(mf):
+    A = mf.synth_poisson3d_scaled(16, 1)
+    b = A.matvec(mf.synth_xstar(1, A.n_rows))
+    M = mf.Matrix(A)
+    x, rep = M.solve_host(b, tol=1e-10, maxiter=5)
+    assert rep.status == 6 and rep.iterations == 5
+    M.close()
+
+
+def test_cg_zero_rhs(mf):
+    A = mf.synth_laplace2d(32, 32)
+    M = mf.Matrix(A)
+    x, rep = M.solve_host(np.zeros(A.n_rows), tol=1e-10, maxiter=100)
+    assert rep.status == 0 and rep.iterations == 0
+    assert not np.any(x)
+    M.close()

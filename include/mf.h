@@ -48,6 +48,8 @@ typedef enum mf_status {
 const char *mf_last_error(void);
 /* Library version string. */
 const char *mf_version(void);
+/* Kernel launches issued by the library since it was loaded. */
+long long mf_kernel_launches(void);
 
 /* ---------------------------------------------------------------------- */
 /* Tiled matrix                                                            */

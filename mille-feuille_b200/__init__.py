@@ -74,6 +74,7 @@ def lib() -> C.CDLL:
         vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)
         L.mf_last_error.restype = C.c_char_p
         L.mf_version.restype = C.c_char_p
+        L.mf_kernel_launches.restype = C.c_longlong
         L.mf_matrix_create.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, C.c_int, vp, C.POINTER(vp)]
         L.mf_matrix_destroy.argtypes = [vp]
         L.mf_matrix_get_info.argtypes = [vp, C.POINTER(MatrixInfo)]

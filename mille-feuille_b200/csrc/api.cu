@@ -1,5 +1,6 @@
 // api.cu -- the C ABI (include/mf.h): handles, status codes, host/device
 // entry points.  No call aborts; every CUDA error becomes an mf_status.
+#include <atomic>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
@@ -10,6 +11,9 @@
 namespace mf {
 
 static thread_local char g_err[1024] = "";
+static std::atomic<long long> g_launches{0};
+
+void note_launch(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
 void set_last_error(const char *fmt, ...)
 {
@@ -59,6 +63,7 @@ extern "C" {
 
 const char *mf_last_error(void) { return g_err; }
 const char *mf_version(void) { return "mille-feuille-b200 0.1 (sm_100a)"; }
+long long mf_kernel_launches(void) { return g_launches.load(); }
 
 void mf_free_host(void *p) { free(p); }
 
@@ -128,7 +133,7 @@ mf_status mf_matrix_destroy(mf_matrix m)
     void *bufs[] = {m->d_tile_ptr, m->d_tile_columnidx, m->d_tile_nnz, m->d_csrptr_offset, m->d_blknnznnz, m->d_val,
                     m->d_val_low, m->d_col, m->d_ptr, m->d_cidx, m->d_f16, m->d_i8, m->d_class, m->d_nonzero_row_new,
                     m->d_tile_rowidx, m->d_block_signal, m->d_blockrowid_new, m->d_blockcsr_ptr_new, m->d_rbb_rowidx,
-                    m->d_rbb_colstart, m->d_rbb_colstop, m->d_part, m->work};
+                    m->d_rbb_colstart, m->d_rbb_colstop, m->d_part, m->work, m->host_io};
     for (void *p : bufs)
         if (p) cudaFree(p);
     delete m;
@@ -242,6 +247,7 @@ mf_status mf_encode_column_index(mf_matrix m, void *stream)
     int grid = ceil_div((n + 1) / 2, 256);
     if (grid > 148 * 16) grid = 148 * 16;
     k_encode<<<grid, 256, 0, (cudaStream_t)stream>>>(n, m->d_col, m->d_cidx);
+    note_launch();
     MF_CUDA(cudaGetLastError());
     return MF_OK;
 }
@@ -303,20 +309,23 @@ mf_status mf_cg_solve_host(mf_matrix m, const double *b_host, double *x_host, co
 {
     if (!m || !b_host || !x_host) return MF_ERR_INVALID_ARG;
     const size_t n = m->v.rows;
-    double *d = nullptr;
-    MF_CUDA(cudaMalloc(&d, sizeof(double) * (2 * n + 2)));
-    double *db = d, *dx = d + n + 1;
+    if (m->host_io_n < n) {
+        if (m->host_io) cudaFree(m->host_io);
+        m->host_io = nullptr;
+        m->host_io_n = 0;
+        MF_CUDA(cudaMalloc(&m->host_io, sizeof(double) * (2 * n + 2)));
+        m->host_io_n = n;
+    }
+    double *db = m->host_io, *dx = m->host_io + n + 1;
     cudaStream_t s = 0;
     cudaError_t e = cudaMemcpyAsync(db, b_host, sizeof(double) * n, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) {
-        cudaFree(d);
         set_last_error("H2D: %s", cudaGetErrorString(e));
         return MF_ERR_CUDA;
     }
     mf_status st = mf_cg_solve(m, db, dx, opts, report, nullptr, s);
     e = cudaMemcpyAsync(x_host, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(d);
     if (e != cudaSuccess) {
         set_last_error("D2H: %s", cudaGetErrorString(e));
         return MF_ERR_CUDA;

@@ -233,8 +233,10 @@ mf_status true_residual(mf_matrix m, const double *b, const double *x, CgWork &w
     MF_TRY(spmv_fp64(m->v, x, w.ax, s));
     const int nblk = 512;
     k_resid_partials<<<nblk, 256, 0, s>>>(n, b, w.ax, w.rpart);
+    note_launch();
     MF_CUDA(cudaGetLastError());
     k_resid_final<<<1, 32, 0, s>>>(nblk, w.rpart, w.out + 4);
+    note_launch();
     MF_CUDA(cudaGetLastError());
     double h[2];
     MF_CUDA(cudaMemcpyAsync(h, w.out + 4, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -274,6 +276,7 @@ mf_status cg_solve_fp64(mf_matrix m, const double *b, double *x, const mf_solve_
     MF_CUDA(cudaEventCreate(&e1));
     MF_CUDA(cudaEventRecord(e0, s));
     void *args[] = {&a};
+    note_launch();
     MF_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg_fp64<CG_NT>, dim3(G), dim3(CG_NT), args, 0, s));
     MF_CUDA(cudaEventRecord(e1, s));
     double h_out[3];

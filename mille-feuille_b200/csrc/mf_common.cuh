@@ -15,6 +15,8 @@ namespace mf {
 // mf_status; nothing aborts the process.
 // ---------------------------------------------------------------------------
 void set_last_error(const char *fmt, ...);
+// Counts kernel launches issued by the library (mf_kernel_launches()).
+void note_launch(int k = 1);
 
 #define MF_CUDA(expr)                                                                     \
     do {                                                                                  \

@@ -55,6 +55,9 @@ struct mf_matrix_s {
     // cached per-matrix solver workspace
     void *work = nullptr;
     size_t work_bytes = 0;
+    // device staging of b and x for the host-buffer solve entry points
+    double *host_io = nullptr;
+    size_t host_io_n = 0;
 };
 
 namespace mf {

@@ -78,17 +78,20 @@ mf_status scan_rec(const int *in, int *out, int n, cudaStream_t s, int *d_total)
     int blocks = ceil_div(n, SCAN_CHUNK);
     if (blocks <= 1) {
         k_block_scan<<<1, SCAN_NT, 0, s>>>(in, out, n, nullptr, d_total);
+        note_launch();
         MF_CUDA(cudaGetLastError());
         return MF_OK;
     }
     int *tot = nullptr;
     MF_CUDA(cudaMallocAsync(&tot, sizeof(int) * (blocks + 1), s));
     k_block_totals<<<blocks, SCAN_NT, 0, s>>>(in, n, tot);
+    note_launch();
     mf_status st = MF_OK;
     if (cudaGetLastError() != cudaSuccess) st = MF_ERR_CUDA;
     if (st == MF_OK) st = scan_rec(tot, tot, blocks, s, nullptr);
     if (st == MF_OK) {
         k_block_scan<<<blocks, SCAN_NT, 0, s>>>(in, out, n, tot, d_total);
+        note_launch();
         if (cudaGetLastError() != cudaSuccess) st = MF_ERR_CUDA;
     }
     cudaFreeAsync(tot, s);

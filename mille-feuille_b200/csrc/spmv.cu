@@ -26,6 +26,7 @@ mf_status spmv_fp64(const MfTiles &A, const double *x, double *y, cudaStream_t s
     if (A.tilem == 0) return MF_OK;
     int grid = ceil_div(A.tilem, SPMV_NT / MF_TILE);
     k_spmv_fp64<<<grid, SPMV_NT, 0, s>>>(A, x, y);
+    note_launch();
     MF_CUDA(cudaGetLastError());
     return MF_OK;
 }

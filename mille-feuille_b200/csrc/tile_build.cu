@@ -412,6 +412,7 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
     int *d_maxnz = d_err + 6;
     if (rowA > 0) {
         k_validate<<<grid_for((long long)rowA + nnz, 256), 256, 0, s>>>(rowA, colA, d_rowptr, d_colidx, d_err);
+        note_launch();
         MF_CUDA(cudaGetLastError());
     }
     int h_err = 0;
@@ -433,6 +434,7 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
     MF_TRY(dalloc(&m->d_tile_ptr, tilem + 1, &acc));
     if (tilem > 0) {
         k_sort_tilerows<<<grid_for(tilem, 1) , BUILD_NT, 0, s>>>(tilem, rowA, d_rowptr, d_colidx, d_perm, d_big, d_cnt);
+        note_launch();
         MF_CUDA(cudaGetLastError());
     }
     MF_CUDA(cudaMemsetAsync(d_cnt + tilem, 0, sizeof(int), s));
@@ -456,6 +458,7 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
         k_fill_tilerows<<<grid_for(tilem, 1), BUILD_NT, 0, s>>>(tilem, rowA, rp0, d_rowptr, d_colidx, d_val, d_val_low,
                                                                 d_perm, m->d_tile_ptr, m->d_tile_columnidx, m->d_tile_nnz,
                                                                 m->d_tile_rowidx, d_run, m->d_val, m->d_val_low, m->d_col);
+        note_launch();
         MF_CUDA(cudaGetLastError());
     }
     const int csrptrlen = (tilem > 0) ? 0 : 0;  // computed below from csrptr_offset[T]
@@ -476,9 +479,11 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
         k_tile_finish<<<grid_for(T, 256), 256, 0, s>>>(tilem, rowA, T, m->d_tile_ptr, m->d_tile_rowidx, m->d_tile_nnz,
                                                        d_run, m->d_csrptr_offset, m->d_ptr, m->d_blknnznnz, d_nzr, d_err,
                                                        nnz);
+        note_launch();
     } else {
         k_tile_finish<<<1, 32, 0, s>>>(tilem, rowA, 0, m->d_tile_ptr, m->d_tile_rowidx, m->d_tile_nnz, d_run,
                                        m->d_csrptr_offset, m->d_ptr, m->d_blknnznnz, d_nzr, d_err, nnz);
+        note_launch();
     }
     MF_CUDA(cudaGetLastError());
     MF_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -505,6 +510,7 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
         k_nonzero_lists<<<grid_for(T, 256), 256, 0, s>>>(tilem, rowA, T, m->d_tile_rowidx, m->d_tile_nnz,
                                                          m->d_csrptr_offset, m->d_ptr, d_nzr, m->d_blockrowid_new,
                                                          m->d_blockcsr_ptr_new);
+        note_launch();
         MF_CUDA(cudaGetLastError());
     }
 
@@ -515,6 +521,7 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
         int *d_rc = nullptr;
         MF_CUDA(cudaMallocAsync(&d_rc, sizeof(int) * (tilem + 1), s));
         k_rbb_count<<<grid_for(tilem + 1, 256), 256, 0, s>>>(tilem, m->d_tile_ptr, d_rc, m->d_block_signal);
+        note_launch();
         MF_CUDA(cudaGetLastError());
         MF_TRY(exclusive_scan_i32(d_rc, d_rc, tilem + 1, s, &rbb));
         MF_TRY(dalloc(&m->d_rbb_rowidx, rbb, &acc));
@@ -523,6 +530,7 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
         if (tilem > 0) {
             k_rbb_fill<<<grid_for(tilem, 256), 256, 0, s>>>(tilem, m->d_tile_ptr, d_rc, m->d_rbb_rowidx,
                                                             m->d_rbb_colstart, m->d_rbb_colstop);
+            note_launch();
             MF_CUDA(cudaGetLastError());
         }
         cudaFreeAsync(d_rc, s);
@@ -535,6 +543,7 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
     if (T > 0) {
         k_payloads<<<grid_for(T, 256), 256, 0, s>>>(T, m->d_tile_nnz, m->d_val, m->d_val_low, m->d_f16, m->d_i8,
                                                     m->d_class, d_class_count, d_maxnz);
+        note_launch();
         MF_CUDA(cudaGetLastError());
     }
     int host_counts[8] = {0};
@@ -581,9 +590,11 @@ mf_status strip_partition(mf_matrix m, int ctas, cudaStream_t s)
     int *d_cost = nullptr;
     MF_CUDA(cudaMallocAsync(&d_cost, sizeof(int) * (tilem + 1), s));
     k_strip_cost<<<grid_for(tilem + 1, 256), 256, 0, s>>>(tilem, m->d_tile_ptr, m->d_tile_nnz, d_cost);
+    note_launch();
     MF_CUDA(cudaGetLastError());
     MF_TRY(exclusive_scan_i32(d_cost, d_cost, tilem + 1, s, nullptr));
     k_strip_split<<<grid_for(ctas + 1, 256), 256, 0, s>>>(tilem, ctas, d_cost, m->d_part);
+    note_launch();
     MF_CUDA(cudaGetLastError());
     cudaFreeAsync(d_cost, s);
     m->part_ctas = ctas;

@@ -124,3 +124,46 @@ void ref_read_mtx_fetch(int *rp, int *ci, double *v)
     memcpy(ci, g_ci, sizeof(int) * g_nnz);
     memcpy(v, g_v, sizeof(double) * g_nnz);
 }
+
+/* CPU baseline: `iters` iterations of FP64 CG whose SpMV is one call of the
+ * reference blockspmv_cpu per iteration (its schedule allocation included,
+ * as the reference does per call), on the last created (and encoded)
+ * matrix.  The reference has no CPU CG; the vector updates and dot products
+ * are this harness's own loops, OpenMP-parallel over `threads` threads.
+ * Returns the elapsed wall time in seconds; x, r, p are caller buffers of
+ * tilen*16 doubles (x0 = 0, r = p = b on entry when start != 0). */
+double ref_cg_iterations(int rowA, int colA, int nnzA, const double *b, double *x, double *r, double *p,
+                         double *q, int iters, int threads, int start, double *rho_io)
+{
+    Tile_matrix *m = g_last;
+    int n = rowA;
+    int *p1 = (int *)malloc(sizeof(int) * (m->tilenum + 1));
+    int *p2 = (int *)malloc(sizeof(int) * (m->tilenum + 1));
+    omp_set_num_threads(threads);
+    double rho = *rho_io;
+    if (start) {
+        rho = 0;
+#pragma omp parallel for reduction(+ : rho)
+        for (int i = 0; i < n; i++) { x[i] = 0; r[i] = b[i]; p[i] = b[i]; rho += b[i] * b[i]; }
+    }
+    double t0 = omp_get_wtime();
+    for (int it = 0; it < iters; it++) {
+        int rbb; unsigned int *ri; int *cs, *ce;
+        blockspmv_cpu(m, p1, p2, &rbb, &ri, &cs, &ce, rowA, colA, nnzA, NULL, NULL, NULL, p, q, NULL);
+        free(ri); free(cs); free(ce);
+        double pq = 0;
+#pragma omp parallel for reduction(+ : pq)
+        for (int i = 0; i < n; i++) pq += p[i] * q[i];
+        double alpha = rho / pq, rr = 0;
+#pragma omp parallel for reduction(+ : rr)
+        for (int i = 0; i < n; i++) { x[i] += alpha * p[i]; r[i] -= alpha * q[i]; rr += r[i] * r[i]; }
+        double beta = rr / rho;
+        rho = rr;
+#pragma omp parallel for
+        for (int i = 0; i < n; i++) p[i] = r[i] + beta * p[i];
+    }
+    double t1 = omp_get_wtime();
+    *rho_io = rho;
+    free(p1); free(p2);
+    return t1 - t0;
+}

@@ -34,8 +34,8 @@ mf_status ensure_work(mf_matrix m, size_t bytes)
     return MF_OK;
 }
 
-mf_status cg_solve_fp64(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,
-                        double *history, cudaStream_t s);
+mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,
+                   double *history, cudaStream_t s);
 
 static mf_status check_device()
 {
@@ -133,7 +133,8 @@ mf_status mf_matrix_destroy(mf_matrix m)
     void *bufs[] = {m->d_tile_ptr, m->d_tile_columnidx, m->d_tile_nnz, m->d_csrptr_offset, m->d_blknnznnz, m->d_val,
                     m->d_val_low, m->d_col, m->d_ptr, m->d_cidx, m->d_f16, m->d_i8, m->d_class, m->d_nonzero_row_new,
                     m->d_tile_rowidx, m->d_block_signal, m->d_blockrowid_new, m->d_blockcsr_ptr_new, m->d_rbb_rowidx,
-                    m->d_rbb_colstart, m->d_rbb_colstop, m->d_part, m->work, m->host_io};
+                    m->d_rbb_colstart, m->d_rbb_colstop, m->d_part, m->work, m->host_io,
+                    m->d_wcls, m->d_poff, m->d_pay};
     for (void *p : bufs)
         if (p) cudaFree(p);
     delete m;
@@ -293,8 +294,8 @@ mf_status mf_cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_op
     mf_status st;
     if (m->v.rows == 0) {
         st = MF_OK;
-    } else if (o.policy == MF_POLICY_FP64) {
-        st = cg_solve_fp64(m, b, x, o, rep, history, (cudaStream_t)stream);
+    } else if (o.policy == MF_POLICY_FP64 || o.policy == MF_POLICY_STATIC || o.policy == MF_POLICY_RULE) {
+        st = cg_solve(m, b, x, o, rep, history, (cudaStream_t)stream);
     } else {
         set_last_error("policy %d not available in this build", o.policy);
         st = MF_ERR_UNSUPPORTED;

@@ -55,6 +55,12 @@ struct mf_matrix_s {
     // cached per-matrix solver workspace
     void *work = nullptr;
     size_t work_bytes = 0;
+    // mixed precision: working class per tile and the packed payload
+    unsigned char *d_wcls = nullptr;
+    unsigned *d_poff = nullptr;
+    unsigned char *d_pay = nullptr;
+    size_t pay_bytes = 0, pay_used = 0;
+    int packed_policy = -1;
     // device staging of b and x for the host-buffer solve entry points
     double *host_io = nullptr;
     size_t host_io_n = 0;

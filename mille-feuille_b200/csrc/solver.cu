@@ -1,0 +1,127 @@
+// solver.cu -- host orchestration of the persistent CG solves (policies,
+// checkpoints, reports).
+#include <cmath>
+#include <cstring>
+
+#include "solver.h"
+
+namespace mf {
+
+mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,
+                   double *history, cudaStream_t s)
+{
+    const bool mixed = o.policy != MF_POLICY_FP64;
+    const int G = solver_grid(m, mixed);
+    MF_TRY(strip_partition(m, G, s));
+    SolverWork w;
+    MF_TRY(solver_resources(m, G, w));
+    const int T = m->v.tilenum;
+    if (mixed) {
+        if (!m->d_wcls) MF_CUDA(cudaMalloc(&m->d_wcls, (size_t)T + 16));
+        if (m->packed_policy != MF_POLICY_STATIC) {
+            MF_TRY(static_working_classes(m, m->d_wcls, s));
+            MF_TRY(pack_payload(m, m->d_wcls, s));
+            m->packed_policy = MF_POLICY_STATIC;
+        }
+    }
+    CgArgs a;
+    memset(&a, 0, sizeof(a));
+    a.A = m->v;
+    a.part = m->d_part;
+    a.pay = m->d_pay;
+    a.poff = m->d_poff;
+    a.wcls = m->d_wcls;
+    a.b = b;
+    a.xhi = x;
+    a.r = w.r;
+    a.p0 = w.p0;
+    a.p1 = w.p1;
+    a.q = w.q;
+    a.xlo = w.xlo;
+    a.partials = w.partials;
+    a.bar = w.bar;
+    a.status = w.status;
+    a.state = w.state;
+    a.hist = (o.record_history && history) ? history : nullptr;
+    a.maxiter = o.maxiter;
+    a.tol = o.tol;
+    a.fixed = o.tol < 0 ? 1 : 0;
+    a.delta = o.refine_delta > 0 && o.refine_delta < 1 ? o.refine_delta : 0.1;
+    a.exit_on_refine = (mixed && o.policy != MF_POLICY_STATIC) ? 1 : 0;
+    a.budget_ns = (unsigned long long)(o.wait_budget_s * 1e9);
+    a.start = 1;
+    MF_CUDA(cudaMemsetAsync(w.status, 0, sizeof(int), s));
+    cudaEvent_t e0, e1;
+    MF_CUDA(cudaEventCreate(&e0));
+    MF_CUDA(cudaEventCreate(&e1));
+    MF_CUDA(cudaEventRecord(e0, s));
+    double st[S_COUNT];
+    int h_status = 0, launches = 0;
+    for (;;) {
+        MF_CUDA(cudaMemsetAsync(w.bar, 0, sizeof(unsigned long long), s));
+        MF_TRY(launch_cg(mixed, a, G, s));
+        launches++;
+        if (!a.exit_on_refine) break;
+        MF_CUDA(cudaMemcpyAsync(st, w.state, sizeof(st), cudaMemcpyDeviceToHost, s));
+        MF_CUDA(cudaMemcpyAsync(&h_status, w.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MF_CUDA(cudaStreamSynchronize(s));
+        if (h_status != 0 || (int)st[S_EXIT] != EXIT_CHECKPOINT) break;
+        // checkpoint: the policy picks new working classes, the payload is
+        // repacked, and the solve resumes from the saved state
+        const int it = (int)st[S_ITERS];
+        const void *pnew = (it & 1) ? w.p1 : w.p0;  // written by the last iteration
+        const void *pold = (it & 1) ? w.p0 : w.p1;
+        if (o.policy == MF_POLICY_RULE) {
+            MF_TRY(rule_working_classes(m, pnew, pold, m->d_wcls, s));
+        } else {
+            MF_TRY(learned_working_classes(m, w, pnew, pold, m->d_wcls, s));
+        }
+        MF_TRY(pack_payload(m, m->d_wcls, s));
+        m->packed_policy = o.policy;
+        a.start = 0;
+    }
+    MF_CUDA(cudaEventRecord(e1, s));
+    MF_CUDA(cudaMemcpyAsync(st, w.state, sizeof(st), cudaMemcpyDeviceToHost, s));
+    MF_CUDA(cudaMemcpyAsync(&h_status, w.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MF_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    rep.iterations = (int)st[S_ITERS];
+    rep.refinements = (int)st[S_REFS];
+    rep.grid_ctas = G;
+    rep.kernel_ms = ms;
+    rep.relres = st[S_RELRES];
+    const long long n = m->v.rows, nnz = m->v.nnz;
+    if (!mixed) {
+        rep.bytes_moved = (long long)rep.iterations * (nnz * 9 + 24LL * T + 16 * n + 72 * n);
+    } else {
+        // per iteration: packed payload + column bytes + tile metadata + FP32
+        // vectors (p, q gathered/written, x_lo, r: 9 streams of 4 bytes);
+        // per reliable update: an FP64 SpMV plus 5 FP64/FP32 streams
+        const long long spmv_mixed = (long long)m->pay_used + nnz + 24LL * T + 8 * n;
+        const long long spmv_fp64 = nnz * 9 + 24LL * T + 16 * n;
+        rep.bytes_moved = (long long)rep.iterations * (spmv_mixed + 36 * n) +
+                          (long long)rep.refinements * (spmv_fp64 + 32 * n);
+    }
+    (void)launches;
+    MF_TRY(true_residual(m, b, x, w, &rep.relres_true, s));
+    if (h_status != 0) {
+        rep.status = h_status;
+        set_last_error(h_status == MF_ERR_TIMEOUT ? "grid-wide wait exceeded its budget" : "CG breakdown");
+        return (mf_status)h_status;
+    }
+    if (!a.fixed && !(rep.relres_true <= o.tol * (1.0 + 1e-6) || rep.relres <= o.tol)) {
+        rep.status = MF_ERR_NOT_CONVERGED;
+        return MF_ERR_NOT_CONVERGED;
+    }
+    if (!a.fixed && (int)st[S_EXIT] == EXIT_MAXITER) {
+        rep.status = MF_ERR_NOT_CONVERGED;
+        return MF_ERR_NOT_CONVERGED;
+    }
+    rep.status = MF_OK;
+    return MF_OK;
+}
+
+}  // namespace mf

@@ -1,0 +1,54 @@
+// solver.h -- internal interface of the persistent solver kernels.
+#pragma once
+#include "mf_internal.h"
+
+namespace mf {
+
+// Persistent solver state kept in device memory between launches.
+enum : int { S_RHO = 0, S_BETA, S_NB, S_RMAX, S_ITERS, S_REFS, S_EXIT, S_RELRES, S_COUNT };
+// Why a launch returned.
+enum : int { EXIT_CONVERGED = 1, EXIT_MAXITER = 2, EXIT_BREAKDOWN = 3, EXIT_CHECKPOINT = 4 };
+
+struct CgArgs {
+    MfTiles A;
+    const int *part;               // [G+1] strip range of each CTA
+    const unsigned char *pay;      // mixed: packed per-tile payload bytes
+    const unsigned *poff;          // mixed: [T+1] byte offset of each tile's payload
+    const unsigned char *wcls;     // mixed: [T] working class of each tile
+    const double *b;
+    double *xhi;                   // solution (FP64)
+    void *r, *p0, *p1, *q, *xlo;   // vectors (FP64, or FP32 when mixed)
+    double *partials;              // [4][G] per-CTA dot partials
+    unsigned long long *bar;       // grid barrier counter (0 at launch)
+    int *status;                   // device status word (mf_status codes)
+    double *state;                 // [S_COUNT]
+    double *hist;                  // optional per-iteration ||r||/||b||
+    int maxiter;
+    double tol;
+    int fixed;                     // 1: run exactly maxiter iterations
+    double delta;                  // reliable-update trigger
+    int exit_on_refine;            // 1: return after each reliable update
+    unsigned long long budget_ns;  // bound of every grid-wide wait
+    int start;                     // 1: initialise x, r, p and the state
+};
+
+struct SolverWork {
+    void *r, *p0, *p1, *q, *xlo;
+    double *ax, *partials, *rpart, *out, *state;
+    unsigned long long *bar;
+    int *status;
+};
+
+mf_status solver_resources(mf_matrix m, int G, SolverWork &w);
+int solver_grid(mf_matrix m, bool mixed);
+mf_status launch_cg(bool mixed, CgArgs &a, int G, cudaStream_t s);
+mf_status true_residual(mf_matrix m, const double *b, const double *x, SolverWork &w, double *relres, cudaStream_t s);
+// payload.cu
+mf_status pack_payload(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s);
+mf_status static_working_classes(mf_matrix m, unsigned char *d_wcls, cudaStream_t s);
+mf_status learned_working_classes(mf_matrix m, SolverWork &w, const void *p_new, const void *p_old,
+                                  unsigned char *d_wcls, cudaStream_t s);
+mf_status rule_working_classes(mf_matrix m, const void *p_new, const void *p_old, unsigned char *d_wcls,
+                               cudaStream_t s);
+
+}  // namespace mf

@@ -297,10 +297,11 @@ __global__ void k_rbb_fill(int tilem, const int *__restrict__ tile_ptr, const in
     }
 }
 
-// Static (value-range) class per tile and the low-precision payloads.
+// Static (value-range) class per tile: the smallest format that holds every
+// value of the tile exactly.
 //   int8 : every value an integer in [-128, 127]
-//   fp16 : every nonzero |v| inside the fp16 normal range [2^-14, 65504]
-//   fp32 : every nonzero |v| inside the fp32 normal range
+//   fp16 : every value exactly representable in binary16
+//   fp32 : every value exactly representable in binary32
 //   fp64 : otherwise
 // Payloads: fp16 = (half)(float)v, int8 = (int8_t)v (low byte of the
 // truncated 32-bit integer), as src/main-cg-mixed.cu:2333-2336 builds them.
@@ -314,15 +315,14 @@ __global__ void k_payloads(int T, const int *__restrict__ tile_nnz, const double
         for (int k = a; k < b; k++) {
             const double v = val[k];
             const double av = fabs(v);
-            half h = __float2half_rn(low[k]);
+            const half h = __float2half_rn(low[k]);
             f16[k] = __half_as_ushort(h);
             long long w = (av < 2147483648.0) ? (long long)__double2int_rz(v) : (long long)INT_MIN;
             i8[k] = (int8_t)(unsigned char)(unsigned)(int)w;
             if (!(v == trunc(v) && v >= -128.0 && v <= 127.0)) is_int8 = false;
-            if (v != 0.0) {
-                if (!(av >= 6.103515625e-05 && av <= 65504.0)) in16 = false;
-                if (!(av >= 1.1754943508222875e-38 && av <= 3.4028234663852886e38)) in32 = false;
-            }
+            const float vf = (float)v;
+            if ((double)vf != v) in32 = false;
+            if ((double)__half2float(h) != v) in16 = false;
         }
         unsigned char c = is_int8 ? MF_CLASS_INT8 : in16 ? MF_CLASS_FP16 : in32 ? MF_CLASS_FP32 : MF_CLASS_FP64;
         cls[t] = c;

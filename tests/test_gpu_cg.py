@@ -89,3 +89,54 @@ def test_cg_zero_rhs(mf):
     assert rep.status == 0 and rep.iterations == 0
     assert not np.any(x)
     M.close()
+
+
+@pytest.mark.parametrize("policy", ["static", "rule"])
+@pytest.mark.parametrize("name,make,seed", [
+    ("laplace2d_128", lambda mf: mf.synth_laplace2d(128, 128), 0),
+    ("poisson3d_32", lambda mf: mf.synth_poisson3d_scaled(32, 1), 1),
+    ("aniso_16", lambda mf: mf.synth_aniso3d(16, 3), 3),
+])
+def test_mixed_precision_reaches_fp64_accuracy(mf, policy, name, make, seed):
+    """Mixed tiles with FP32 accumulation and FP64 reliable updates reach the
+    same 1e-10 FP64 true residual as the plain oracle; the error against the
+    FP64 oracle solution is reported by the tolerance of the assertion."""
+    A = make(mf)
+    xs = mf.synth_xstar(seed, A.n_rows)
+    b = A.matvec(xs)
+    M = mf.Matrix(A)
+    x, rep = M.solve_host(b, tol=1e-10, maxiter=50000, policy=policy)
+    Ac = _oracle_csr(A)
+    it_o, x_o, _ = ol.oracle_cg(Ac, b, 50000, 1e-10)
+    assert rep.status == 0, rep.as_dict()
+    assert rep.refinements >= 1
+    true_rr = ol.oracle_true_relres(Ac, b, x)
+    assert true_rr <= 1.05e-10, (true_rr, rep.as_dict())
+    # same accuracy class as the FP64 solve: error vs the oracle solution
+    # bounded by the error the oracle itself has against x*
+    err_o = np.max(np.abs(x_o - xs))
+    assert np.max(np.abs(x - x_o)) <= 10 * err_o + 1e-12
+    # the iteration count stays near the FP64 one
+    assert rep.iterations <= 2 * it_o + 50, (rep.iterations, it_o)
+    M.close()
+
+
+def test_static_classes_laplacian_is_int8(mf):
+    A = mf.synth_laplace2d(64, 64)
+    M = mf.Matrix(A)
+    inf = M.info()
+    assert inf.class_tiles[2] == inf.tilenum  # every tile integer-valued
+    cls = M.export("tile_class")
+    assert np.all(cls == 2)
+    M.close()
+
+
+def test_mixed_deterministic(mf):
+    A = mf.synth_poisson3d_scaled(24, 1)
+    b = A.matvec(mf.synth_xstar(1, A.n_rows))
+    M = mf.Matrix(A)
+    x1, r1 = M.solve_host(b, tol=1e-10, maxiter=20000, policy="static")
+    x2, r2 = M.solve_host(b, tol=1e-10, maxiter=20000, policy="static")
+    assert r1.iterations == r2.iterations and r1.refinements == r2.refinements
+    assert np.array_equal(x1, x2)
+    M.close()

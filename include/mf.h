@@ -141,6 +141,7 @@ typedef struct mf_solve_opts {
                              since the last FP64 residual (mixed policies) */
     double wait_budget_s; /* bound on every grid-wide wait inside a kernel */
     int record_history;   /* keep ||r_k||/||b|| per iteration (see report) */
+    int phase_times;      /* fill mf_solve_report.phase_us (device timers) */
 } mf_solve_opts;
 
 typedef struct mf_solve_report {
@@ -152,6 +153,11 @@ typedef struct mf_solve_report {
     double kernel_ms;      /* device time of the solve kernels */
     long long bytes_moved; /* algorithmic bytes of the solve */
     int grid_ctas;         /* CTAs of the persistent launch */
+    /* with opts.phase_times: mean over CTAs of the time (us, whole solve)
+     * spent in [0] the SpMV phase, [1] its reduction wait, [2] the vector
+     * update phase, [3] its reduction wait, [4] reliable updates, and [5]
+     * the largest per-CTA SpMV-phase time */
+    double phase_us[6];
 } mf_solve_report;
 
 /* Fills opts with the defaults (maxiter 20000, tol 1e-10, FP64 policy). */

@@ -39,16 +39,18 @@ class MatrixInfo(C.Structure):
 
 class SolveOpts(C.Structure):
     _fields_ = [("maxiter", C.c_int), ("tol", C.c_double), ("policy", C.c_int), ("refine_delta", C.c_double),
-                ("wait_budget_s", C.c_double), ("record_history", C.c_int)]
+                ("wait_budget_s", C.c_double), ("record_history", C.c_int), ("phase_times", C.c_int)]
 
 
 class SolveReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("refinements", C.c_int), ("relres", C.c_double),
                 ("relres_true", C.c_double), ("kernel_ms", C.c_double), ("bytes_moved", C.c_longlong),
-                ("grid_ctas", C.c_int)]
+                ("grid_ctas", C.c_int), ("phase_us", C.c_double * 6)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["phase_us"] = list(self.phase_us)
+        return d
 
 
 ARRAY_DTYPES = {

@@ -268,6 +268,7 @@ void mf_solve_opts_default(mf_solve_opts *o)
     o->refine_delta = 0.1;
     o->wait_budget_s = 5.0;
     o->record_history = 0;
+    o->phase_times = 0;
 }
 
 mf_status mf_cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts *opts, mf_solve_report *report,

@@ -24,6 +24,8 @@
 //     by refine_delta, the FP32 correction is added to the FP64 solution and
 //     r is replaced by the FP64 true residual b - A x computed from the FP64
 //     payload.  Convergence is only declared on that FP64 true residual.
+#include <cstdlib>
+
 #include "strip_stage.cuh"
 #include "solver.h"
 
@@ -276,6 +278,15 @@ __global__ void __launch_bounds__(NT, 4) k_cg(CgArgs a)
     }
     int exit_reason = EXIT_MAXITER;
     double relres_true = sqrt(rho) / nb;
+    // optional phase timers (thread 0 of each CTA)
+    unsigned long long tph[5] = {0, 0, 0, 0, 0}, tmark = 0;
+    const bool timed = a.timing != nullptr && threadIdx.x == 0;
+#define MF_MARK(k)                                        \
+    if (timed) {                                          \
+        const unsigned long long now_ = globaltimer_ns(); \
+        if ((k) >= 0) tph[(k)] += now_ - tmark;           \
+        tmark = now_;                                     \
+    }
     bool converged_check = false;
     while (gc.ok) {
         if (!a.fixed && sqrt(rho) <= a.tol * nb) {
@@ -289,6 +300,7 @@ __global__ void __launch_bounds__(NT, 4) k_cg(CgArgs a)
         const VT *pold = (const VT *)((it & 1) ? a.p1 : a.p0);
         VT *pnew = (VT *)((it & 1) ? a.p0 : a.p1);
         const VT bt = (VT)beta;
+        MF_MARK(-1);
         // ---- q = A p_new with p_new = r + beta p_old formed on the fly ----
         double loc = 0.0;
         auto psrc = [=](int c) -> VT {
@@ -307,7 +319,9 @@ __global__ void __launch_bounds__(NT, 4) k_cg(CgArgs a)
                 loc = __dadd_rn(loc, __dmul_rn((double)pn, (double)qi));
             }
         }
+        MF_MARK(0);
         const double pq = grid_sum(a, loc, 2, gc, s_warp, &s_res);
+        MF_MARK(1);
         if (!gc.ok) break;
         if (!(pq != 0.0) || !isfinite(pq)) {
             if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(a.status, DEV_OK, DEV_BREAKDOWN);
@@ -334,7 +348,9 @@ __global__ void __launch_bounds__(NT, 4) k_cg(CgArgs a)
                 }
             }
         }
+        MF_MARK(2);
         double rho_new = grid_sum(a, loc, 3, gc, s_warp, &s_res);
+        MF_MARK(3);
         if (!gc.ok) break;
         it++;
         bool refined = false;
@@ -370,6 +386,7 @@ __global__ void __launch_bounds__(NT, 4) k_cg(CgArgs a)
             relres_true = sqrt(rho_new) / nb;
             refs++;
             refined = true;
+            MF_MARK(4);
         }
         beta = rho_new / rho;
         rho = rho_new;
@@ -393,6 +410,9 @@ __global__ void __launch_bounds__(NT, 4) k_cg(CgArgs a)
             }
         }
     }
+#undef MF_MARK
+    if (timed)
+        for (int k = 0; k < 5; k++) a.timing[blockIdx.x * 8 + k] += tph[k];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         st[S_RHO] = rho;
         st[S_BETA] = beta;
@@ -475,6 +495,7 @@ mf_status solver_resources(mf_matrix m, int G, SolverWork &w)
     const size_t o_rp = off; off += align256((size_t)2 * 1024 * 8);
     const size_t o_out = off; off += align256(8 * 8);
     const size_t o_state = off; off += align256(32 * 8);
+    const size_t o_tim = off; off += align256((size_t)G * 8 * 8);
     const size_t o_bar = off; off += align256(8);
     const size_t o_st = off; off += align256(8);
     MF_TRY(ensure_work(m, off));
@@ -489,6 +510,7 @@ mf_status solver_resources(mf_matrix m, int G, SolverWork &w)
     w.rpart = (double *)(base + o_rp);
     w.out = (double *)(base + o_out);
     w.state = (double *)(base + o_state);
+    w.timing = (unsigned long long *)(base + o_tim);
     w.bar = (unsigned long long *)(base + o_bar);
     w.status = (int *)(base + o_st);
     return MF_OK;
@@ -496,7 +518,11 @@ mf_status solver_resources(mf_matrix m, int G, SolverWork &w)
 
 int solver_grid(mf_matrix m, bool mixed)
 {
-    const int maxc = mixed ? max_ctas_for<true>() : max_ctas_for<false>();
+    int maxc = mixed ? max_ctas_for<true>() : max_ctas_for<false>();
+    if (const char *e = getenv("MF_SOLVER_CTAS")) {
+        const int v = atoi(e);
+        if (v > 0 && v < maxc) maxc = v;
+    }
     int want = ceil_div(m->v.tilem, NT / MF_TILE);
     if (want < 1) want = 1;
     return want < maxc ? want : maxc;

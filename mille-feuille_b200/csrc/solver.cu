@@ -1,7 +1,9 @@
 // solver.cu -- host orchestration of the persistent CG solves (policies,
 // checkpoints, reports).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "solver.h"
 
@@ -50,6 +52,8 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
     a.exit_on_refine = (mixed && o.policy != MF_POLICY_STATIC) ? 1 : 0;
     a.budget_ns = (unsigned long long)(o.wait_budget_s * 1e9);
     a.start = 1;
+    a.timing = o.phase_times ? w.timing : nullptr;
+    if (a.timing) MF_CUDA(cudaMemsetAsync(w.timing, 0, sizeof(unsigned long long) * 8 * G, s));
     MF_CUDA(cudaMemsetAsync(w.status, 0, sizeof(int), s));
     cudaEvent_t e0, e1;
     MF_CUDA(cudaEventCreate(&e0));
@@ -106,6 +110,17 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
                           (long long)rep.refinements * (spmv_fp64 + 32 * n);
     }
     (void)launches;
+    if (a.timing) {
+        std::vector<unsigned long long> t((size_t)G * 8);
+        MF_CUDA(cudaMemcpy(t.data(), w.timing, sizeof(unsigned long long) * 8 * G, cudaMemcpyDeviceToHost));
+        double mx = 0;
+        for (int k = 0; k < 6; k++) rep.phase_us[k] = 0;
+        for (int g = 0; g < G; g++) {
+            for (int k = 0; k < 5; k++) rep.phase_us[k] += t[(size_t)g * 8 + k] * 1e-3 / G;
+            mx = std::max(mx, t[(size_t)g * 8] * 1e-3);
+        }
+        rep.phase_us[5] = mx;
+    }
     MF_TRY(true_residual(m, b, x, w, &rep.relres_true, s));
     if (h_status != 0) {
         rep.status = h_status;

@@ -30,11 +30,13 @@ struct CgArgs {
     int exit_on_refine;            // 1: return after each reliable update
     unsigned long long budget_ns;  // bound of every grid-wide wait
     int start;                     // 1: initialise x, r, p and the state
+    unsigned long long *timing;    // optional [G][8] per-CTA phase nanoseconds
 };
 
 struct SolverWork {
     void *r, *p0, *p1, *q, *xlo;
     double *ax, *partials, *rpart, *out, *state;
+    unsigned long long *timing;
     unsigned long long *bar;
     int *status;
 };

@@ -7,15 +7,19 @@
 // one launch runs the whole iteration loop -- and changes how it maps to a
 // B200:
 //   * cooperative launch sized to the resident CTAs, so every grid-wide wait
-//     can finish; every wait is bounded and reports MF_ERR_TIMEOUT;
-//   * each CTA owns a contiguous, cost-balanced range of 16-row strips, both
-//     for the SpMV and for the vector updates; a half-warp stages one strip
-//     (payload, column bytes, row pointers, x segments) in shared memory with
-//     asynchronous 16-byte copies before computing its 16 rows;
+//     can finish; every wait (grid barrier, mbarrier) is bounded in time and
+//     reports MF_ERR_TIMEOUT through a status word instead of hanging;
+//   * each CTA owns a contiguous, cost-balanced range of 16-row strips, cut
+//     into chunks of up to 16 strips.  A chunk's tile metadata, u8 row
+//     pointers, column bytes and payload are contiguous byte ranges; one
+//     thread stages them into shared memory with bulk asynchronous copies
+//     (TMA, cp.async.bulk, completion on an mbarrier), two chunks in flight;
+//     the CTA then builds the chunk's x segments and computes its rows from
+//     shared memory, one half-warp per strip and one lane per row;
 //   * two grid-wide reductions per iteration and no third barrier: the new
-//     search direction p = r + beta p is formed on the fly while the SpMV
-//     gathers its x segments (p is double-buffered), so no pass writes p
-//     before the next SpMV may read it;
+//     search direction p = r + beta p is formed while the SpMV builds its x
+//     segments (p is double-buffered), so no pass must write p before the
+//     next SpMV can start;
 //   * deterministic dot products (fixed per-thread order, fixed CTA tree,
 //     per-CTA partials summed in the same order by every CTA);
 //   * mixed precision (policies STATIC/RULE/LEARNED): per-tile payload classes
@@ -24,15 +28,48 @@
 //     by refine_delta, the FP32 correction is added to the FP64 solution and
 //     r is replaced by the FP64 true residual b - A x computed from the FP64
 //     payload.  Convergence is only declared on that FP64 true residual.
+#include <cuda_fp16.h>
+
 #include <cstdlib>
 
-#include "strip_stage.cuh"
 #include "solver.h"
+#include "tma.cuh"
 
 namespace mf {
 namespace {
 
 constexpr int NT = 256;
+constexpr int HWS = NT / MF_TILE;  // half-warps per CTA = strips per chunk
+static_assert(HWS == CH_STRIPS, "one half-warp per strip of a chunk");
+
+// Byte layout of one shared-memory stage (every region 16-byte aligned,
+// sized for the largest 16-byte-rounded range it receives).
+constexpr int OFF_TPTR = 0;                                   // tile_ptr[s0..s1]
+constexpr int OFF_TCOL = 112;                                 // tile_columnidx[t0..t1)
+constexpr int OFF_TNNZ = OFF_TCOL + CH_TILES * 4 + 32;        // tile_nnz[t0..t1]
+constexpr int OFF_POFF = OFF_TNNZ + CH_TILES * 4 + 48;        // packed offsets[t0..t1]
+constexpr int OFF_WCLS = OFF_POFF + CH_TILES * 4 + 48;        // classes[t0..t1)
+constexpr int OFF_PTR = OFF_WCLS + CH_TILES + 32;             // u8 row pointers
+constexpr int OFF_COL = OFF_PTR + CH_TILES * MF_TILE + 32;    // in-tile column bytes
+constexpr int OFF_PAY = OFF_COL + CH_ENTRIES + 32;            // payload
+constexpr int STAGE_BYTES = OFF_PAY + CH_ENTRIES * 8 + 32;
+static_assert(OFF_TNNZ % 16 == 0 && OFF_POFF % 16 == 0 && OFF_WCLS % 16 == 0 && OFF_PTR % 16 == 0 &&
+                  OFF_COL % 16 == 0 && OFF_PAY % 16 == 0 && STAGE_BYTES % 16 == 0,
+              "stage regions must be 16-byte aligned");
+
+struct StageHdr {
+    ChunkRec rec;
+    int sh_tptr, sh_tcol, sh_tnnz, sh_poff, sh_wcls, sh_ptr, sh_col, sh_pay;
+};
+
+struct __align__(16) SolverSmem {
+    unsigned char stage[2][STAGE_BYTES];
+    double seg[CH_TILES * MF_TILE];
+    StageHdr hdr[2];
+    uint64_t bar[2];
+    double warp[NT / 32];
+    double res;
+};
 
 template <bool MIX>
 struct VecT {
@@ -46,228 +83,275 @@ struct VecT<true> {
 struct GridCtx {
     unsigned long long epoch;
     bool ok;
+    unsigned use[2];  // completed uses of each stage (mbarrier phase parity)
 };
 
-__device__ __forceinline__ double grid_sum(const CgArgs &a, double local, int slot, GridCtx &gc, double *s_warp,
-                                           double *s_res)
+__device__ __forceinline__ double grid_sum(const CgArgs &a, double local, int slot, GridCtx &gc, SolverSmem &S)
 {
     const int G = gridDim.x;
-    double cta = block_sum<NT>(local, s_warp);
+    double cta = block_sum<NT>(local, S.warp);
     if (threadIdx.x == 0) a.partials[slot * G + blockIdx.x] = cta;
     gc.epoch++;
-    gc.ok = gc.ok && grid_barrier(a.bar, gc.epoch * (unsigned long long)G, a.status, a.budget_ns);
+    gc.ok = gc.ok && grid_barrier_sharded(a.bar, gc.epoch, a.status, a.budget_ns);
     if (threadIdx.x < 32) {
         double s = warp_sum_partials(a.partials + slot * G, G);
-        if (threadIdx.x == 0) *s_res = s;
+        if (threadIdx.x == 0) S.res = s;
     }
     __syncthreads();
-    return *s_res;
+    return S.res;
 }
 
 __device__ __forceinline__ void grid_sync(const CgArgs &a, GridCtx &gc)
 {
     gc.epoch++;
-    gc.ok = gc.ok && grid_barrier(a.bar, gc.epoch * (unsigned long long)gridDim.x, a.status, a.budget_ns);
+    gc.ok = gc.ok && grid_barrier_sharded(a.bar, gc.epoch, a.status, a.budget_ns);
 }
 
-// Stage strip bi: metadata into lanes, payload/column/row-pointer bytes into
-// shared memory.  PK 0: FP64 canonical payload; PK 1: packed mixed payload.
-template <int PK>
-__device__ __forceinline__ StripMeta stage_strip(const CgArgs &a, StripBuf &sb, int bi, int hl)
+// Offset of tile t's u8 row pointers in Blockcsr_Ptr (csrptr_offset without
+// a memory access: every tile has 16 pointers except those of a short last
+// strip).
+__device__ __forceinline__ long long ptr_off(const CgArgs &a, int t)
 {
+    return (t < a.last_tile_begin) ? 16ll * t
+                                   : 16ll * a.last_tile_begin + (long long)(t - a.last_tile_begin) * a.last_rowlen;
+}
+
+__device__ __forceinline__ void add_range(unsigned char *dst, const unsigned char *src, long long a0, long long a1,
+                                          uint64_t *bar, int &shift)
+{
+    const long long c0 = a0 & ~15ll, c1 = (a1 + 15) & ~15ll;
+    shift = (int)(a0 - c0);
+    if (c1 > c0) bulk_g2s(dst, src + c0, (unsigned)(c1 - c0), bar);
+}
+
+__device__ __forceinline__ unsigned range_bytes(long long a0, long long a1)
+{
+    const long long c0 = a0 & ~15ll, c1 = (a1 + 15) & ~15ll;
+    return (unsigned)(c1 - c0);
+}
+
+// Thread 0: stage chunk c into stage k.
+template <int PK>
+__device__ void issue_chunk(const CgArgs &a, SolverSmem &S, int c, int k)
+{
+    const ChunkRec r = a.chunks[c];
+    StageHdr &h = S.hdr[k];
+    h.rec = r;
+    unsigned char *st = S.stage[k];
     const MfTiles &A = a.A;
-    StripMeta m;
-    m.t0 = A.tile_ptr[bi];
-    const int t1 = A.tile_ptr[bi + 1];
-    m.cnt = t1 - m.t0;
-    m.e0 = A.tile_nnz[m.t0];
-    const int e1 = A.tile_nnz[t1];
-    m.staged = (m.cnt <= STAGE_MAXT) && (e1 - m.e0 <= STAGE_CAPE);
-    m.my_tc = 0;
-    m.my_off = 0;
-    m.my_nz = 0;
-    m.my_pb = 0;
-    m.my_cls = MF_CLASS_FP64;
-    long long pb_abs = 0;
-    if (hl < m.cnt) {
-        const int t = m.t0 + hl;
-        m.my_tc = A.tile_columnidx[t];
-        const int o = A.tile_nnz[t];
-        m.my_off = o - m.e0;
-        m.my_nz = A.tile_nnz[t + 1] - o;
+    // expected bytes first (the barrier counts them down as copies land)
+    unsigned total = range_bytes(4ll * r.s0, 4ll * (r.s1 + 1));
+    if (!r.direct) {
+        total += range_bytes(4ll * r.t0, 4ll * r.t1) + range_bytes(4ll * r.t0, 4ll * (r.t1 + 1));
+        total += range_bytes(ptr_off(a, r.t0), ptr_off(a, r.t1)) + range_bytes(r.e0, r.e1);
         if (PK == 1) {
-            pb_abs = (long long)a.poff[t];
-            m.my_cls = a.wcls[t];
+            total += range_bytes(4ll * r.t0, 4ll * (r.t1 + 1)) + range_bytes(r.t0, r.t1) + range_bytes(r.y0, r.y1);
         } else {
-            pb_abs = 8ll * o;
+            total += range_bytes(8ll * r.e0, 8ll * r.e1);
         }
     }
-    if (!m.staged) return m;
-    long long pbase;
-    if (PK == 1)
-        pbase = stage_range(sb.pay, a.pay, a.poff[m.t0], a.poff[t1], hl);
-    else
-        pbase = stage_range(sb.pay, (const unsigned char *)A.val, 8ll * m.e0, 8ll * e1, hl);
-    m.my_pb = (int)(pb_abs - pbase);
-    const long long cbase = stage_range(sb.col, A.col, m.e0, e1, hl);
-    // keep the column base in my_off (entries are addressed relative to it)
-    m.my_off += (int)(m.e0 - cbase);
-    const int rowlen = (bi == A.tilem - 1) ? A.rows - bi * MF_TILE : MF_TILE;
-    const long long pr0 = A.rows_multiple_of_16 ? 16ll * m.t0 : (long long)A.csrptr_offset[m.t0];
-    const long long pbase2 = stage_range(sb.ptr, A.ptr, pr0, pr0 + (long long)m.cnt * rowlen, hl);
-    // ptr of tile j, row r lives at sb.ptr[pshift + j*rowlen + r]
-    sb.pshift = (int)(pr0 - pbase2);
-    return m;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&S.bar[k], total);
+    add_range(st + OFF_TPTR, (const unsigned char *)A.tile_ptr, 4ll * r.s0, 4ll * (r.s1 + 1), &S.bar[k], h.sh_tptr);
+    if (r.direct) return;
+    add_range(st + OFF_TCOL, (const unsigned char *)A.tile_columnidx, 4ll * r.t0, 4ll * r.t1, &S.bar[k], h.sh_tcol);
+    add_range(st + OFF_TNNZ, (const unsigned char *)A.tile_nnz, 4ll * r.t0, 4ll * (r.t1 + 1), &S.bar[k], h.sh_tnnz);
+    add_range(st + OFF_PTR, A.ptr, ptr_off(a, r.t0), ptr_off(a, r.t1), &S.bar[k], h.sh_ptr);
+    add_range(st + OFF_COL, A.col, r.e0, r.e1, &S.bar[k], h.sh_col);
+    if (PK == 1) {
+        add_range(st + OFF_POFF, (const unsigned char *)a.poff, 4ll * r.t0, 4ll * (r.t1 + 1), &S.bar[k], h.sh_poff);
+        add_range(st + OFF_WCLS, a.wcls, r.t0, r.t1, &S.bar[k], h.sh_wcls);
+        add_range(st + OFF_PAY, a.pay, r.y0, r.y1, &S.bar[k], h.sh_pay);
+    } else {
+        add_range(st + OFF_PAY, (const unsigned char *)A.val, 8ll * r.e0, 8ll * r.e1, &S.bar[k], h.sh_pay);
+    }
 }
 
-// Row r of a staged strip: sum over tiles in column order of the sequential
-// per-tile row sums.  FP64 mode: rounded separately (bit-identical to
-// blockspmv_cpu); mixed: FP32 fused multiply-add accumulation.
+// Row r of strip s from a staged chunk (reference order: tiles in column
+// order, each tile's row entries in order).  FP64 payload: products and sums
+// rounded separately (bit-identical to blockspmv_cpu); packed payload: FP32
+// fused multiply-add accumulation.
 template <int PK>
-__device__ __forceinline__ double staged_row(const StripBuf &sb, const StripMeta &m, int hl, unsigned hmask,
-                                             int rowlen)
+__device__ __forceinline__ double chunk_row(const CgArgs &a, const SolverSmem &S, int k, int s, int r, int rowlen)
 {
+    const StageHdr &h = S.hdr[k];
+    const ChunkRec &rec = h.rec;
+    const unsigned char *st = S.stage[k];
+    const int *tp = (const int *)(st + OFF_TPTR + h.sh_tptr);
+    const int *tn = (const int *)(st + OFF_TNNZ + h.sh_tnnz);
+    const unsigned char *cb = st + OFF_COL + h.sh_col;
+    const unsigned char *pb = st + OFF_PTR + h.sh_ptr;
+    const long long p00 = ptr_off(a, rec.t0);
+    const int ta = tp[s - rec.s0], tb = tp[s - rec.s0 + 1];
     double accd = 0.0;
     float accf = 0.0f;
-    for (int j = 0; j < m.cnt; j++) {
-        const int off = __shfl_sync(hmask, m.my_off, j, 16);
-        const int nz = __shfl_sync(hmask, m.my_nz, j, 16);
-        const int pb = __shfl_sync(hmask, m.my_pb, j, 16);
-        const int cls = __shfl_sync(hmask, m.my_cls, j, 16);
-        if (hl >= rowlen) continue;
-        const int pj = sb.pshift + j * rowlen;
-        const int lo = sb.ptr[pj + hl];
-        const int hi = (hl == rowlen - 1) ? nz : (int)sb.ptr[pj + hl + 1];
-        const double *seg = sb.seg[j];
+    for (int t = ta; t < tb; t++) {
+        const int jl = t - rec.t0;
+        const int off = tn[jl] - rec.e0;
+        const int nz = tn[jl + 1] - tn[jl];
+        const unsigned char *prow = pb + (ptr_off(a, t) - p00);
+        const int lo = prow[r];
+        const int hi = (r == rowlen - 1) ? nz : (int)prow[r + 1];
+        const double *seg = S.seg + jl * MF_TILE;
+        const unsigned char *cl = cb + off;
         if (PK == 0) {
-            const double *v = (const double *)(sb.pay + pb);
-            double s = 0.0;
-            for (int k = lo; k < hi; k++) s = __dadd_rn(s, __dmul_rn(seg[sb.col[off + k]], v[k]));
-            accd = __dadd_rn(accd, s);
+            const double *v = (const double *)(st + OFF_PAY + h.sh_pay) + off;
+            double sm = 0.0;
+            for (int q = lo; q < hi; q++) sm = __dadd_rn(sm, __dmul_rn(seg[cl[q]], v[q]));
+            accd = __dadd_rn(accd, sm);
         } else {
-            float s = 0.0f;
+            const unsigned *po = (const unsigned *)(st + OFF_POFF + h.sh_poff);
+            const int cls = (st + OFF_WCLS + h.sh_wcls)[jl];
+            const unsigned char *vb = st + OFF_PAY + h.sh_pay + (po[jl] - rec.y0);
+            float sm = 0.0f;
             if (cls == MF_CLASS_FP32 || cls == MF_CLASS_FP64) {
-                const float *v = (const float *)(sb.pay + pb);
-                for (int k = lo; k < hi; k++) s = fmaf(v[k], (float)seg[sb.col[off + k]], s);
+                const float *v = (const float *)vb;
+                for (int q = lo; q < hi; q++) sm = fmaf(v[q], (float)seg[cl[q]], sm);
             } else if (cls == MF_CLASS_FP16) {
-                const __half *v = (const __half *)(sb.pay + pb);
-                for (int k = lo; k < hi; k++) s = fmaf(__half2float(v[k]), (float)seg[sb.col[off + k]], s);
+                const __half *v = (const __half *)vb;
+                for (int q = lo; q < hi; q++) sm = fmaf(__half2float(v[q]), (float)seg[cl[q]], sm);
             } else if (cls == MF_CLASS_INT8) {
-                const int8_t *v = (const int8_t *)(sb.pay + pb);
-                for (int k = lo; k < hi; k++) s = fmaf((float)v[k], (float)seg[sb.col[off + k]], s);
+                const int8_t *v = (const int8_t *)vb;
+                for (int q = lo; q < hi; q++) sm = fmaf((float)v[q], (float)seg[cl[q]], sm);
             }
-            accf += s;
+            accf += sm;
         }
     }
     return PK == 0 ? accd : (double)accf;
 }
 
-// Direct (unstaged) row for strips above the staging caps; same order.
+// Row r of strip s straight from global memory (chunks flagged direct).
 template <int PK, class Src>
-__device__ __forceinline__ double direct_row(const CgArgs &a, int bi, int r, int rowlen, Src src)
+__device__ double direct_row(const CgArgs &a, int s, int r, int rowlen, Src src)
 {
     const MfTiles &A = a.A;
-    const int t0 = A.tile_ptr[bi], t1 = A.tile_ptr[bi + 1];
+    const int t0 = A.tile_ptr[s], t1 = A.tile_ptr[s + 1];
     double accd = 0.0;
     float accf = 0.0f;
     for (int t = t0; t < t1; t++) {
         const int off = A.tile_nnz[t], nz = A.tile_nnz[t + 1] - off;
         const int xo = A.tile_columnidx[t] * MF_TILE;
-        const int po = A.rows_multiple_of_16 ? t * MF_TILE : A.csrptr_offset[t];
+        const long long po = ptr_off(a, t);
         const int lo = A.ptr[po + r];
         const int hi = (r == rowlen - 1) ? nz : (int)A.ptr[po + r + 1];
         if (PK == 0) {
-            double s = 0.0;
-            for (int k = lo; k < hi; k++) s = __dadd_rn(s, __dmul_rn((double)src(xo + A.col[off + k]), A.val[off + k]));
-            accd = __dadd_rn(accd, s);
+            double sm = 0.0;
+            for (int q = lo; q < hi; q++)
+                sm = __dadd_rn(sm, __dmul_rn((double)src(xo + A.col[off + q]), A.val[off + q]));
+            accd = __dadd_rn(accd, sm);
         } else {
             const int cls = a.wcls[t];
-            const unsigned char *pb = a.pay + a.poff[t];
-            float s = 0.0f;
-            for (int k = lo; k < hi; k++) {
-                float v = 0.0f;
-                if (cls == MF_CLASS_FP32 || cls == MF_CLASS_FP64) v = ((const float *)pb)[k];
-                else if (cls == MF_CLASS_FP16) v = __half2float(((const __half *)pb)[k]);
-                else if (cls == MF_CLASS_INT8) v = (float)((const int8_t *)pb)[k];
+            const unsigned char *vb = a.pay + a.poff[t];
+            float sm = 0.0f;
+            for (int q = lo; q < hi; q++) {
+                float v;
+                if (cls == MF_CLASS_FP32 || cls == MF_CLASS_FP64) v = ((const float *)vb)[q];
+                else if (cls == MF_CLASS_FP16) v = __half2float(((const __half *)vb)[q]);
+                else if (cls == MF_CLASS_INT8) v = (float)((const int8_t *)vb)[q];
                 else break;
-                s = fmaf(v, (float)src(xo + A.col[off + k]), s);
+                sm = fmaf(v, (float)src(xo + A.col[off + q]), sm);
             }
-            accf += s;
+            accf += sm;
         }
     }
     return PK == 0 ? accd : (double)accf;
 }
 
-// One strip's 16 rows of y = A src (src: functor giving the x value of a
-// column).  Returns row hl's value (0 for lanes past rowlen).
-template <int PK, class Src>
-__device__ __forceinline__ double strip_product(const CgArgs &a, StripBuf &sb, int bi, int hl, unsigned hmask,
-                                                Src src)
+// y = A src over this CTA's chunks [cb, ce); out(s, r, y) receives every row.
+// Returns false when a bounded wait expired (status set).
+template <int PK, class Src, class Out>
+__device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb, int ce, Src src, Out &out)
 {
     const MfTiles &A = a.A;
-    const int rowlen = (bi == A.tilem - 1) ? A.rows - bi * MF_TILE : MF_TILE;
-    StripMeta m = stage_strip<PK>(a, sb, bi, hl);
-    if (!m.staged) {
-        __syncwarp(hmask);
-        return (hl < rowlen) ? direct_row<PK>(a, bi, hl, rowlen, src) : 0.0;
+    const int tid = threadIdx.x, hw = tid >> 4, hl = tid & 15;
+    if (tid == 0) {
+        if (cb < ce) issue_chunk<PK>(a, S, cb, 0);
+        if (cb + 1 < ce) issue_chunk<PK>(a, S, cb + 1, 1);
     }
-    // x segments: lane hl computes element hl of every tile's 16-column segment
-    for (int j = 0; j < m.cnt; j++) {
-        const int tc = __shfl_sync(hmask, m.my_tc, j, 16);
-        const int c = tc * MF_TILE + hl;
-        sb.seg[j][hl] = (c < A.cols) ? (double)src(c) : 0.0;
+    __syncthreads();
+    bool ok = true;
+    for (int c = cb; c < ce; c++) {
+        const int k = (c - cb) & 1;
+        if (!mbar_wait_bounded(&S.bar[k], gc.use[k] & 1u, a.status, a.budget_ns)) {
+            ok = false;
+            // the other stage may still have a copy in flight: wait for it
+            // (bounded) before leaving so no copy lands in freed memory
+            if (c + 1 < ce) mbar_wait_bounded(&S.bar[k ^ 1], gc.use[k ^ 1] & 1u, a.status, a.budget_ns);
+            break;
+        }
+        gc.use[k]++;
+        const ChunkRec &rec = S.hdr[k].rec;
+        if (rec.direct) {
+            const int s = rec.s0;
+            const int rowlen = (s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE;
+            if (hw == 0 && hl < rowlen) out(s, hl, direct_row<PK>(a, s, hl, rowlen, src));
+        } else {
+            const int nt = rec.t1 - rec.t0;
+            const int *tc = (const int *)(S.stage[k] + OFF_TCOL + S.hdr[k].sh_tcol);
+            for (int v = tid; v < nt * MF_TILE; v += NT) {
+                const int col = tc[v >> 4] * MF_TILE + (v & 15);
+                S.seg[v] = (col < A.cols) ? (double)src(col) : 0.0;
+            }
+            __syncthreads();
+            const int s = rec.s0 + hw;
+            if (s < rec.s1) {
+                const int rowlen = (s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE;
+                if (hl < rowlen) out(s, hl, chunk_row<PK>(a, S, k, s, hl, rowlen));
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && c + 2 < ce) issue_chunk<PK>(a, S, c + 2, k);
     }
-    cp_async_wait_all();
-    __syncwarp(hmask);
-    const double y = staged_row<PK>(sb, m, hl, hmask, rowlen);
-    __syncwarp(hmask);
-    return y;
+    return ok;
 }
 
 template <bool MIX>
-__global__ void __launch_bounds__(NT, 4) k_cg(CgArgs a)
+__global__ void __launch_bounds__(NT, 3) k_cg(CgArgs a)
 {
     using VT = typename VecT<MIX>::T;
+    constexpr int PK = MIX ? 1 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double s_warp[NT / 32];
-    __shared__ double s_res;
-    StripBuf *bufs = (StripBuf *)smem_raw;
+    SolverSmem &S = *reinterpret_cast<SolverSmem *>(smem_raw);
     const MfTiles &A = a.A;
-    const int sb0 = a.part[blockIdx.x], se0 = a.part[blockIdx.x + 1];
-    const int lane = threadIdx.x & 31, hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
-    const unsigned hmask = (lane < 16) ? 0x0000ffffu : 0xffff0000u;
-    StripBuf &sb = bufs[hw];
-    const int hstep = NT / MF_TILE;
+    const int g = blockIdx.x;
+    const int sb0 = a.part[g], se0 = a.part[g + 1];
+    const int cb = a.cta_chunk[g], ce = a.cta_chunk[g + 1];
+    const int row0 = sb0 * MF_TILE, row1 = min(se0 * MF_TILE, A.rows);
     VT *r = (VT *)a.r, *q = (VT *)a.q, *xlo = (VT *)a.xlo;
-    GridCtx gc{0ull, true};
+    GridCtx gc;
+    gc.epoch = 0;
+    gc.ok = true;
+    gc.use[0] = gc.use[1] = 0;
     double *st = a.state;
+    if (threadIdx.x == 0) {
+        mbar_init(&S.bar[0], 1);
+        mbar_init(&S.bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
 
     double rho, beta, nb, rmax;
     int it, refs;
     if (a.start) {
         double lb = 0.0, lr = 0.0;
-        for (int bi = sb0 + hw; bi < se0; bi += hstep) {
-            const int rowlen = (bi == A.tilem - 1) ? A.rows - bi * MF_TILE : MF_TILE;
-            if (hl < rowlen) {
-                const int i = bi * MF_TILE + hl;
-                const double bv = a.b[i];
-                const VT rv = (VT)bv;
-                a.xhi[i] = 0.0;
-                r[i] = rv;
-                ((VT *)a.p0)[i] = (VT)0;
-                if (MIX) xlo[i] = (VT)0;
-                lb = __dadd_rn(lb, __dmul_rn(bv, bv));
-                lr = __dadd_rn(lr, __dmul_rn((double)rv, (double)rv));
-            }
+        for (int i = row0 + threadIdx.x; i < row1; i += NT) {
+            const double bv = a.b[i];
+            const VT rv = (VT)bv;
+            a.xhi[i] = 0.0;
+            r[i] = rv;
+            ((VT *)a.p0)[i] = (VT)0;
+            if (MIX) xlo[i] = (VT)0;
+            lb = __dadd_rn(lb, __dmul_rn(bv, bv));
+            lr = __dadd_rn(lr, __dmul_rn((double)rv, (double)rv));
         }
-        const double bb = grid_sum(a, lb, 0, gc, s_warp, &s_res);
-        rho = MIX ? grid_sum(a, lr, 1, gc, s_warp, &s_res) : bb;
+        const double bb = grid_sum(a, lb, 0, gc, S);
+        rho = MIX ? grid_sum(a, lr, 1, gc, S) : bb;
         nb = sqrt(bb) > 0.0 ? sqrt(bb) : 1.0;
         beta = 0.0;
         rmax = sqrt(rho);
         it = 0;
         refs = 0;
-        if (a.hist && blockIdx.x == 0 && threadIdx.x == 0) a.hist[0] = sqrt(bb) / nb;
+        if (a.hist && g == 0 && threadIdx.x == 0) a.hist[0] = sqrt(bb) / nb;
     } else {
         rho = st[S_RHO];
         beta = st[S_BETA];
@@ -278,7 +362,6 @@ __global__ void __launch_bounds__(NT, 4) k_cg(CgArgs a)
     }
     int exit_reason = EXIT_MAXITER;
     double relres_true = sqrt(rho) / nb;
-    // optional phase timers (thread 0 of each CTA)
     unsigned long long tph[5] = {0, 0, 0, 0, 0}, tmark = 0;
     const bool timed = a.timing != nullptr && threadIdx.x == 0;
 #define MF_MARK(k)                                        \
@@ -287,7 +370,6 @@ __global__ void __launch_bounds__(NT, 4) k_cg(CgArgs a)
         if ((k) >= 0) tph[(k)] += now_ - tmark;           \
         tmark = now_;                                     \
     }
-    bool converged_check = false;
     while (gc.ok) {
         if (!a.fixed && sqrt(rho) <= a.tol * nb) {
             exit_reason = EXIT_CONVERGED;
@@ -300,87 +382,76 @@ __global__ void __launch_bounds__(NT, 4) k_cg(CgArgs a)
         const VT *pold = (const VT *)((it & 1) ? a.p1 : a.p0);
         VT *pnew = (VT *)((it & 1) ? a.p0 : a.p1);
         const VT bt = (VT)beta;
-        MF_MARK(-1);
-        // ---- q = A p_new with p_new = r + beta p_old formed on the fly ----
-        double loc = 0.0;
+        const VT *rr = r;
         auto psrc = [=](int c) -> VT {
-            if constexpr (MIX) return fmaf(bt, pold[c], r[c]);
-            else return fma(bt, pold[c], r[c]);
+            if constexpr (MIX) return fmaf(bt, pold[c], rr[c]);
+            else return fma(bt, pold[c], rr[c]);
         };
-        for (int bi = sb0 + hw; bi < se0; bi += hstep) {
-            const double y = strip_product<MIX ? 1 : 0>(a, sb, bi, hl, hmask, psrc);
-            const int rowlen = (bi == A.tilem - 1) ? A.rows - bi * MF_TILE : MF_TILE;
-            if (hl < rowlen) {
-                const int i = bi * MF_TILE + hl;
-                const VT pn = psrc(i);
-                const VT qi = (VT)y;
-                pnew[i] = pn;
-                q[i] = qi;
-                loc = __dadd_rn(loc, __dmul_rn((double)pn, (double)qi));
-            }
-        }
+        MF_MARK(-1);
+        // ---- q = A p_new, p_new = r + beta p_old formed on the fly ----
+        double loc = 0.0;
+        auto aout = [&](int s, int rw, double y) {
+            const int i = s * MF_TILE + rw;
+            const VT pn = psrc(i);
+            const VT qi = (VT)y;
+            pnew[i] = pn;
+            q[i] = qi;
+            loc = __dadd_rn(loc, __dmul_rn((double)pn, (double)qi));
+        };
+        if (!spmv_chunks<PK>(a, S, gc, cb, ce, psrc, aout)) gc.ok = false;
         MF_MARK(0);
-        const double pq = grid_sum(a, loc, 2, gc, s_warp, &s_res);
+        const double pq = grid_sum(a, loc, 2, gc, S);
         MF_MARK(1);
         if (!gc.ok) break;
         if (!(pq != 0.0) || !isfinite(pq)) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(a.status, DEV_OK, DEV_BREAKDOWN);
+            if (g == 0 && threadIdx.x == 0) atomicCAS(a.status, DEV_OK, DEV_BREAKDOWN);
             exit_reason = EXIT_BREAKDOWN;
             break;
         }
         const double alpha = rho / pq;
-        // ---- x += alpha p, r -= alpha q ----
+        // ---- x += alpha p, r -= alpha q over this CTA's rows ----
         loc = 0.0;
-        for (int bi = sb0 + hw; bi < se0; bi += hstep) {
-            const int rowlen = (bi == A.tilem - 1) ? A.rows - bi * MF_TILE : MF_TILE;
-            if (hl < rowlen) {
-                const int i = bi * MF_TILE + hl;
-                if (MIX) {
-                    xlo[i] = fmaf((float)alpha, (float)pnew[i], (float)xlo[i]);
-                    const float ri = fmaf(-(float)alpha, (float)q[i], (float)r[i]);
-                    r[i] = ri;
-                    loc = __dadd_rn(loc, __dmul_rn((double)ri, (double)ri));
-                } else {
-                    a.xhi[i] = fma(alpha, (double)pnew[i], a.xhi[i]);
-                    const double ri = fma(-alpha, (double)q[i], (double)r[i]);
-                    r[i] = ri;
-                    loc = __dadd_rn(loc, __dmul_rn(ri, ri));
-                }
+        if (MIX) {
+            const float af = (float)alpha;
+            for (int i = row0 + threadIdx.x; i < row1; i += NT) {
+                xlo[i] = fmaf(af, (float)pnew[i], (float)xlo[i]);
+                const float ri = fmaf(-af, (float)q[i], (float)r[i]);
+                r[i] = ri;
+                loc = __dadd_rn(loc, __dmul_rn((double)ri, (double)ri));
+            }
+        } else {
+            for (int i = row0 + threadIdx.x; i < row1; i += NT) {
+                a.xhi[i] = fma(alpha, (double)pnew[i], a.xhi[i]);
+                const double ri = fma(-alpha, (double)q[i], (double)r[i]);
+                r[i] = ri;
+                loc = __dadd_rn(loc, __dmul_rn(ri, ri));
             }
         }
         MF_MARK(2);
-        double rho_new = grid_sum(a, loc, 3, gc, s_warp, &s_res);
+        double rho_new = grid_sum(a, loc, 3, gc, S);
         MF_MARK(3);
         if (!gc.ok) break;
         it++;
         bool refined = false;
         if (MIX && (sqrt(rho_new) <= a.delta * rmax || (!a.fixed && sqrt(rho_new) <= a.tol * nb))) {
             // ---- reliable update: x_hi += x_lo; r = b - A x_hi in FP64 ----
-            for (int bi = sb0 + hw; bi < se0; bi += hstep) {
-                const int rowlen = (bi == A.tilem - 1) ? A.rows - bi * MF_TILE : MF_TILE;
-                if (hl < rowlen) {
-                    const int i = bi * MF_TILE + hl;
-                    a.xhi[i] = a.xhi[i] + (double)xlo[i];
-                    xlo[i] = (VT)0;
-                }
+            for (int i = row0 + threadIdx.x; i < row1; i += NT) {
+                a.xhi[i] = a.xhi[i] + (double)xlo[i];
+                xlo[i] = (VT)0;
             }
             grid_sync(a, gc);
             if (!gc.ok) break;
             loc = 0.0;
             const double *xh = a.xhi;
             auto xsrc = [=](int c) -> double { return xh[c]; };
-            for (int bi = sb0 + hw; bi < se0; bi += hstep) {
-                const double y = strip_product<0>(a, sb, bi, hl, hmask, xsrc);
-                const int rowlen = (bi == A.tilem - 1) ? A.rows - bi * MF_TILE : MF_TILE;
-                if (hl < rowlen) {
-                    const int i = bi * MF_TILE + hl;
-                    const double rt = a.b[i] - y;
-                    const VT rv = (VT)rt;
-                    r[i] = rv;
-                    loc = __dadd_rn(loc, __dmul_rn((double)rv, (double)rv));
-                }
-            }
-            rho_new = grid_sum(a, loc, 1, gc, s_warp, &s_res);
+            auto rout = [&](int s, int rw, double y) {
+                const int i = s * MF_TILE + rw;
+                const VT rv = (VT)(a.b[i] - y);
+                r[i] = rv;
+                loc = __dadd_rn(loc, __dmul_rn((double)rv, (double)rv));
+            };
+            if (!spmv_chunks<0>(a, S, gc, cb, ce, xsrc, rout)) gc.ok = false;
+            rho_new = grid_sum(a, loc, 1, gc, S);
             if (!gc.ok) break;
             rmax = sqrt(rho_new);
             relres_true = sqrt(rho_new) / nb;
@@ -391,29 +462,23 @@ __global__ void __launch_bounds__(NT, 4) k_cg(CgArgs a)
         beta = rho_new / rho;
         rho = rho_new;
         if (!MIX) relres_true = sqrt(rho) / nb;
-        if (a.hist && blockIdx.x == 0 && threadIdx.x == 0) a.hist[it] = sqrt(rho) / nb;
+        if (a.hist && g == 0 && threadIdx.x == 0) a.hist[it] = sqrt(rho) / nb;
         if (refined && a.exit_on_refine) {
             exit_reason = EXIT_CHECKPOINT;
-            converged_check = true;
             break;
         }
     }
-    (void)converged_check;
+#undef MF_MARK
     if (MIX && exit_reason != EXIT_CONVERGED && exit_reason != EXIT_CHECKPOINT && gc.ok) {
         // leaving with an unflushed FP32 correction: fold it into x
-        for (int bi = sb0 + hw; bi < se0; bi += hstep) {
-            const int rowlen = (bi == A.tilem - 1) ? A.rows - bi * MF_TILE : MF_TILE;
-            if (hl < rowlen) {
-                const int i = bi * MF_TILE + hl;
-                a.xhi[i] = a.xhi[i] + (double)xlo[i];
-                xlo[i] = (VT)0;
-            }
+        for (int i = row0 + threadIdx.x; i < row1; i += NT) {
+            a.xhi[i] = a.xhi[i] + (double)xlo[i];
+            xlo[i] = (VT)0;
         }
     }
-#undef MF_MARK
     if (timed)
-        for (int k = 0; k < 5; k++) a.timing[blockIdx.x * 8 + k] += tph[k];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int k = 0; k < 5; k++) a.timing[g * 8 + k] += tph[k];
+    if (g == 0 && threadIdx.x == 0) {
         st[S_RHO] = rho;
         st[S_BETA] = beta;
         st[S_NB] = nb;
@@ -469,7 +534,7 @@ int max_ctas_for()
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const size_t dyn = sizeof(StripBuf) * (NT / MF_TILE);
+        const size_t dyn = sizeof(SolverSmem);
         cudaFuncSetAttribute(k_cg<MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg<MIX>, NT, dyn);
         cached = sms * (per > 0 ? per : 1);
@@ -496,7 +561,7 @@ mf_status solver_resources(mf_matrix m, int G, SolverWork &w)
     const size_t o_out = off; off += align256(8 * 8);
     const size_t o_state = off; off += align256(32 * 8);
     const size_t o_tim = off; off += align256((size_t)G * 8 * 8);
-    const size_t o_bar = off; off += align256(8);
+    const size_t o_bar = off; off += align256(9 * 128);
     const size_t o_st = off; off += align256(8);
     MF_TRY(ensure_work(m, off));
     char *base = (char *)m->work;
@@ -523,7 +588,7 @@ int solver_grid(mf_matrix m, bool mixed)
         const int v = atoi(e);
         if (v > 0 && v < maxc) maxc = v;
     }
-    int want = ceil_div(m->v.tilem, NT / MF_TILE);
+    int want = ceil_div(m->v.tilem, CH_STRIPS);
     if (want < 1) want = 1;
     return want < maxc ? want : maxc;
 }
@@ -548,7 +613,7 @@ mf_status true_residual(mf_matrix m, const double *b, const double *x, SolverWor
 
 mf_status launch_cg(bool mixed, CgArgs &a, int G, cudaStream_t s)
 {
-    const size_t dyn = sizeof(StripBuf) * (NT / MF_TILE);
+    const size_t dyn = sizeof(SolverSmem);
     void *args[] = {&a};
     note_launch();
     if (mixed) {

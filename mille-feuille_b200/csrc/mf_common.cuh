@@ -94,6 +94,48 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long *counter, unsign
     return s_ok != 0;
 }
 
+// Grid-wide barrier with sharded arrival: CTA g arrives on sub-counter
+// g % 8 (each on its own 128-byte line); the last arrival of a group bumps
+// the top counter, on which every CTA spins.  ctr points at 9 lines
+// (ctr[0], ctr[16], ..., ctr[128]), zeroed before the launch.  `epoch` is
+// the 1-based count of barriers this launch has passed.
+__device__ __forceinline__ bool grid_barrier_sharded(unsigned long long *ctr, unsigned long long epoch, int *status,
+                                                     unsigned long long budget_ns)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned G = gridDim.x;
+        const unsigned sub = blockIdx.x & 7u;
+        const unsigned long long gsize = (G - sub + 7u) / 8u;
+        const unsigned long long ng = G < 8u ? G : 8u;
+        __threadfence();
+        const unsigned long long old = atomicAdd(ctr + 16 * sub, 1ull);
+        if (old + 1ull == epoch * gsize) {
+            __threadfence();
+            atomicAdd(ctr + 128, 1ull);
+        }
+        unsigned long long t0 = globaltimer_ns();
+        unsigned spins = 0;
+        while (ld_acquire_u64(ctr + 128) < epoch * ng) {
+            if (((++spins) & 63u) == 0u) {
+                if (ld_volatile_i32(status) != DEV_OK) { ok = 0; break; }
+                if (globaltimer_ns() - t0 > budget_ns) {
+                    atomicCAS(status, DEV_OK, DEV_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        if (ld_volatile_i32(status) != DEV_OK) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 // Deterministic CTA reduction of one double per thread: warp butterfly, then
 // the warp results summed in warp order.  All threads get the result.
 template <int NT>

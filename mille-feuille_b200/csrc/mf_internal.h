@@ -31,6 +31,7 @@ struct mf_matrix_s {
     int max_tile_nnz;
     int class_tiles[5];
     int nonzero_rows;          // cnt_non_new
+    int last_tile_begin;       // tile_ptr[tilem-1]
     int rowblkblock;
     size_t device_bytes;
 
@@ -52,6 +53,9 @@ struct mf_matrix_s {
     // strip partitions for the persistent kernels, cached per CTA count
     int part_ctas = 0;
     int *d_part = nullptr;     // [part_ctas+1] strip boundaries
+    int *d_cta_chunk = nullptr;  // [part_ctas+1] chunk ranges
+    void *d_chunks = nullptr;    // chunk records
+    int nchunks = 0;
     // cached per-matrix solver workspace
     void *work = nullptr;
     size_t work_bytes = 0;

@@ -14,7 +14,11 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
 {
     const bool mixed = o.policy != MF_POLICY_FP64;
     const int G = solver_grid(m, mixed);
-    MF_TRY(strip_partition(m, G, s));
+    if (m->part_ctas != G || !m->d_chunks) {
+        MF_TRY(strip_partition(m, G, s));
+        MF_TRY(build_chunks(m, s));
+        m->packed_policy = -1;  // chunk payload offsets must be refreshed
+    }
     SolverWork w;
     MF_TRY(solver_resources(m, G, w));
     const int T = m->v.tilenum;
@@ -23,6 +27,7 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
         if (m->packed_policy != MF_POLICY_STATIC) {
             MF_TRY(static_working_classes(m, m->d_wcls, s));
             MF_TRY(pack_payload(m, m->d_wcls, s));
+            MF_TRY(refresh_chunk_payload(m, s));
             m->packed_policy = MF_POLICY_STATIC;
         }
     }
@@ -30,6 +35,10 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
     memset(&a, 0, sizeof(a));
     a.A = m->v;
     a.part = m->d_part;
+    a.cta_chunk = m->d_cta_chunk;
+    a.chunks = (const ChunkRec *)m->d_chunks;
+    a.last_tile_begin = m->last_tile_begin;
+    a.last_rowlen = m->v.rows - (m->v.tilem - 1) * MF_TILE;
     a.pay = m->d_pay;
     a.poff = m->d_poff;
     a.wcls = m->d_wcls;
@@ -62,7 +71,7 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
     double st[S_COUNT];
     int h_status = 0, launches = 0;
     for (;;) {
-        MF_CUDA(cudaMemsetAsync(w.bar, 0, sizeof(unsigned long long), s));
+        MF_CUDA(cudaMemsetAsync(w.bar, 0, 9 * 128, s));
         MF_TRY(launch_cg(mixed, a, G, s));
         launches++;
         if (!a.exit_on_refine) break;
@@ -81,6 +90,7 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
             MF_TRY(learned_working_classes(m, w, pnew, pold, m->d_wcls, s));
         }
         MF_TRY(pack_payload(m, m->d_wcls, s));
+        MF_TRY(refresh_chunk_payload(m, s));
         m->packed_policy = o.policy;
         a.start = 0;
     }

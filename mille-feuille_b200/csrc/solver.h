@@ -4,6 +4,22 @@
 
 namespace mf {
 
+// A chunk: up to CH_STRIPS consecutive strips of one CTA whose tiles,
+// entries and bytes fit one shared-memory stage.  A strip too large for a
+// stage on its own is a one-strip chunk with `direct` set (computed from
+// global memory).
+constexpr int CH_STRIPS = 16;
+constexpr int CH_TILES = 128;
+constexpr int CH_ENTRIES = 2048;
+struct ChunkRec {
+    int s0, s1;       // strips [s0, s1)
+    int t0, t1;       // tiles [t0, t1)
+    int e0, e1;       // entries [e0, e1)
+    unsigned y0, y1;  // packed payload bytes [y0, y1) (mixed)
+    int direct;
+    int pad;
+};
+
 // Persistent solver state kept in device memory between launches.
 enum : int { S_RHO = 0, S_BETA, S_NB, S_RMAX, S_ITERS, S_REFS, S_EXIT, S_RELRES, S_COUNT };
 // Why a launch returned.
@@ -12,6 +28,8 @@ enum : int { EXIT_CONVERGED = 1, EXIT_MAXITER = 2, EXIT_BREAKDOWN = 3, EXIT_CHEC
 struct CgArgs {
     MfTiles A;
     const int *part;               // [G+1] strip range of each CTA
+    const int *cta_chunk;          // [G+1] chunk range of each CTA
+    const ChunkRec *chunks;
     const unsigned char *pay;      // mixed: packed per-tile payload bytes
     const unsigned *poff;          // mixed: [T+1] byte offset of each tile's payload
     const unsigned char *wcls;     // mixed: [T] working class of each tile
@@ -19,7 +37,7 @@ struct CgArgs {
     double *xhi;                   // solution (FP64)
     void *r, *p0, *p1, *q, *xlo;   // vectors (FP64, or FP32 when mixed)
     double *partials;              // [4][G] per-CTA dot partials
-    unsigned long long *bar;       // grid barrier counter (0 at launch)
+    unsigned long long *bar;       // sharded grid barrier counters (9 lines, 0 at launch)
     int *status;                   // device status word (mf_status codes)
     double *state;                 // [S_COUNT]
     double *hist;                  // optional per-iteration ||r||/||b||
@@ -31,6 +49,8 @@ struct CgArgs {
     unsigned long long budget_ns;  // bound of every grid-wide wait
     int start;                     // 1: initialise x, r, p and the state
     unsigned long long *timing;    // optional [G][8] per-CTA phase nanoseconds
+    int last_tile_begin;           // first tile of the last strip
+    int last_rowlen;               // rows of the last strip
 };
 
 struct SolverWork {
@@ -42,6 +62,9 @@ struct SolverWork {
 };
 
 mf_status solver_resources(mf_matrix m, int G, SolverWork &w);
+// chunks.cu: chunk table for the current partition; payload offsets refresh
+mf_status build_chunks(mf_matrix m, cudaStream_t s);
+mf_status refresh_chunk_payload(mf_matrix m, cudaStream_t s);
 int solver_grid(mf_matrix m, bool mixed);
 mf_status launch_cg(bool mixed, CgArgs &a, int G, cudaStream_t s);
 mf_status true_residual(mf_matrix m, const double *b, const double *x, SolverWork &w, double *relres, cudaStream_t s);

@@ -574,6 +574,7 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
     for (int c = 0; c < 5; c++) m->class_tiles[c] = host_counts[1 + c];
     m->max_tile_nnz = host_counts[6];
     m->nonzero_rows = cnt_non;
+    m->last_tile_begin = last_begin;
     m->rowblkblock = rbb;
     m->device_bytes = acc;
     return MF_OK;

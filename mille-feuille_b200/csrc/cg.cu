@@ -172,7 +172,8 @@ __device__ void issue_chunk(const CgArgs &a, SolverSmem &S, int c, int k)
 // rounded separately (bit-identical to blockspmv_cpu); packed payload: FP32
 // fused multiply-add accumulation.
 template <int PK>
-__device__ __forceinline__ double chunk_row(const CgArgs &a, const SolverSmem &S, int k, int s, int r, int rowlen)
+__device__ __forceinline__ double chunk_row(const CgArgs &a, const SolverSmem &S, int k, int s, int r, int rowlen,
+                                            double &xown, bool &has_own)
 {
     const StageHdr &h = S.hdr[k];
     const ChunkRec &rec = h.rec;
@@ -182,11 +183,17 @@ __device__ __forceinline__ double chunk_row(const CgArgs &a, const SolverSmem &S
     const unsigned char *cb = st + OFF_COL + h.sh_col;
     const unsigned char *pb = st + OFF_PTR + h.sh_ptr;
     const long long p00 = ptr_off(a, rec.t0);
+    const int *tcl = (const int *)(st + OFF_TCOL + h.sh_tcol);
     const int ta = tp[s - rec.s0], tb = tp[s - rec.s0 + 1];
     double accd = 0.0;
     float accf = 0.0f;
+    has_own = false;
     for (int t = ta; t < tb; t++) {
         const int jl = t - rec.t0;
+        if (tcl[jl] == s) {  // diagonal tile: its segment holds this row's x value
+            xown = S.seg[jl * MF_TILE + r];
+            has_own = true;
+        }
         const int off = tn[jl] - rec.e0;
         const int nz = tn[jl + 1] - tn[jl];
         const unsigned char *prow = pb + (ptr_off(a, t) - p00);
@@ -284,19 +291,34 @@ __device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb,
         if (rec.direct) {
             const int s = rec.s0;
             const int rowlen = (s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE;
-            if (hw == 0 && hl < rowlen) out(s, hl, direct_row<PK>(a, s, hl, rowlen, src));
+            if (hw == 0 && hl < rowlen) out(s, hl, direct_row<PK>(a, s, hl, rowlen, src), 0.0, false);
         } else {
             const int nt = rec.t1 - rec.t0;
             const int *tc = (const int *)(S.stage[k] + OFF_TCOL + S.hdr[k].sh_tcol);
-            for (int v = tid; v < nt * MF_TILE; v += NT) {
-                const int col = tc[v >> 4] * MF_TILE + (v & 15);
-                S.seg[v] = (col < A.cols) ? (double)src(col) : 0.0;
+            // x segments: all of a thread's gathers issued before any is used
+            constexpr int SEGV = CH_TILES * MF_TILE / NT;
+            decltype(src(0)) sv[SEGV];
+#pragma unroll
+            for (int u = 0; u < SEGV; u++) {
+                const int v = tid + u * NT;
+                const int col = (v < nt * MF_TILE) ? tc[v >> 4] * MF_TILE + (v & 15) : A.cols;
+                sv[u] = (col < A.cols) ? src(col) : (decltype(src(0)))0;
+            }
+#pragma unroll
+            for (int u = 0; u < SEGV; u++) {
+                const int v = tid + u * NT;
+                if (v < nt * MF_TILE) S.seg[v] = (double)sv[u];
             }
             __syncthreads();
             const int s = rec.s0 + hw;
             if (s < rec.s1) {
                 const int rowlen = (s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE;
-                if (hl < rowlen) out(s, hl, chunk_row<PK>(a, S, k, s, hl, rowlen));
+                if (hl < rowlen) {
+                    double xown = 0.0;
+                    bool has_own = false;
+                    const double y = chunk_row<PK>(a, S, k, s, hl, rowlen, xown, has_own);
+                    out(s, hl, y, xown, has_own);
+                }
             }
         }
         __syncthreads();
@@ -390,9 +412,9 @@ __global__ void __launch_bounds__(NT, 3) k_cg(CgArgs a)
         MF_MARK(-1);
         // ---- q = A p_new, p_new = r + beta p_old formed on the fly ----
         double loc = 0.0;
-        auto aout = [&](int s, int rw, double y) {
+        auto aout = [&](int s, int rw, double y, double xown, bool has_own) {
             const int i = s * MF_TILE + rw;
-            const VT pn = psrc(i);
+            const VT pn = has_own ? (VT)xown : psrc(i);
             const VT qi = (VT)y;
             pnew[i] = pn;
             q[i] = qi;
@@ -411,20 +433,36 @@ __global__ void __launch_bounds__(NT, 3) k_cg(CgArgs a)
         const double alpha = rho / pq;
         // ---- x += alpha p, r -= alpha q over this CTA's rows ----
         loc = 0.0;
-        if (MIX) {
-            const float af = (float)alpha;
-            for (int i = row0 + threadIdx.x; i < row1; i += NT) {
-                xlo[i] = fmaf(af, (float)pnew[i], (float)xlo[i]);
-                const float ri = fmaf(-af, (float)q[i], (float)r[i]);
-                r[i] = ri;
-                loc = __dadd_rn(loc, __dmul_rn((double)ri, (double)ri));
-            }
-        } else {
-            for (int i = row0 + threadIdx.x; i < row1; i += NT) {
-                a.xhi[i] = fma(alpha, (double)pnew[i], a.xhi[i]);
-                const double ri = fma(-alpha, (double)q[i], (double)r[i]);
-                r[i] = ri;
-                loc = __dadd_rn(loc, __dmul_rn(ri, ri));
+        {
+            constexpr int U = 4;
+            for (int i0 = row0 + threadIdx.x; i0 < row1; i0 += NT * U) {
+                VT xv[U], pv[U], qv[U], rv[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int i = i0 + u * NT;
+                    const bool in = i < row1;
+                    xv[u] = in ? (MIX ? (VT)xlo[i] : (VT)a.xhi[i]) : (VT)0;
+                    pv[u] = in ? pnew[i] : (VT)0;
+                    qv[u] = in ? q[i] : (VT)0;
+                    rv[u] = in ? r[i] : (VT)0;
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int i = i0 + u * NT;
+                    if (i >= row1) break;
+                    if constexpr (MIX) {
+                        const float af = (float)alpha;
+                        xlo[i] = fmaf(af, pv[u], xv[u]);
+                        const float ri = fmaf(-af, qv[u], rv[u]);
+                        r[i] = ri;
+                        loc = __dadd_rn(loc, __dmul_rn((double)ri, (double)ri));
+                    } else {
+                        a.xhi[i] = fma(alpha, (double)pv[u], (double)xv[u]);
+                        const double ri = fma(-alpha, (double)qv[u], (double)rv[u]);
+                        r[i] = ri;
+                        loc = __dadd_rn(loc, __dmul_rn(ri, ri));
+                    }
+                }
             }
         }
         MF_MARK(2);
@@ -444,7 +482,7 @@ __global__ void __launch_bounds__(NT, 3) k_cg(CgArgs a)
             loc = 0.0;
             const double *xh = a.xhi;
             auto xsrc = [=](int c) -> double { return xh[c]; };
-            auto rout = [&](int s, int rw, double y) {
+            auto rout = [&](int s, int rw, double y, double, bool) {
                 const int i = s * MF_TILE + rw;
                 const VT rv = (VT)(a.b[i] - y);
                 r[i] = rv;

@@ -159,7 +159,17 @@ __device__ __forceinline__ double warp_sum_partials(const double *part, int coun
 {
     const int lane = threadIdx.x & 31;
     double s = 0.0;
-    for (int i = lane; i < count; i += 32) s += __ldcg(part + i);
+    // batches of 8 independent loads per lane (one L2 round trip per batch)
+    for (int i0 = lane; i0 < count; i0 += 32 * 8) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int i = i0 + 32 * u;
+            v[u] = (i < count) ? __ldcg(part + i) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) s += v[u];
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     return s;

@@ -38,9 +38,9 @@
 namespace mf {
 namespace {
 
-constexpr int NT = 256;
-constexpr int HWS = NT / MF_TILE;  // half-warps per CTA = strips per chunk
-static_assert(HWS == CH_STRIPS, "one half-warp per strip of a chunk");
+constexpr int NT = CH_STRIPS * MF_TILE;  // one half-warp per strip of a chunk
+constexpr int MINB = (NT == 256) ? 3 : 6;   // CTAs per SM the registers allow
+constexpr int RECS = 64;                    // chunk records cached in shared memory
 
 // Byte layout of one shared-memory stage (every region 16-byte aligned,
 // sized for the largest 16-byte-rounded range it receives).
@@ -66,6 +66,7 @@ struct __align__(16) SolverSmem {
     unsigned char stage[2][STAGE_BYTES];
     double seg[CH_TILES * MF_TILE];
     StageHdr hdr[2];
+    ChunkRec recs[RECS];
     uint64_t bar[2];
     double warp[NT / 32];
     double res;
@@ -134,7 +135,8 @@ __device__ __forceinline__ unsigned range_bytes(long long a0, long long a1)
 template <int PK>
 __device__ void issue_chunk(const CgArgs &a, SolverSmem &S, int c, int k)
 {
-    const ChunkRec r = a.chunks[c];
+    const int cb = a.cta_chunk[blockIdx.x];
+    const ChunkRec r = (c - cb < RECS) ? S.recs[c - cb] : a.chunks[c];
     StageHdr &h = S.hdr[k];
     h.rec = r;
     unsigned char *st = S.stage[k];
@@ -267,8 +269,17 @@ __device__ double direct_row(const CgArgs &a, int s, int r, int rowlen, Src src)
 // y = A src over this CTA's chunks [cb, ce); out(s, r, y) receives every row.
 // Returns false when a bounded wait expired (status set).
 template <int PK, class Src, class Out>
-__device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb, int ce, Src src, Out &out)
+__device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb, int ce, Src src, Out &out,
+                            unsigned long long *tph)
 {
+    const bool timed = tph != nullptr && threadIdx.x == 0;
+    unsigned long long tm = timed ? globaltimer_ns() : 0ull;
+#define MF_SUB(k)                                          \
+    if (timed) {                                           \
+        const unsigned long long nw_ = globaltimer_ns();   \
+        tph[(k)] += nw_ - tm;                              \
+        tm = nw_;                                          \
+    }
     const MfTiles &A = a.A;
     const int tid = threadIdx.x, hw = tid >> 4, hl = tid & 15;
     if (tid == 0) {
@@ -287,6 +298,7 @@ __device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb,
             break;
         }
         gc.use[k]++;
+        MF_SUB(5);
         const ChunkRec &rec = S.hdr[k].rec;
         if (rec.direct) {
             const int s = rec.s0;
@@ -310,6 +322,7 @@ __device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb,
                 if (v < nt * MF_TILE) S.seg[v] = (double)sv[u];
             }
             __syncthreads();
+            MF_SUB(6);
             const int s = rec.s0 + hw;
             if (s < rec.s1) {
                 const int rowlen = (s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE;
@@ -323,12 +336,14 @@ __device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb,
         }
         __syncthreads();
         if (tid == 0 && c + 2 < ce) issue_chunk<PK>(a, S, c + 2, k);
+        MF_SUB(7);
     }
+#undef MF_SUB
     return ok;
 }
 
 template <bool MIX>
-__global__ void __launch_bounds__(NT, 3) k_cg(CgArgs a)
+__global__ void __launch_bounds__(NT, MINB) k_cg(CgArgs a)
 {
     using VT = typename VecT<MIX>::T;
     constexpr int PK = MIX ? 1 : 0;
@@ -350,6 +365,7 @@ __global__ void __launch_bounds__(NT, 3) k_cg(CgArgs a)
         mbar_init(&S.bar[1], 1);
         mbar_fence_init();
     }
+    for (int c = cb + threadIdx.x; c < ce && c - cb < RECS; c += NT) S.recs[c - cb] = a.chunks[c];
     __syncthreads();
 
     double rho, beta, nb, rmax;
@@ -384,7 +400,7 @@ __global__ void __launch_bounds__(NT, 3) k_cg(CgArgs a)
     }
     int exit_reason = EXIT_MAXITER;
     double relres_true = sqrt(rho) / nb;
-    unsigned long long tph[5] = {0, 0, 0, 0, 0}, tmark = 0;
+    unsigned long long tph[8] = {0, 0, 0, 0, 0, 0, 0, 0}, tmark = 0;
     const bool timed = a.timing != nullptr && threadIdx.x == 0;
 #define MF_MARK(k)                                        \
     if (timed) {                                          \
@@ -420,7 +436,7 @@ __global__ void __launch_bounds__(NT, 3) k_cg(CgArgs a)
             q[i] = qi;
             loc = __dadd_rn(loc, __dmul_rn((double)pn, (double)qi));
         };
-        if (!spmv_chunks<PK>(a, S, gc, cb, ce, psrc, aout)) gc.ok = false;
+        if (!spmv_chunks<PK>(a, S, gc, cb, ce, psrc, aout, timed ? tph : nullptr)) gc.ok = false;
         MF_MARK(0);
         const double pq = grid_sum(a, loc, 2, gc, S);
         MF_MARK(1);
@@ -488,7 +504,7 @@ __global__ void __launch_bounds__(NT, 3) k_cg(CgArgs a)
                 r[i] = rv;
                 loc = __dadd_rn(loc, __dmul_rn((double)rv, (double)rv));
             };
-            if (!spmv_chunks<0>(a, S, gc, cb, ce, xsrc, rout)) gc.ok = false;
+            if (!spmv_chunks<0>(a, S, gc, cb, ce, xsrc, rout, nullptr)) gc.ok = false;
             rho_new = grid_sum(a, loc, 1, gc, S);
             if (!gc.ok) break;
             rmax = sqrt(rho_new);
@@ -515,7 +531,7 @@ __global__ void __launch_bounds__(NT, 3) k_cg(CgArgs a)
         }
     }
     if (timed)
-        for (int k = 0; k < 5; k++) a.timing[g * 8 + k] += tph[k];
+        for (int k = 0; k < 8; k++) a.timing[g * 8 + k] += tph[k];
     if (g == 0 && threadIdx.x == 0) {
         st[S_RHO] = rho;
         st[S_BETA] = beta;

@@ -124,9 +124,10 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
         std::vector<unsigned long long> t((size_t)G * 8);
         MF_CUDA(cudaMemcpy(t.data(), w.timing, sizeof(unsigned long long) * 8 * G, cudaMemcpyDeviceToHost));
         double mx = 0;
-        for (int k = 0; k < 6; k++) rep.phase_us[k] = 0;
+        for (int k = 0; k < 9; k++) rep.phase_us[k] = 0;
         for (int g = 0; g < G; g++) {
             for (int k = 0; k < 5; k++) rep.phase_us[k] += t[(size_t)g * 8 + k] * 1e-3 / G;
+            for (int k = 5; k < 8; k++) rep.phase_us[k + 1] += t[(size_t)g * 8 + k] * 1e-3 / G;
             mx = std::max(mx, t[(size_t)g * 8] * 1e-3);
         }
         rep.phase_us[5] = mx;

@@ -8,9 +8,12 @@ namespace mf {
 // entries and bytes fit one shared-memory stage.  A strip too large for a
 // stage on its own is a one-strip chunk with `direct` set (computed from
 // global memory).
-constexpr int CH_STRIPS = 16;
-constexpr int CH_TILES = 128;
-constexpr int CH_ENTRIES = 2048;
+#ifndef MF_CHUNK_STRIPS
+#define MF_CHUNK_STRIPS 16
+#endif
+constexpr int CH_STRIPS = MF_CHUNK_STRIPS;
+constexpr int CH_TILES = 8 * CH_STRIPS;
+constexpr int CH_ENTRIES = 128 * CH_STRIPS;
 struct ChunkRec {
     int s0, s1;       // strips [s0, s1)
     int t0, t1;       // tiles [t0, t1)

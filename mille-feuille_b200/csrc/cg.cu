@@ -122,7 +122,7 @@ __device__ __forceinline__ void add_range(unsigned char *dst, const unsigned cha
 {
     const long long c0 = a0 & ~15ll, c1 = (a1 + 15) & ~15ll;
     shift = (int)(a0 - c0);
-    if (c1 > c0) bulk_g2s(dst, src + c0, (unsigned)(c1 - c0), bar);
+    if (c1 > c0) bulk_g2s_hint(dst, src + c0, (unsigned)(c1 - c0), bar, l2_policy_evict_first());
 }
 
 __device__ __forceinline__ unsigned range_bytes(long long a0, long long a1)

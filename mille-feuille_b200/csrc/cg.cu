@@ -31,6 +31,7 @@
 #include <cuda_fp16.h>
 
 #include <cstdlib>
+#include <type_traits>
 
 #include "solver.h"
 #include "tma.cuh"
@@ -39,7 +40,10 @@ namespace mf {
 namespace {
 
 constexpr int NT = CH_STRIPS * MF_TILE;  // one half-warp per strip of a chunk
-constexpr int MINB = (NT == 256) ? 3 : 6;   // CTAs per SM the registers allow
+#ifndef MF_CG_MINB
+#define MF_CG_MINB 3
+#endif
+constexpr int MINB = MF_CG_MINB;  // CTAs per SM the registers allow
 constexpr int RECS = 64;                    // chunk records cached in shared memory
 
 // Byte layout of one shared-memory stage (every region 16-byte aligned,
@@ -172,7 +176,12 @@ __device__ void issue_chunk(const CgArgs &a, SolverSmem &S, int c, int k)
 // Row r of strip s from a staged chunk (reference order: tiles in column
 // order, each tile's row entries in order).  FP64 payload: products and sums
 // rounded separately (bit-identical to blockspmv_cpu); packed payload: FP32
-// fused multiply-add accumulation.
+// fused multiply-add accumulation.  Tiles are taken eight at a time: every
+// shared-memory load that locates a tile's row run, and the first ENT entries
+// of each run, are issued before any is used, so one row costs a few
+// shared-memory round trips instead of several per tile.
+constexpr int RT = 4;   // tiles per batch
+constexpr int ENT = 2;  // entries per tile run loaded ahead
 template <int PK>
 __device__ __forceinline__ double chunk_row(const CgArgs &a, const SolverSmem &S, int k, int s, int r, int rowlen,
                                             double &xown, bool &has_own)
@@ -182,48 +191,100 @@ __device__ __forceinline__ double chunk_row(const CgArgs &a, const SolverSmem &S
     const unsigned char *st = S.stage[k];
     const int *tp = (const int *)(st + OFF_TPTR + h.sh_tptr);
     const int *tn = (const int *)(st + OFF_TNNZ + h.sh_tnnz);
+    const int *tcl = (const int *)(st + OFF_TCOL + h.sh_tcol);
     const unsigned char *cb = st + OFF_COL + h.sh_col;
     const unsigned char *pb = st + OFF_PTR + h.sh_ptr;
+    const unsigned char *payb = st + OFF_PAY + h.sh_pay;
+    const unsigned *po = (const unsigned *)(st + OFF_POFF + h.sh_poff);
+    const unsigned char *wc = st + OFF_WCLS + h.sh_wcls;
     const long long p00 = ptr_off(a, rec.t0);
-    const int *tcl = (const int *)(st + OFF_TCOL + h.sh_tcol);
     const int ta = tp[s - rec.s0], tb = tp[s - rec.s0 + 1];
     double accd = 0.0;
     float accf = 0.0f;
     has_own = false;
-    for (int t = ta; t < tb; t++) {
-        const int jl = t - rec.t0;
-        if (tcl[jl] == s) {  // diagonal tile: its segment holds this row's x value
-            xown = S.seg[jl * MF_TILE + r];
-            has_own = true;
-        }
-        const int off = tn[jl] - rec.e0;
-        const int nz = tn[jl + 1] - tn[jl];
-        const unsigned char *prow = pb + (ptr_off(a, t) - p00);
-        const int lo = prow[r];
-        const int hi = (r == rowlen - 1) ? nz : (int)prow[r + 1];
-        const double *seg = S.seg + jl * MF_TILE;
-        const unsigned char *cl = cb + off;
-        if (PK == 0) {
-            const double *v = (const double *)(st + OFF_PAY + h.sh_pay) + off;
-            double sm = 0.0;
-            for (int q = lo; q < hi; q++) sm = __dadd_rn(sm, __dmul_rn(seg[cl[q]], v[q]));
-            accd = __dadd_rn(accd, sm);
-        } else {
-            const unsigned *po = (const unsigned *)(st + OFF_POFF + h.sh_poff);
-            const int cls = (st + OFF_WCLS + h.sh_wcls)[jl];
-            const unsigned char *vb = st + OFF_PAY + h.sh_pay + (po[jl] - rec.y0);
-            float sm = 0.0f;
-            if (cls == MF_CLASS_FP32 || cls == MF_CLASS_FP64) {
-                const float *v = (const float *)vb;
-                for (int q = lo; q < hi; q++) sm = fmaf(v[q], (float)seg[cl[q]], sm);
-            } else if (cls == MF_CLASS_FP16) {
-                const __half *v = (const __half *)vb;
-                for (int q = lo; q < hi; q++) sm = fmaf(__half2float(v[q]), (float)seg[cl[q]], sm);
-            } else if (cls == MF_CLASS_INT8) {
-                const int8_t *v = (const int8_t *)vb;
-                for (int q = lo; q < hi; q++) sm = fmaf((float)v[q], (float)seg[cl[q]], sm);
+    for (int tbase = ta; tbase < tb; tbase += RT) {
+        int lo[RT], hi[RT], off[RT], jls[RT], cls[RT];
+        unsigned voff[RT];
+#pragma unroll
+        for (int u = 0; u < RT; u++) {
+            const int t = tbase + u;
+            const bool v = t < tb;
+            const int jl = v ? t - rec.t0 : 0;
+            jls[u] = jl;
+            const int o0 = tn[jl], o1 = tn[jl + 1];
+            const unsigned char *prow = pb + (ptr_off(a, v ? t : rec.t0) - p00);
+            const int l = prow[r];
+            const int hh = (r == rowlen - 1) ? (o1 - o0) : (int)prow[r + 1];
+            lo[u] = v ? l : 0;
+            hi[u] = v ? hh : 0;
+            off[u] = o0 - rec.e0;
+            if (PK == 1) {
+                voff[u] = po[jl] - rec.y0;
+                cls[u] = wc[jl];
+            } else {
+                voff[u] = 0;
+                cls[u] = 0;
             }
-            accf += sm;
+            if (v && tcl[jl] == s) {
+                xown = S.seg[jl * MF_TILE + r];
+                has_own = true;
+            }
+        }
+        // first ENT entries of each run: column bytes and values
+        using PV = typename std::conditional<PK == 0, double, float>::type;
+        int cc[RT][ENT];
+        PV vv[RT][ENT];
+#pragma unroll
+        for (int u = 0; u < RT; u++) {
+#pragma unroll
+            for (int e = 0; e < ENT; e++) {
+                const int q = lo[u] + e;
+                const bool in = q < hi[u];
+                const int idx = off[u] + (in ? q : 0);
+                cc[u][e] = in ? cb[idx] : 0;
+                if (PK == 0) {
+                    vv[u][e] = in ? ((const double *)payb)[idx] : 0.0;
+                } else {
+                    const unsigned char *vb = payb + voff[u];
+                    const int qq = in ? q : 0;
+                    float f = 0.f;
+                    if (cls[u] == MF_CLASS_FP32 || cls[u] == MF_CLASS_FP64) f = ((const float *)vb)[qq];
+                    else if (cls[u] == MF_CLASS_FP16) f = __half2float(((const __half *)vb)[qq]);
+                    else if (cls[u] == MF_CLASS_INT8) f = (float)((const int8_t *)vb)[qq];
+                    vv[u][e] = (in && cls[u] != MF_CLASS_BYPASS) ? f : 0.0f;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < RT; u++) {
+            if (tbase + u >= tb) break;
+            const double *seg = S.seg + jls[u] * MF_TILE;
+            if (PK == 0) {
+                double sm = 0.0;
+#pragma unroll
+                for (int e = 0; e < ENT; e++)
+                    if (lo[u] + e < hi[u]) sm = __dadd_rn(sm, __dmul_rn(seg[cc[u][e]], vv[u][e]));
+                for (int q = lo[u] + ENT; q < hi[u]; q++) {
+                    const int idx = off[u] + q;
+                    sm = __dadd_rn(sm, __dmul_rn(seg[cb[idx]], ((const double *)payb)[idx]));
+                }
+                accd = __dadd_rn(accd, sm);
+            } else {
+                if (cls[u] == MF_CLASS_BYPASS) continue;
+                float sm = 0.0f;
+#pragma unroll
+                for (int e = 0; e < ENT; e++)
+                    if (lo[u] + e < hi[u]) sm = fmaf((float)vv[u][e], (float)seg[cc[u][e]], sm);
+                const unsigned char *vb = payb + voff[u];
+                for (int q = lo[u] + ENT; q < hi[u]; q++) {
+                    float f;
+                    if (cls[u] == MF_CLASS_FP32 || cls[u] == MF_CLASS_FP64) f = ((const float *)vb)[q];
+                    else if (cls[u] == MF_CLASS_FP16) f = __half2float(((const __half *)vb)[q]);
+                    else f = (float)((const int8_t *)vb)[q];
+                    sm = fmaf(f, (float)seg[cb[off[u] + q]], sm);
+                }
+                accf += sm;
+            }
         }
     }
     return PK == 0 ? accd : (double)accf;

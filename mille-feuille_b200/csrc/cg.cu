@@ -31,7 +31,6 @@
 #include <cuda_fp16.h>
 
 #include <cstdlib>
-#include <type_traits>
 
 #include "solver.h"
 #include "tma.cuh"
@@ -176,12 +175,8 @@ __device__ void issue_chunk(const CgArgs &a, SolverSmem &S, int c, int k)
 // Row r of strip s from a staged chunk (reference order: tiles in column
 // order, each tile's row entries in order).  FP64 payload: products and sums
 // rounded separately (bit-identical to blockspmv_cpu); packed payload: FP32
-// fused multiply-add accumulation.  Tiles are taken eight at a time: every
-// shared-memory load that locates a tile's row run, and the first ENT entries
-// of each run, are issued before any is used, so one row costs a few
-// shared-memory round trips instead of several per tile.
-constexpr int RT = 4;   // tiles per batch
-constexpr int ENT = 2;  // entries per tile run loaded ahead
+// fused multiply-add accumulation.  The walk advances pointers tile by tile
+// so that each tile costs a handful of shared-memory loads.
 template <int PK>
 __device__ __forceinline__ double chunk_row(const CgArgs &a, const SolverSmem &S, int k, int s, int r, int rowlen,
                                             double &xown, bool &has_own)
@@ -190,102 +185,54 @@ __device__ __forceinline__ double chunk_row(const CgArgs &a, const SolverSmem &S
     const ChunkRec &rec = h.rec;
     const unsigned char *st = S.stage[k];
     const int *tp = (const int *)(st + OFF_TPTR + h.sh_tptr);
-    const int *tn = (const int *)(st + OFF_TNNZ + h.sh_tnnz);
-    const int *tcl = (const int *)(st + OFF_TCOL + h.sh_tcol);
-    const unsigned char *cb = st + OFF_COL + h.sh_col;
-    const unsigned char *pb = st + OFF_PTR + h.sh_ptr;
+    const int ja = tp[s - rec.s0] - rec.t0, jb = tp[s - rec.s0 + 1] - rec.t0;
+    const int *tn = (const int *)(st + OFF_TNNZ + h.sh_tnnz) + ja;
+    const int *tcl = (const int *)(st + OFF_TCOL + h.sh_tcol) + ja;
+    const unsigned char *cb = st + OFF_COL + h.sh_col - rec.e0;
+    // row pointers of tile ja; every tile has `rowlen` pointers in a strip
+    const unsigned char *prow = st + OFF_PTR + h.sh_ptr + (ptr_off(a, rec.t0 + ja) - ptr_off(a, rec.t0)) + r;
+    const double *seg = S.seg + ja * MF_TILE;
     const unsigned char *payb = st + OFF_PAY + h.sh_pay;
-    const unsigned *po = (const unsigned *)(st + OFF_POFF + h.sh_poff);
-    const unsigned char *wc = st + OFF_WCLS + h.sh_wcls;
-    const long long p00 = ptr_off(a, rec.t0);
-    const int ta = tp[s - rec.s0], tb = tp[s - rec.s0 + 1];
+    const unsigned *po = (const unsigned *)(st + OFF_POFF + h.sh_poff) + ja;
+    const unsigned char *wc = st + OFF_WCLS + h.sh_wcls + ja;
+    const bool last = (r == rowlen - 1);
     double accd = 0.0;
     float accf = 0.0f;
     has_own = false;
-    for (int tbase = ta; tbase < tb; tbase += RT) {
-        int lo[RT], hi[RT], off[RT], jls[RT], cls[RT];
-        unsigned voff[RT];
-#pragma unroll
-        for (int u = 0; u < RT; u++) {
-            const int t = tbase + u;
-            const bool v = t < tb;
-            const int jl = v ? t - rec.t0 : 0;
-            jls[u] = jl;
-            const int o0 = tn[jl], o1 = tn[jl + 1];
-            const unsigned char *prow = pb + (ptr_off(a, v ? t : rec.t0) - p00);
-            const int l = prow[r];
-            const int hh = (r == rowlen - 1) ? (o1 - o0) : (int)prow[r + 1];
-            lo[u] = v ? l : 0;
-            hi[u] = v ? hh : 0;
-            off[u] = o0 - rec.e0;
-            if (PK == 1) {
-                voff[u] = po[jl] - rec.y0;
-                cls[u] = wc[jl];
-            } else {
-                voff[u] = 0;
-                cls[u] = 0;
-            }
-            if (v && tcl[jl] == s) {
-                xown = S.seg[jl * MF_TILE + r];
-                has_own = true;
-            }
+    int o0 = tn[0];
+    for (int j = 0; j < jb - ja; j++) {
+        const int o1 = tn[j + 1];
+        const int lo = prow[0];
+        const int hi = last ? (o1 - o0) : (int)prow[1];
+        if (!has_own && tcl[j] == s) {  // diagonal tile: its segment holds this row's x value
+            xown = seg[r];
+            has_own = true;
         }
-        // first ENT entries of each run: column bytes and values
-        using PV = typename std::conditional<PK == 0, double, float>::type;
-        int cc[RT][ENT];
-        PV vv[RT][ENT];
-#pragma unroll
-        for (int u = 0; u < RT; u++) {
-#pragma unroll
-            for (int e = 0; e < ENT; e++) {
-                const int q = lo[u] + e;
-                const bool in = q < hi[u];
-                const int idx = off[u] + (in ? q : 0);
-                cc[u][e] = in ? cb[idx] : 0;
-                if (PK == 0) {
-                    vv[u][e] = in ? ((const double *)payb)[idx] : 0.0;
-                } else {
-                    const unsigned char *vb = payb + voff[u];
-                    const int qq = in ? q : 0;
-                    float f = 0.f;
-                    if (cls[u] == MF_CLASS_FP32 || cls[u] == MF_CLASS_FP64) f = ((const float *)vb)[qq];
-                    else if (cls[u] == MF_CLASS_FP16) f = __half2float(((const __half *)vb)[qq]);
-                    else if (cls[u] == MF_CLASS_INT8) f = (float)((const int8_t *)vb)[qq];
-                    vv[u][e] = (in && cls[u] != MF_CLASS_BYPASS) ? f : 0.0f;
-                }
+        const unsigned char *cl = cb + o0;
+        if (PK == 0) {
+            const double *v = (const double *)payb + (o0 - rec.e0);
+            double sm = 0.0;
+            for (int q = lo; q < hi; q++) sm = __dadd_rn(sm, __dmul_rn(seg[cl[q]], v[q]));
+            accd = __dadd_rn(accd, sm);
+        } else {
+            const int cls = wc[j];
+            const unsigned char *vb = payb + (po[j] - rec.y0);
+            float sm = 0.0f;
+            if (cls == MF_CLASS_FP32 || cls == MF_CLASS_FP64) {
+                const float *v = (const float *)vb;
+                for (int q = lo; q < hi; q++) sm = fmaf(v[q], (float)seg[cl[q]], sm);
+            } else if (cls == MF_CLASS_FP16) {
+                const __half *v = (const __half *)vb;
+                for (int q = lo; q < hi; q++) sm = fmaf(__half2float(v[q]), (float)seg[cl[q]], sm);
+            } else if (cls == MF_CLASS_INT8) {
+                const int8_t *v = (const int8_t *)vb;
+                for (int q = lo; q < hi; q++) sm = fmaf((float)v[q], (float)seg[cl[q]], sm);
             }
+            accf += sm;
         }
-#pragma unroll
-        for (int u = 0; u < RT; u++) {
-            if (tbase + u >= tb) break;
-            const double *seg = S.seg + jls[u] * MF_TILE;
-            if (PK == 0) {
-                double sm = 0.0;
-#pragma unroll
-                for (int e = 0; e < ENT; e++)
-                    if (lo[u] + e < hi[u]) sm = __dadd_rn(sm, __dmul_rn(seg[cc[u][e]], vv[u][e]));
-                for (int q = lo[u] + ENT; q < hi[u]; q++) {
-                    const int idx = off[u] + q;
-                    sm = __dadd_rn(sm, __dmul_rn(seg[cb[idx]], ((const double *)payb)[idx]));
-                }
-                accd = __dadd_rn(accd, sm);
-            } else {
-                if (cls[u] == MF_CLASS_BYPASS) continue;
-                float sm = 0.0f;
-#pragma unroll
-                for (int e = 0; e < ENT; e++)
-                    if (lo[u] + e < hi[u]) sm = fmaf((float)vv[u][e], (float)seg[cc[u][e]], sm);
-                const unsigned char *vb = payb + voff[u];
-                for (int q = lo[u] + ENT; q < hi[u]; q++) {
-                    float f;
-                    if (cls[u] == MF_CLASS_FP32 || cls[u] == MF_CLASS_FP64) f = ((const float *)vb)[q];
-                    else if (cls[u] == MF_CLASS_FP16) f = __half2float(((const __half *)vb)[q]);
-                    else f = (float)((const int8_t *)vb)[q];
-                    sm = fmaf(f, (float)seg[cb[off[u] + q]], sm);
-                }
-                accf += sm;
-            }
-        }
+        o0 = o1;
+        prow += rowlen;
+        seg += MF_TILE;
     }
     return PK == 0 ? accd : (double)accf;
 }
@@ -368,19 +315,21 @@ __device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb,
         } else {
             const int nt = rec.t1 - rec.t0;
             const int *tc = (const int *)(S.stage[k] + OFF_TCOL + S.hdr[k].sh_tcol);
-            // x segments: all of a thread's gathers issued before any is used
-            constexpr int SEGV = CH_TILES * MF_TILE / NT;
-            decltype(src(0)) sv[SEGV];
+            // x segments: gathers issued SEGB at a time before any is used
+            constexpr int SEGB = 4;
+            for (int v0 = tid; v0 < nt * MF_TILE; v0 += NT * SEGB) {
+                decltype(src(0)) sv[SEGB];
 #pragma unroll
-            for (int u = 0; u < SEGV; u++) {
-                const int v = tid + u * NT;
-                const int col = (v < nt * MF_TILE) ? tc[v >> 4] * MF_TILE + (v & 15) : A.cols;
-                sv[u] = (col < A.cols) ? src(col) : (decltype(src(0)))0;
-            }
+                for (int u = 0; u < SEGB; u++) {
+                    const int v = v0 + u * NT;
+                    const int col = (v < nt * MF_TILE) ? tc[v >> 4] * MF_TILE + (v & 15) : A.cols;
+                    sv[u] = (col < A.cols) ? src(col) : (decltype(src(0)))0;
+                }
 #pragma unroll
-            for (int u = 0; u < SEGV; u++) {
-                const int v = tid + u * NT;
-                if (v < nt * MF_TILE) S.seg[v] = (double)sv[u];
+                for (int u = 0; u < SEGB; u++) {
+                    const int v = v0 + u * NT;
+                    if (v < nt * MF_TILE) S.seg[v] = (double)sv[u];
+                }
             }
             __syncthreads();
             MF_SUB(6);

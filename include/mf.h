@@ -157,9 +157,8 @@ typedef struct mf_solve_report {
      * spent in [0] the SpMV phase, [1] its reduction wait, [2] the vector
      * update phase, [3] its reduction wait, [4] reliable updates, [5] the
      * largest per-CTA SpMV-phase time; inside the SpMV phase: [6] waiting
-     * for staged chunks, [7] building x segments, [8] computing rows, [9]
-     * issuing the bulk copies of the next chunk */
-    double phase_us[10];
+     * for staged chunks, [7] building x segments, [8] computing rows */
+    double phase_us[9];
 } mf_solve_report;
 
 /* Fills opts with the defaults (maxiter 20000, tol 1e-10, FP64 policy). */

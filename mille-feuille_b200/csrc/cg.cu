@@ -38,8 +38,7 @@
 namespace mf {
 namespace {
 
-constexpr int NCONS = CH_STRIPS * MF_TILE;  // consumer threads: one half-warp per strip of a chunk
-constexpr int NT = NCONS + 32;              // plus one producer warp that issues the bulk copies
+constexpr int NT = CH_STRIPS * MF_TILE;  // one half-warp per strip of a chunk
 #ifndef MF_CG_MINB
 #define MF_CG_MINB 3
 #endif
@@ -71,10 +70,7 @@ struct __align__(16) SolverSmem {
     double seg[CH_TILES * MF_TILE];
     StageHdr hdr[2];
     ChunkRec recs[RECS];
-    uint64_t bar[2];    // "full": the chunk's bytes landed
-    uint64_t empty[2];  // "empty": the consumers released the stage
-    unsigned issued[2], used[2];
-    int wait_ok;
+    uint64_t bar[2];
     double warp[NT / 32];
     double res;
 };
@@ -124,24 +120,21 @@ __device__ __forceinline__ long long ptr_off(const CgArgs &a, int t)
                                    : 16ll * a.last_tile_begin + (long long)(t - a.last_tile_begin) * a.last_rowlen;
 }
 
-struct Range {
-    const unsigned char *src;
-    long long c0;
-    unsigned bytes;
-    int dst_off;
-};
-
-__device__ __forceinline__ Range make_range(const unsigned char *src, long long a0, long long a1, int dst_off,
-                                            int &shift)
+__device__ __forceinline__ void add_range(unsigned char *dst, const unsigned char *src, long long a0, long long a1,
+                                          uint64_t *bar, int &shift)
 {
     const long long c0 = a0 & ~15ll, c1 = (a1 + 15) & ~15ll;
     shift = (int)(a0 - c0);
-    return Range{src, c0, (unsigned)(c1 > c0 ? c1 - c0 : 0), dst_off};
+    if (c1 > c0) bulk_g2s_hint(dst, src + c0, (unsigned)(c1 - c0), bar, l2_policy_evict_first());
 }
 
-// Producer lane: stage chunk c into stage k.  The header (chunk record and
-// the shift of each range) is written before the arrive that the consumers
-// acquire; then the copies are issued.
+__device__ __forceinline__ unsigned range_bytes(long long a0, long long a1)
+{
+    const long long c0 = a0 & ~15ll, c1 = (a1 + 15) & ~15ll;
+    return (unsigned)(c1 - c0);
+}
+
+// Thread 0: stage chunk c into stage k.
 template <int PK>
 __device__ void issue_chunk(const CgArgs &a, SolverSmem &S, int c, int k)
 {
@@ -149,31 +142,34 @@ __device__ void issue_chunk(const CgArgs &a, SolverSmem &S, int c, int k)
     const ChunkRec r = (c - cb < RECS) ? S.recs[c - cb] : a.chunks[c];
     StageHdr &h = S.hdr[k];
     h.rec = r;
+    unsigned char *st = S.stage[k];
     const MfTiles &A = a.A;
-    Range rg[8];
-    int n = 0;
-    rg[n++] = make_range((const unsigned char *)A.tile_ptr, 4ll * r.s0, 4ll * (r.s1 + 1), OFF_TPTR, h.sh_tptr);
+    // expected bytes first (the barrier counts them down as copies land)
+    unsigned total = range_bytes(4ll * r.s0, 4ll * (r.s1 + 1));
     if (!r.direct) {
-        rg[n++] = make_range((const unsigned char *)A.tile_columnidx, 4ll * r.t0, 4ll * r.t1, OFF_TCOL, h.sh_tcol);
-        rg[n++] = make_range((const unsigned char *)A.tile_nnz, 4ll * r.t0, 4ll * (r.t1 + 1), OFF_TNNZ, h.sh_tnnz);
-        rg[n++] = make_range(A.ptr, ptr_off(a, r.t0), ptr_off(a, r.t1), OFF_PTR, h.sh_ptr);
-        rg[n++] = make_range(A.col, r.e0, r.e1, OFF_COL, h.sh_col);
+        total += range_bytes(4ll * r.t0, 4ll * r.t1) + range_bytes(4ll * r.t0, 4ll * (r.t1 + 1));
+        total += range_bytes(ptr_off(a, r.t0), ptr_off(a, r.t1)) + range_bytes(r.e0, r.e1);
         if (PK == 1) {
-            rg[n++] = make_range((const unsigned char *)a.poff, 4ll * r.t0, 4ll * (r.t1 + 1), OFF_POFF, h.sh_poff);
-            rg[n++] = make_range(a.wcls, r.t0, r.t1, OFF_WCLS, h.sh_wcls);
-            rg[n++] = make_range(a.pay, r.y0, r.y1, OFF_PAY, h.sh_pay);
+            total += range_bytes(4ll * r.t0, 4ll * (r.t1 + 1)) + range_bytes(r.t0, r.t1) + range_bytes(r.y0, r.y1);
         } else {
-            rg[n++] = make_range((const unsigned char *)A.val, 8ll * r.e0, 8ll * r.e1, OFF_PAY, h.sh_pay);
+            total += range_bytes(8ll * r.e0, 8ll * r.e1);
         }
     }
-    unsigned total = 0;
-    for (int i = 0; i < n; i++) total += rg[i].bytes;
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(&S.bar[k], total);
-    const uint64_t pol = l2_policy_evict_first();
-    unsigned char *st = S.stage[k];
-    for (int i = 0; i < n; i++)
-        if (rg[i].bytes) bulk_g2s_hint(st + rg[i].dst_off, rg[i].src + rg[i].c0, rg[i].bytes, &S.bar[k], pol);
+    add_range(st + OFF_TPTR, (const unsigned char *)A.tile_ptr, 4ll * r.s0, 4ll * (r.s1 + 1), &S.bar[k], h.sh_tptr);
+    if (r.direct) return;
+    add_range(st + OFF_TCOL, (const unsigned char *)A.tile_columnidx, 4ll * r.t0, 4ll * r.t1, &S.bar[k], h.sh_tcol);
+    add_range(st + OFF_TNNZ, (const unsigned char *)A.tile_nnz, 4ll * r.t0, 4ll * (r.t1 + 1), &S.bar[k], h.sh_tnnz);
+    add_range(st + OFF_PTR, A.ptr, ptr_off(a, r.t0), ptr_off(a, r.t1), &S.bar[k], h.sh_ptr);
+    add_range(st + OFF_COL, A.col, r.e0, r.e1, &S.bar[k], h.sh_col);
+    if (PK == 1) {
+        add_range(st + OFF_POFF, (const unsigned char *)a.poff, 4ll * r.t0, 4ll * (r.t1 + 1), &S.bar[k], h.sh_poff);
+        add_range(st + OFF_WCLS, a.wcls, r.t0, r.t1, &S.bar[k], h.sh_wcls);
+        add_range(st + OFF_PAY, a.pay, r.y0, r.y1, &S.bar[k], h.sh_pay);
+    } else {
+        add_range(st + OFF_PAY, (const unsigned char *)A.val, 8ll * r.e0, 8ll * r.e1, &S.bar[k], h.sh_pay);
+    }
 }
 
 // Row r of strip s from a staged chunk (reference order: tiles in column
@@ -280,61 +276,36 @@ __device__ double direct_row(const CgArgs &a, int s, int r, int rowlen, Src src)
 
 // y = A src over this CTA's chunks [cb, ce); out(s, r, y) receives every row.
 // Returns false when a bounded wait expired (status set).
-__device__ __forceinline__ void cons_sync() { asm volatile("bar.sync 1, %0;\n" ::"n"(NCONS) : "memory"); }
-__device__ __forceinline__ void mbar_arrive1(uint64_t *bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
-}
-
-// y = A src over this CTA's chunks [cb, ce); out(s, r, y, x_own, has_own)
-// receives every row.  Warp NCONS/32 is the producer: its lane 0 stages each
-// chunk into the stage the consumers last released.  The consumers wait for
-// the bytes, build the x segments, compute the rows and release the stage.
-// Returns false when a bounded wait expired (status set).
 template <int PK, class Src, class Out>
 __device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb, int ce, Src src, Out &out,
                             unsigned long long *tph)
 {
+    const bool timed = tph != nullptr && threadIdx.x == 0;
+    unsigned long long tm = timed ? globaltimer_ns() : 0ull;
+#define MF_SUB(k)                                          \
+    if (timed) {                                           \
+        const unsigned long long nw_ = globaltimer_ns();   \
+        tph[(k)] += nw_ - tm;                              \
+        tm = nw_;                                          \
+    }
     const MfTiles &A = a.A;
     const int tid = threadIdx.x, hw = tid >> 4, hl = tid & 15;
-    if (tid >= NCONS) {
-        if (tid == NCONS) {
-            for (int c = cb; c < ce; c++) {
-                const int k = (c - cb) & 1;
-                if (S.issued[k] > 0 &&
-                    !mbar_wait_bounded(&S.empty[k], (S.issued[k] - 1) & 1u, a.status, a.budget_ns))
-                    break;
-                issue_chunk<PK>(a, S, c, k);
-                S.issued[k]++;
-            }
-        }
-        __syncwarp();
-        return true;
+    if (tid == 0) {
+        if (cb < ce) issue_chunk<PK>(a, S, cb, 0);
+        if (cb + 1 < ce) issue_chunk<PK>(a, S, cb + 1, 1);
     }
-    const bool timed = tph != nullptr && tid == 0;
-    unsigned long long tm = timed ? globaltimer_ns() : 0ull;
-#define MF_SUB(k)                                        \
-    if (timed) {                                         \
-        const unsigned long long nw_ = globaltimer_ns(); \
-        tph[(k)] += nw_ - tm;                            \
-        tm = nw_;                                        \
-    }
+    __syncthreads();
     bool ok = true;
     for (int c = cb; c < ce; c++) {
         const int k = (c - cb) & 1;
-        // one thread waits with a bound and tells the others
-        if (tid == 0) S.wait_ok = mbar_wait_bounded(&S.bar[k], S.used[k] & 1u, a.status, a.budget_ns) ? 1 : 0;
-        cons_sync();
-        if (!S.wait_ok) {
+        if (!mbar_wait_bounded(&S.bar[k], gc.use[k] & 1u, a.status, a.budget_ns)) {
             ok = false;
+            // the other stage may still have a copy in flight: wait for it
+            // (bounded) before leaving so no copy lands in freed memory
+            if (c + 1 < ce) mbar_wait_bounded(&S.bar[k ^ 1], gc.use[k ^ 1] & 1u, a.status, a.budget_ns);
             break;
         }
-        // observe the completed phase (makes the staged bytes visible); the
-        // phase already completed, so this returns at once
-        for (int spin = 0; spin < (1 << 20) && !mbar_try_wait(&S.bar[k], S.used[k] & 1u); spin++) {
-        }
-        cons_sync();
-        if (tid == 0) S.used[k]++;
+        gc.use[k]++;
         MF_SUB(5);
         const ChunkRec &rec = S.hdr[k].rec;
         if (rec.direct) {
@@ -346,21 +317,21 @@ __device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb,
             const int *tc = (const int *)(S.stage[k] + OFF_TCOL + S.hdr[k].sh_tcol);
             // x segments: gathers issued SEGB at a time before any is used
             constexpr int SEGB = 4;
-            for (int v0 = tid; v0 < nt * MF_TILE; v0 += NCONS * SEGB) {
+            for (int v0 = tid; v0 < nt * MF_TILE; v0 += NT * SEGB) {
                 decltype(src(0)) sv[SEGB];
 #pragma unroll
                 for (int u = 0; u < SEGB; u++) {
-                    const int v = v0 + u * NCONS;
+                    const int v = v0 + u * NT;
                     const int col = (v < nt * MF_TILE) ? tc[v >> 4] * MF_TILE + (v & 15) : A.cols;
                     sv[u] = (col < A.cols) ? src(col) : (decltype(src(0)))0;
                 }
 #pragma unroll
                 for (int u = 0; u < SEGB; u++) {
-                    const int v = v0 + u * NCONS;
+                    const int v = v0 + u * NT;
                     if (v < nt * MF_TILE) S.seg[v] = (double)sv[u];
                 }
             }
-            cons_sync();
+            __syncthreads();
             MF_SUB(6);
             const int s = rec.s0 + hw;
             if (s < rec.s1) {
@@ -373,14 +344,9 @@ __device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb,
                 }
             }
         }
-        cons_sync();
+        __syncthreads();
+        if (tid == 0 && c + 2 < ce) issue_chunk<PK>(a, S, c + 2, k);
         MF_SUB(7);
-        if (tid == 0) mbar_arrive1(&S.empty[k]);
-    }
-    if (!ok && tid == 0) {
-        // leave no copy in flight: wait (bounded) for stages issued but unused
-        for (int k = 0; k < 2; k++)
-            if (S.issued[k] > S.used[k]) mbar_wait_bounded(&S.bar[k], S.used[k] & 1u, a.status, a.budget_ns);
     }
 #undef MF_SUB
     return ok;
@@ -407,10 +373,6 @@ __global__ void __launch_bounds__(NT, MINB) k_cg(CgArgs a)
     if (threadIdx.x == 0) {
         mbar_init(&S.bar[0], 1);
         mbar_init(&S.bar[1], 1);
-        mbar_init(&S.empty[0], 1);
-        mbar_init(&S.empty[1], 1);
-        S.issued[0] = S.issued[1] = 0;
-        S.used[0] = S.used[1] = 0;
         mbar_fence_init();
     }
     for (int c = cb + threadIdx.x; c < ce && c - cb < RECS; c += NT) S.recs[c - cb] = a.chunks[c];
@@ -448,7 +410,7 @@ __global__ void __launch_bounds__(NT, MINB) k_cg(CgArgs a)
     }
     int exit_reason = EXIT_MAXITER;
     double relres_true = sqrt(rho) / nb;
-    unsigned long long tph[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, tmark = 0;
+    unsigned long long tph[8] = {0, 0, 0, 0, 0, 0, 0, 0}, tmark = 0;
     const bool timed = a.timing != nullptr && threadIdx.x == 0;
 #define MF_MARK(k)                                        \
     if (timed) {                                          \
@@ -579,7 +541,7 @@ __global__ void __launch_bounds__(NT, MINB) k_cg(CgArgs a)
         }
     }
     if (timed)
-        for (int k = 0; k < 9; k++) a.timing[g * 16 + k] += tph[k];
+        for (int k = 0; k < 8; k++) a.timing[g * 8 + k] += tph[k];
     if (g == 0 && threadIdx.x == 0) {
         st[S_RHO] = rho;
         st[S_BETA] = beta;
@@ -662,7 +624,7 @@ mf_status solver_resources(mf_matrix m, int G, SolverWork &w)
     const size_t o_rp = off; off += align256((size_t)2 * 1024 * 8);
     const size_t o_out = off; off += align256(8 * 8);
     const size_t o_state = off; off += align256(32 * 8);
-    const size_t o_tim = off; off += align256((size_t)G * 16 * 8);
+    const size_t o_tim = off; off += align256((size_t)G * 8 * 8);
     const size_t o_bar = off; off += align256(9 * 128);
     const size_t o_st = off; off += align256(8);
     MF_TRY(ensure_work(m, off));

@@ -62,7 +62,7 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
     a.budget_ns = (unsigned long long)(o.wait_budget_s * 1e9);
     a.start = 1;
     a.timing = o.phase_times ? w.timing : nullptr;
-    if (a.timing) MF_CUDA(cudaMemsetAsync(w.timing, 0, sizeof(unsigned long long) * 16 * G, s));
+    if (a.timing) MF_CUDA(cudaMemsetAsync(w.timing, 0, sizeof(unsigned long long) * 8 * G, s));
     MF_CUDA(cudaMemsetAsync(w.status, 0, sizeof(int), s));
     cudaEvent_t e0, e1;
     MF_CUDA(cudaEventCreate(&e0));
@@ -121,14 +121,14 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
     }
     (void)launches;
     if (a.timing) {
-        std::vector<unsigned long long> t((size_t)G * 16);
-        MF_CUDA(cudaMemcpy(t.data(), w.timing, sizeof(unsigned long long) * 16 * G, cudaMemcpyDeviceToHost));
+        std::vector<unsigned long long> t((size_t)G * 8);
+        MF_CUDA(cudaMemcpy(t.data(), w.timing, sizeof(unsigned long long) * 8 * G, cudaMemcpyDeviceToHost));
         double mx = 0;
-        for (int k = 0; k < 10; k++) rep.phase_us[k] = 0;
+        for (int k = 0; k < 9; k++) rep.phase_us[k] = 0;
         for (int g = 0; g < G; g++) {
-            for (int k = 0; k < 5; k++) rep.phase_us[k] += t[(size_t)g * 16 + k] * 1e-3 / G;
-            for (int k = 5; k < 9; k++) rep.phase_us[k + 1] += t[(size_t)g * 16 + k] * 1e-3 / G;
-            mx = std::max(mx, t[(size_t)g * 16] * 1e-3);
+            for (int k = 0; k < 5; k++) rep.phase_us[k] += t[(size_t)g * 8 + k] * 1e-3 / G;
+            for (int k = 5; k < 8; k++) rep.phase_us[k + 1] += t[(size_t)g * 8 + k] * 1e-3 / G;
+            mx = std::max(mx, t[(size_t)g * 8] * 1e-3);
         }
         rep.phase_us[5] = mx;
     }

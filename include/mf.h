@@ -174,6 +174,16 @@ mf_status mf_cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_op
 mf_status mf_cg_solve_host(mf_matrix m, const double *b_host, double *x_host,
                            const mf_solve_opts *opts, mf_solve_report *report);
 
+/* Solves A x = b (A need not be symmetric) with one persistent cooperative
+ * BiCGSTAB kernel, x0 = 0, shadow residual r0 = b; the algorithm of
+ * src/Mille-feuille-bicg.h:202-474, stopped on ||r|| <= tol ||b||.  The
+ * mixed policies use the value-range tile classes with FP64 reliable
+ * updates (no checkpoint policies for BiCGSTAB). */
+mf_status mf_bicgstab_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts *opts,
+                            mf_solve_report *report, double *history, void *stream);
+mf_status mf_bicgstab_solve_host(mf_matrix m, const double *b_host, double *x_host,
+                                 const mf_solve_opts *opts, mf_solve_report *report);
+
 /* ---------------------------------------------------------------------- */
 /* Matrix Market input and synthetic matrices                              */
 /* ---------------------------------------------------------------------- */

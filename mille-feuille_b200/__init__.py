@@ -88,6 +88,8 @@ def lib() -> C.CDLL:
         L.mf_solve_opts_default.restype = None
         L.mf_cg_solve.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport), vp, vp]
         L.mf_cg_solve_host.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]
+        L.mf_bicgstab_solve.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport), vp, vp]
+        L.mf_bicgstab_solve_host.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]
         L.mf_read_matrix_market.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
         L.mf_free_host.argtypes = [vp]
         L.mf_free_host.restype = None
@@ -244,13 +246,15 @@ class Matrix:
     def encode_column_index(self):
         check(lib().mf_encode_column_index(self.h, None))
 
-    def solve_host(self, b, **opts):
-        """CG with host b/x through mf_cg_solve_host; returns (x, report)."""
+    def solve_host(self, b, method="cg", **opts):
+        """CG (or BiCGSTAB) with host b/x through mf_*_solve_host; returns
+        (x, report)."""
         b = np.ascontiguousarray(b, np.float64)
         x = np.zeros(self.info().rows, np.float64)
         rep = SolveReport()
         o = solve_opts(**opts)
-        st = lib().mf_cg_solve_host(self.h, b.ctypes.data, x.ctypes.data, C.byref(o), C.byref(rep))
+        fn = lib().mf_bicgstab_solve_host if method == "bicgstab" else lib().mf_cg_solve_host
+        st = fn(self.h, b.ctypes.data, x.ctypes.data, C.byref(o), C.byref(rep))
         if st not in (MF_OK, 6):
             check(st)
         return x, rep

@@ -36,6 +36,8 @@ mf_status ensure_work(mf_matrix m, size_t bytes)
 
 mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,
                    double *history, cudaStream_t s);
+mf_status bicgstab_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,
+                         double *history, cudaStream_t s);
 
 static mf_status check_device()
 {
@@ -271,23 +273,23 @@ void mf_solve_opts_default(mf_solve_opts *o)
     o->phase_times = 0;
 }
 
-mf_status mf_cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts *opts, mf_solve_report *report,
-                      double *history, void *stream)
+static mf_status solve_common(bool bicg, mf_matrix m, const double *b, double *x, const mf_solve_opts *opts,
+                              mf_solve_report *report, double *history, void *stream)
 {
     g_err[0] = 0;
     if (!m || !b || !x) {
-        set_last_error("mf_cg_solve: null argument");
+        set_last_error("solve: null argument");
         return MF_ERR_INVALID_ARG;
     }
     mf_solve_opts o;
     mf_solve_opts_default(&o);
     if (opts) o = *opts;
-    if (o.maxiter < 0 || o.wait_budget_s <= 0) {
-        set_last_error("mf_cg_solve: maxiter < 0 or wait budget <= 0");
+    if (o.maxiter < 0 || o.wait_budget_s <= 0 || o.policy < 0 || o.policy > MF_POLICY_LEARNED) {
+        set_last_error("solve: maxiter < 0, wait budget <= 0 or unknown policy");
         return MF_ERR_INVALID_ARG;
     }
     if (m->v.rows != m->v.cols) {
-        set_last_error("mf_cg_solve: matrix is %d x %d, a square system is required", m->v.rows, m->v.cols);
+        set_last_error("solve: matrix is %d x %d, a square system is required", m->v.rows, m->v.cols);
         return MF_ERR_INVALID_ARG;
     }
     mf_solve_report rep;
@@ -295,19 +297,20 @@ mf_status mf_cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_op
     mf_status st;
     if (m->v.rows == 0) {
         st = MF_OK;
-    } else if (o.policy == MF_POLICY_FP64 || o.policy == MF_POLICY_STATIC || o.policy == MF_POLICY_RULE) {
-        st = cg_solve(m, b, x, o, rep, history, (cudaStream_t)stream);
-    } else {
-        set_last_error("policy %d not available in this build", o.policy);
+    } else if (!bicg && o.policy == MF_POLICY_LEARNED && !m->policy_loaded) {
+        set_last_error("learned policy requested but no policy is loaded (mf_policy_load / mf_policy_train)");
         st = MF_ERR_UNSUPPORTED;
+    } else {
+        st = bicg ? bicgstab_solve(m, b, x, o, rep, history, (cudaStream_t)stream)
+                  : cg_solve(m, b, x, o, rep, history, (cudaStream_t)stream);
     }
     rep.status = st;
     if (report) *report = rep;
     return st;
 }
 
-mf_status mf_cg_solve_host(mf_matrix m, const double *b_host, double *x_host, const mf_solve_opts *opts,
-                           mf_solve_report *report)
+static mf_status solve_host_common(bool bicg, mf_matrix m, const double *b_host, double *x_host,
+                                   const mf_solve_opts *opts, mf_solve_report *report)
 {
     if (!m || !b_host || !x_host) return MF_ERR_INVALID_ARG;
     const size_t n = m->v.rows;
@@ -325,7 +328,7 @@ mf_status mf_cg_solve_host(mf_matrix m, const double *b_host, double *x_host, co
         set_last_error("H2D: %s", cudaGetErrorString(e));
         return MF_ERR_CUDA;
     }
-    mf_status st = mf_cg_solve(m, db, dx, opts, report, nullptr, s);
+    mf_status st = solve_common(bicg, m, db, dx, opts, report, nullptr, s);
     e = cudaMemcpyAsync(x_host, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
@@ -333,6 +336,30 @@ mf_status mf_cg_solve_host(mf_matrix m, const double *b_host, double *x_host, co
         return MF_ERR_CUDA;
     }
     return st;
+}
+
+mf_status mf_cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts *opts, mf_solve_report *report,
+                      double *history, void *stream)
+{
+    return solve_common(false, m, b, x, opts, report, history, stream);
+}
+
+mf_status mf_cg_solve_host(mf_matrix m, const double *b_host, double *x_host, const mf_solve_opts *opts,
+                           mf_solve_report *report)
+{
+    return solve_host_common(false, m, b_host, x_host, opts, report);
+}
+
+mf_status mf_bicgstab_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts *opts,
+                            mf_solve_report *report, double *history, void *stream)
+{
+    return solve_common(true, m, b, x, opts, report, history, stream);
+}
+
+mf_status mf_bicgstab_solve_host(mf_matrix m, const double *b_host, double *x_host, const mf_solve_opts *opts,
+                                 mf_solve_report *report)
+{
+    return solve_host_common(true, m, b_host, x_host, opts, report);
 }
 
 }  // extern "C"

@@ -65,6 +65,7 @@ struct mf_matrix_s {
     unsigned char *d_pay = nullptr;
     size_t pay_bytes = 0, pay_used = 0;
     int packed_policy = -1;
+    int policy_loaded = 0;     // a learned policy is attached
     // device staging of b and x for the host-buffer solve entry points
     double *host_io = nullptr;
     size_t host_io_n = 0;

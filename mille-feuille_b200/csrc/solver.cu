@@ -9,11 +9,11 @@
 
 namespace mf {
 
-mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,
-                   double *history, cudaStream_t s)
+static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, double *x, const mf_solve_opts &o,
+                                  mf_solve_report &rep, double *history, cudaStream_t s)
 {
     const bool mixed = o.policy != MF_POLICY_FP64;
-    const int G = solver_grid(m, mixed);
+    const int G = bicg ? bicgstab_grid(m, mixed) : solver_grid(m, mixed);
     if (m->part_ctas != G || !m->d_chunks) {
         MF_TRY(strip_partition(m, G, s));
         MF_TRY(build_chunks(m, s));
@@ -49,6 +49,10 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
     a.p1 = w.p1;
     a.q = w.q;
     a.xlo = w.xlo;
+    a.rhat = w.rhat;
+    a.v0 = w.v0;
+    a.v1 = w.v1;
+    a.t = w.t;
     a.partials = w.partials;
     a.bar = w.bar;
     a.status = w.status;
@@ -58,7 +62,8 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
     a.tol = o.tol;
     a.fixed = o.tol < 0 ? 1 : 0;
     a.delta = o.refine_delta > 0 && o.refine_delta < 1 ? o.refine_delta : 0.1;
-    a.exit_on_refine = (mixed && o.policy != MF_POLICY_STATIC) ? 1 : 0;
+    // checkpoints (policy updates between launches) for CG's dynamic policies
+    a.exit_on_refine = (!bicg && mixed && o.policy != MF_POLICY_STATIC) ? 1 : 0;
     a.budget_ns = (unsigned long long)(o.wait_budget_s * 1e9);
     a.start = 1;
     a.timing = o.phase_times ? w.timing : nullptr;
@@ -72,7 +77,8 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
     int h_status = 0, launches = 0;
     for (;;) {
         MF_CUDA(cudaMemsetAsync(w.bar, 0, 9 * 128, s));
-        MF_TRY(launch_cg(mixed, a, G, s));
+        if (bicg) MF_TRY(launch_bicgstab(mixed, a, G, s));
+        else MF_TRY(launch_cg(mixed, a, G, s));
         launches++;
         if (!a.exit_on_refine) break;
         MF_CUDA(cudaMemcpyAsync(st, w.state, sizeof(st), cudaMemcpyDeviceToHost, s));
@@ -108,7 +114,15 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
     rep.kernel_ms = ms;
     rep.relres = st[S_RELRES];
     const long long n = m->v.rows, nnz = m->v.nnz;
-    if (!mixed) {
+    if (bicg) {
+        // per iteration: two SpMVs plus 15 vector streams (FP64), or their
+        // mixed-precision counterparts; reliable updates as for CG
+        const long long spmv_fp64 = nnz * 9 + 24LL * T + 16 * n;
+        const long long spmv_mixed = (long long)m->pay_used + nnz + 24LL * T + 8 * n;
+        rep.bytes_moved = mixed ? (long long)rep.iterations * (2 * spmv_mixed + 60 * n) +
+                                      (long long)rep.refinements * (spmv_fp64 + 32 * n)
+                                : (long long)rep.iterations * (2 * spmv_fp64 + 120 * n);
+    } else if (!mixed) {
         rep.bytes_moved = (long long)rep.iterations * (nnz * 9 + 24LL * T + 16 * n + 72 * n);
     } else {
         // per iteration: packed payload + column bytes + tile metadata + FP32
@@ -135,7 +149,8 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
     MF_TRY(true_residual(m, b, x, w, &rep.relres_true, s));
     if (h_status != 0) {
         rep.status = h_status;
-        set_last_error(h_status == MF_ERR_TIMEOUT ? "grid-wide wait exceeded its budget" : "CG breakdown");
+        set_last_error(h_status == MF_ERR_TIMEOUT ? "grid-wide wait exceeded its budget"
+                                                  : (bicg ? "BiCGSTAB breakdown" : "CG breakdown"));
         return (mf_status)h_status;
     }
     if (!a.fixed && !(rep.relres_true <= o.tol * (1.0 + 1e-6) || rep.relres <= o.tol)) {
@@ -148,6 +163,22 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
     }
     rep.status = MF_OK;
     return MF_OK;
+}
+
+mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,
+                   double *history, cudaStream_t s)
+{
+    return persistent_solve(false, m, b, x, o, rep, history, s);
+}
+
+mf_status bicgstab_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,
+                         double *history, cudaStream_t s)
+{
+    mf_solve_opts oo = o;
+    // BiCGSTAB has no checkpoint policies: dynamic policies run with the
+    // value-range (static) classes
+    if (oo.policy == MF_POLICY_RULE || oo.policy == MF_POLICY_LEARNED) oo.policy = MF_POLICY_STATIC;
+    return persistent_solve(true, m, b, x, oo, rep, history, s);
 }
 
 }  // namespace mf

@@ -24,7 +24,7 @@ struct ChunkRec {
 };
 
 // Persistent solver state kept in device memory between launches.
-enum : int { S_RHO = 0, S_BETA, S_NB, S_RMAX, S_ITERS, S_REFS, S_EXIT, S_RELRES, S_COUNT };
+enum : int { S_RHO = 0, S_BETA, S_NB, S_RMAX, S_ITERS, S_REFS, S_EXIT, S_RELRES, S_ALPHA, S_OMEGA, S_COUNT };
 // Why a launch returned.
 enum : int { EXIT_CONVERGED = 1, EXIT_MAXITER = 2, EXIT_BREAKDOWN = 3, EXIT_CHECKPOINT = 4 };
 
@@ -39,7 +39,8 @@ struct CgArgs {
     const double *b;
     double *xhi;                   // solution (FP64)
     void *r, *p0, *p1, *q, *xlo;   // vectors (FP64, or FP32 when mixed)
-    double *partials;              // [4][G] per-CTA dot partials
+    void *rhat, *v0, *v1, *t;      // BiCGSTAB: shadow residual, A p (double-buffered), A s
+    double *partials;              // [8][G] per-CTA dot partials
     unsigned long long *bar;       // sharded grid barrier counters (9 lines, 0 at launch)
     int *status;                   // device status word (mf_status codes)
     double *state;                 // [S_COUNT]
@@ -57,7 +58,7 @@ struct CgArgs {
 };
 
 struct SolverWork {
-    void *r, *p0, *p1, *q, *xlo;
+    void *r, *p0, *p1, *q, *xlo, *rhat, *v0, *v1, *t;
     double *ax, *partials, *rpart, *out, *state;
     unsigned long long *timing;
     unsigned long long *bar;
@@ -70,6 +71,8 @@ mf_status build_chunks(mf_matrix m, cudaStream_t s);
 mf_status refresh_chunk_payload(mf_matrix m, cudaStream_t s);
 int solver_grid(mf_matrix m, bool mixed);
 mf_status launch_cg(bool mixed, CgArgs &a, int G, cudaStream_t s);
+mf_status launch_bicgstab(bool mixed, CgArgs &a, int G, cudaStream_t s);
+int bicgstab_grid(mf_matrix m, bool mixed);
 mf_status true_residual(mf_matrix m, const double *b, const double *x, SolverWork &w, double *relres, cudaStream_t s);
 // payload.cu
 mf_status pack_payload(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s);

@@ -185,6 +185,49 @@ mf_status mf_bicgstab_solve_host(mf_matrix m, const double *b_host, double *x_ho
                                  const mf_solve_opts *opts, mf_solve_report *report);
 
 /* ---------------------------------------------------------------------- */
+/* Batched solves                                                          */
+/* ---------------------------------------------------------------------- */
+
+/* Many independent square systems of uneven size held on the device.  No
+ * reference counterpart (the reference solves one system per launch). */
+typedef struct mf_batch_s *mf_batch;
+
+typedef struct mf_batch_report {
+    int systems, failed;
+    long long iterations_total;
+    int iterations_max;
+    int refinements_total;
+    double relres_true_max;  /* largest FP64 ||b - A x|| / ||b|| over the systems */
+    double kernel_ms;        /* device time of the whole batch */
+    int lanes_per_row;       /* schedule used: lanes per row in the SpMV */
+    int cluster_ctas;        /* schedule used: CTAs per system (thread-block cluster) */
+    int status;
+} mf_batch_report;
+
+/* count systems; system s has n[s] rows, CSR rowptr[s] (rowptr[s][0] = 0),
+ * colidx[s] in [0, n[s]), val[s] (host pointers). */
+mf_status mf_batch_create(int count, const int *n, const int *const *rowptr, const int *const *colidx,
+                          const double *const *val, mf_batch *out);
+mf_status mf_batch_destroy(mf_batch bt);
+/* Total rows / entries, and the first row of each system in the stacked
+ * vectors b and x (host array owned by the handle). */
+mf_status mf_batch_info(mf_batch bt, long long *rows_total, long long *nnz_total, const long long **row_offsets);
+/* CG on every system (b, x: device arrays of rows_total doubles, stacked in
+ * system order).  One launch; use_graph != 0 captures the solve (queue reset,
+ * the batched kernel, the FP64 residual check) in a CUDA graph, replayed on
+ * later calls with the same buffers and options.  Policies: FP64 or any mixed
+ * policy (FP32 values/vectors, FP64 reliable updates). */
+mf_status mf_batch_cg_solve(mf_batch bt, const double *b, double *x, const mf_solve_opts *opts, int use_graph,
+                            mf_batch_report *report, void *stream);
+/* Per-system iterations and FP64 true relative residuals of the last solve. */
+mf_status mf_batch_results(mf_batch bt, int *iterations, double *relres_true);
+/* Autotuner: times each schedule (lanes per row 4/8/16/32 x cluster size
+ * 1/2/4/8) on this batch, keeps the fastest on the handle. */
+mf_status mf_batch_tune(mf_batch bt, const double *b, double *x, const mf_solve_opts *opts, int *lanes_out,
+                        int *cluster_out, void *stream);
+mf_status mf_batch_set_schedule(mf_batch bt, int lanes, int cluster);
+
+/* ---------------------------------------------------------------------- */
 /* Matrix Market input and synthetic matrices                              */
 /* ---------------------------------------------------------------------- */
 

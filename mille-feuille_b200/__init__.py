@@ -42,6 +42,16 @@ class SolveOpts(C.Structure):
                 ("wait_budget_s", C.c_double), ("record_history", C.c_int), ("phase_times", C.c_int)]
 
 
+class BatchReport(C.Structure):
+    _fields_ = [("systems", C.c_int), ("failed", C.c_int), ("iterations_total", C.c_longlong),
+                ("iterations_max", C.c_int), ("refinements_total", C.c_int), ("relres_true_max", C.c_double),
+                ("kernel_ms", C.c_double), ("lanes_per_row", C.c_int), ("cluster_ctas", C.c_int),
+                ("status", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class SolveReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("refinements", C.c_int), ("relres", C.c_double),
                 ("relres_true", C.c_double), ("kernel_ms", C.c_double), ("bytes_moved", C.c_longlong),
@@ -100,6 +110,13 @@ def lib() -> C.CDLL:
         L.mf_synth_xstar.argtypes = [C.c_uint64, C.c_int, vp]
         L.mf_synth_random_spd_size.argtypes = [C.c_uint64]
         L.mf_synth_random_spd_size.restype = C.c_int
+        L.mf_batch_create.argtypes = [C.c_int, vp, vp, vp, vp, C.POINTER(vp)]
+        L.mf_batch_destroy.argtypes = [vp]
+        L.mf_batch_info.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), vp]
+        L.mf_batch_cg_solve.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.c_int, C.POINTER(BatchReport), vp]
+        L.mf_batch_results.argtypes = [vp, vp, vp]
+        L.mf_batch_tune.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(C.c_int), C.POINTER(C.c_int), vp]
+        L.mf_batch_set_schedule.argtypes = [vp, C.c_int, C.c_int]
         gen = [ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp)]
         L.mf_synth_laplace2d.argtypes = [C.c_int, C.c_int] + gen
         L.mf_synth_poisson3d_scaled.argtypes = [C.c_int, C.c_uint64] + gen
@@ -258,3 +275,56 @@ class Matrix:
         if st not in (MF_OK, 6):
             check(st)
         return x, rep
+
+
+class Batch:
+    """Many independent systems solved by one batched launch (mf_batch)."""
+
+    def __init__(self, systems):
+        self.systems = list(systems)
+        cnt = len(self.systems)
+        n = np.array([A.n_rows for A in self.systems], np.int32)
+        self._keep = [(A.rowptr, A.colidx, A.val) for A in self.systems]
+        rp = (C.c_void_p * cnt)(*[A.rowptr.ctypes.data for A in self.systems])
+        ci = (C.c_void_p * cnt)(*[A.colidx.ctypes.data for A in self.systems])
+        va = (C.c_void_p * cnt)(*[A.val.ctypes.data for A in self.systems])
+        h = C.c_void_p()
+        check(lib().mf_batch_create(cnt, n.ctypes.data, rp, ci, va, C.byref(h)))
+        self.h = h
+        self.n = n
+        self.offsets = np.concatenate([[0], np.cumsum(n.astype(np.int64))])
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mf_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stack(self, parts):
+        return np.ascontiguousarray(np.concatenate(parts), np.float64)
+
+    def split(self, v):
+        return [v[self.offsets[k]:self.offsets[k + 1]] for k in range(len(self.systems))]
+
+    def solve_device(self, db_ptr, dx_ptr, use_graph=1, stream=None, **opts):
+        rep = BatchReport()
+        o = solve_opts(**opts)
+        st = lib().mf_batch_cg_solve(self.h, db_ptr, dx_ptr, C.byref(o), use_graph, C.byref(rep), stream)
+        return st, rep
+
+    def results(self):
+        it = np.zeros(len(self.systems), np.int32)
+        rr = np.zeros(len(self.systems), np.float64)
+        check(lib().mf_batch_results(self.h, it.ctypes.data, rr.ctypes.data))
+        return it, rr
+
+    def tune(self, db_ptr, dx_ptr, **opts):
+        o = solve_opts(**opts)
+        la, cl = C.c_int(), C.c_int()
+        check(lib().mf_batch_tune(self.h, db_ptr, dx_ptr, C.byref(o), C.byref(la), C.byref(cl), None))
+        return la.value, cl.value

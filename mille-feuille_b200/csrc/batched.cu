@@ -1,0 +1,640 @@
+// batched.cu -- many independent CG solves of uneven size in one launch.
+//
+// No reference counterpart: the reference solves one system per launch.
+// Design for B200: the systems are sorted by size and handed out by a device
+// work queue to thread-block clusters; a cluster of C CTAs solves one system
+// at a time.  The system's rows are split across the cluster's CTAs, the
+// SpMV reads the row-major execution layout of the system (entries of a row
+// in the tile order of the reference format, which for the random systems of
+// this workload is column order), several lanes per row, and every dot
+// product is reduced through distributed shared memory with a hardware
+// cluster barrier -- no grid-wide synchronisation, so small systems cost no
+// more than their own iterations.  Each cluster keeps iterating until its
+// system reaches the tolerance, then takes the next system.  Mixed policy:
+// FP32 values and vectors, FP32 accumulation, FP64 dot products, and FP64
+// reliable updates from the FP64 values, as in the single-system solver.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include <type_traits>
+
+#include "mf_internal.h"
+
+namespace cg = cooperative_groups;
+
+struct mf_batch_s {
+    int count = 0;
+    long long rows_total = 0, nnz_total = 0;
+    std::vector<int> n;           // rows per system (caller order)
+    std::vector<long long> row0;  // first row of each system (caller order)
+    int *d_order = nullptr;       // systems by descending size
+    long long *d_row0 = nullptr, *d_nz0 = nullptr;
+    int *d_n = nullptr;
+    int *d_rowptr = nullptr;      // per system, relative to the system's first entry
+    int *d_col = nullptr;
+    double *d_val = nullptr;
+    float *d_val32 = nullptr;
+    // per-system results
+    int *d_iters = nullptr, *d_refs = nullptr, *d_status = nullptr;
+    double *d_relres = nullptr;
+    void *work = nullptr;
+    size_t work_bytes = 0;
+    int *d_queue = nullptr;
+    // CUDA graph of the last solve configuration
+    cudaGraphExec_t graph = nullptr;
+    const void *graph_b = nullptr;
+    void *graph_x = nullptr;
+    int graph_key[6] = {0, 0, 0, 0, 0, 0};
+    int tuned_lanes = 0, tuned_cluster = 0;
+};
+
+namespace mf {
+namespace {
+
+constexpr int BNT = 256;
+
+struct BatchArgs {
+    int count;
+    const int *order;
+    const int *n;
+    const long long *row0, *nz0;
+    const int *rowptr, *col;
+    const double *val;
+    const float *val32;
+    const double *b;
+    double *x;
+    void *r, *p0, *p1, *q, *xlo;  // workspace vectors (rows_total each)
+    int *queue;
+    int *iters, *refs, *status;
+    double *relres;
+    int maxiter;
+    double tol;
+    double delta;
+};
+
+// Deterministic cluster-wide sum: each CTA reduces its threads in a fixed
+// tree, publishes the value in its shared memory, and after the cluster
+// barrier every CTA adds the CTAs' values in rank order.
+__device__ __forceinline__ double cluster_sum(cg::cluster_group &cl, double v, double *slot, double *s_warp)
+{
+    const double c = block_sum<BNT>(v, s_warp);
+    if (threadIdx.x == 0) *slot = c;
+    cl.sync();
+    double s = 0.0;
+    const unsigned ncta = cl.num_blocks();
+    for (unsigned k = 0; k < ncta; k++) s += *cl.map_shared_rank(slot, k);
+    return s;
+}
+
+// L lanes per row: lanes stride over the row's entries; the partials are
+// combined with a fixed xor tree, so every run gives the same bits.
+template <int L, bool MIX, class Src>
+__device__ __forceinline__ double row_dot(const int *__restrict__ rp, const int *__restrict__ col,
+                                          const double *__restrict__ val, const float *__restrict__ val32, int i,
+                                          int lane, Src src)
+{
+    const int a = (i >= 0) ? rp[i] : 0, e = (i >= 0) ? rp[i + 1] : 0;
+    double s = 0.0;
+    float sf = 0.0f;
+    for (int k = a + lane; k < e; k += L) {
+        if (MIX) sf = fmaf(__ldcs(val32 + k), (float)src(__ldcs(col + k)), sf);
+        else s = fma(__ldcs(val + k), (double)src(__ldcs(col + k)), s);
+    }
+    if (MIX) s = (double)sf;
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, L);
+    return s;
+}
+
+template <int L, bool MIX>
+__global__ void __launch_bounds__(BNT) k_batched_cg(BatchArgs a)
+{
+    using VT = typename std::conditional<MIX, float, double>::type;
+    cg::cluster_group cl = cg::this_cluster();
+    __shared__ double s_warp[BNT / 32];
+    __shared__ double s_slot[4];
+    __shared__ int s_sys;
+    const unsigned rank = cl.block_rank(), ncta = cl.num_blocks();
+    const int tid = threadIdx.x;
+    const int lane = tid % L, grp = tid / L;
+    constexpr int GPB = BNT / L;  // row groups per CTA
+    for (;;) {
+        if (rank == 0 && tid == 0) s_sys = atomicAdd(a.queue, 1);
+        cl.sync();
+        const int qi = *cl.map_shared_rank(&s_sys, 0);
+        cl.sync();  // every CTA has read the index before rank 0 writes the next
+        if (qi >= a.count) break;
+        const int sys = a.order[qi];
+        const int n = a.n[sys];
+        const long long r0 = a.row0[sys], z0 = a.nz0[sys];
+        const int *rp = a.rowptr + r0 + sys;  // n+1 entries per system
+        const int *col = a.col + z0;
+        const double *val = a.val + z0;
+        const float *val32 = a.val32 + z0;
+        const double *b = a.b + r0;
+        double *x = a.x + r0;
+        VT *r = (VT *)a.r + r0, *q = (VT *)a.q + r0, *xlo = (VT *)a.xlo + r0;
+        VT *pb[2] = {(VT *)a.p0 + r0, (VT *)a.p1 + r0};
+        // this CTA's rows
+        const int per = (n + ncta - 1) / ncta;
+        const int ra = min(n, (int)rank * per), rb = min(n, ra + per);
+        double lb = 0.0, lr = 0.0;
+        for (int i = ra + tid; i < rb; i += BNT) {
+            const double bv = b[i];
+            const VT rv = (VT)bv;
+            x[i] = 0.0;
+            r[i] = rv;
+            pb[0][i] = (VT)0;
+            if (MIX) xlo[i] = (VT)0;
+            lb += bv * bv;
+            lr += (double)rv * (double)rv;
+        }
+        const double bb = cluster_sum(cl, lb, &s_slot[0], s_warp);
+        double rho = MIX ? cluster_sum(cl, lr, &s_slot[1], s_warp) : bb;
+        const double nb = sqrt(bb) > 0.0 ? sqrt(bb) : 1.0;
+        double beta = 0.0, rmax = sqrt(rho), relres = sqrt(rho) / nb;
+        int it = 0, refs = 0, status = MF_OK;
+        while (true) {
+            if (sqrt(rho) <= a.tol * nb) break;
+            if (it >= a.maxiter) {
+                status = MF_ERR_NOT_CONVERGED;
+                break;
+            }
+            const VT *pold = pb[it & 1];
+            VT *pnew = pb[(it & 1) ^ 1];
+            const VT bt = (VT)beta;
+            const VT *rr = r;
+            auto psrc = [=](int c) -> VT {
+                if constexpr (MIX) return fmaf(bt, pold[c], rr[c]);
+                else return fma(bt, pold[c], rr[c]);
+            };
+            double loc = 0.0;
+            // the trip count is the same for every lane (shuffles inside)
+            for (int base = ra; base < rb; base += GPB) {
+                const int i = base + grp < rb ? base + grp : -1;
+                const double y = row_dot<L, MIX>(rp, col, val, val32, i, lane, psrc);
+                if (lane == 0 && i >= 0) {
+                    const VT pn = psrc(i);
+                    pnew[i] = pn;
+                    q[i] = (VT)y;
+                    loc += (double)pn * (double)(VT)y;
+                }
+            }
+            const double pq = cluster_sum(cl, loc, &s_slot[2], s_warp);
+            if (!(pq != 0.0) || !isfinite(pq)) {
+                status = MF_ERR_BREAKDOWN;
+                break;
+            }
+            const double alpha = rho / pq;
+            loc = 0.0;
+            for (int i = ra + tid; i < rb; i += BNT) {
+                if (MIX) {
+                    xlo[i] = fmaf((float)alpha, (float)pnew[i], (float)xlo[i]);
+                    const float ri = fmaf(-(float)alpha, (float)q[i], (float)r[i]);
+                    r[i] = ri;
+                    loc += (double)ri * (double)ri;
+                } else {
+                    x[i] = fma(alpha, (double)pnew[i], x[i]);
+                    const double ri = fma(-alpha, (double)q[i], (double)r[i]);
+                    r[i] = ri;
+                    loc += ri * ri;
+                }
+            }
+            double rho_new = cluster_sum(cl, loc, &s_slot[3], s_warp);
+            it++;
+            if (MIX && (sqrt(rho_new) <= a.delta * rmax || sqrt(rho_new) <= a.tol * nb)) {
+                for (int i = ra + tid; i < rb; i += BNT) {
+                    x[i] += (double)xlo[i];
+                    xlo[i] = (VT)0;
+                }
+                cl.sync();
+                loc = 0.0;
+                const double *xh = x;
+                auto xsrc = [=](int c) -> double { return xh[c]; };
+                for (int base = ra; base < rb; base += GPB) {
+                    const int i = base + grp < rb ? base + grp : -1;
+                    const double y = row_dot<L, false>(rp, col, val, val32, i, lane, xsrc);
+                    if (lane == 0 && i >= 0) {
+                        const VT rv = (VT)(b[i] - y);
+                        r[i] = rv;
+                        loc += (double)rv * (double)rv;
+                    }
+                }
+                rho_new = cluster_sum(cl, loc, &s_slot[1], s_warp);
+                rmax = sqrt(rho_new);
+                refs++;
+            }
+            beta = rho_new / rho;
+            rho = rho_new;
+            relres = sqrt(rho) / nb;
+        }
+        if (MIX && status != MF_OK) {
+            for (int i = ra + tid; i < rb; i += BNT) x[i] += (double)xlo[i];
+        }
+        if (rank == 0 && tid == 0) {
+            a.iters[sys] = it;
+            a.refs[sys] = refs;
+            a.status[sys] = status;
+            a.relres[sys] = relres;
+        }
+        cl.sync();  // the cluster's last writes land before the next system
+    }
+}
+
+template <int L, bool MIX>
+mf_status launch_batched(const BatchArgs &a, int cluster, cudaStream_t s)
+{
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(BNT);
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    // enough clusters to fill the GPU (the work queue balances them)
+    int per = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batched_cg<L, MIX>, BNT, 0);
+    int ctas = sms * (per > 0 ? per : 1);
+    ctas = (ctas / cluster) * cluster;
+    const int want = a.count * cluster;
+    if (ctas > want) ctas = want;
+    if (ctas < cluster) ctas = cluster;
+    cfg.gridDim = dim3(ctas);
+    note_launch();
+    MF_CUDA(cudaLaunchKernelEx(&cfg, k_batched_cg<L, MIX>, a));
+    return MF_OK;
+}
+
+template <bool MIX>
+mf_status launch_batched_l(int lanes, const BatchArgs &a, int cluster, cudaStream_t s)
+{
+    switch (lanes) {
+    case 4: return launch_batched<4, MIX>(a, cluster, s);
+    case 8: return launch_batched<8, MIX>(a, cluster, s);
+    case 16: return launch_batched<16, MIX>(a, cluster, s);
+    default: return launch_batched<32, MIX>(a, cluster, s);
+    }
+}
+
+__global__ void k_batch_resid(int count, const int *n, const long long *row0, const long long *nz0,
+                              const int *rowptr, const int *col, const double *val, const double *b, const double *x,
+                              double *out)
+{
+    // one CTA per system: ||b - A x|| / ||b|| in FP64
+    __shared__ double s_warp[8];
+    for (int sys = blockIdx.x; sys < count; sys += gridDim.x) {
+        const int nn = n[sys];
+        const long long r0 = row0[sys], z0 = nz0[sys];
+        const int *rp = rowptr + r0 + sys;
+        double rr = 0.0, bb = 0.0;
+        for (int i = threadIdx.x; i < nn; i += blockDim.x) {
+            double y = 0.0;
+            for (int k = rp[i]; k < rp[i + 1]; k++) y += val[z0 + k] * x[r0 + col[z0 + k]];
+            const double d = b[r0 + i] - y;
+            rr += d * d;
+            bb += b[r0 + i] * b[r0 + i];
+        }
+        rr = block_sum<256>(rr, s_warp);
+        bb = block_sum<256>(bb, s_warp);
+        if (threadIdx.x == 0) out[sys] = bb > 0 ? sqrt(rr) / sqrt(bb) : sqrt(rr);
+        __syncthreads();
+    }
+}
+
+__global__ void k_to_f32(long long n, const double *in, float *out)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+
+}  // namespace
+}  // namespace mf
+
+using namespace mf;
+
+extern "C" {
+
+mf_status mf_batch_create(int count, const int *n, const int *const *rowptr, const int *const *colidx,
+                          const double *const *val, mf_batch *out)
+{
+    if (!out || count <= 0 || !n || !rowptr || !colidx || !val) return MF_ERR_INVALID_ARG;
+    *out = nullptr;
+    mf_batch bt = new mf_batch_s();
+    bt->count = count;
+    bt->n.assign(n, n + count);
+    std::vector<long long> row0(count), nz0(count);
+    long long rows = 0, nz = 0;
+    for (int s = 0; s < count; s++) {
+        if (n[s] <= 0 || !rowptr[s] || rowptr[s][0] != 0) {
+            delete bt;
+            set_last_error("mf_batch_create: system %d has no rows or rowptr[0] != 0", s);
+            return MF_ERR_INVALID_ARG;
+        }
+        row0[s] = rows;
+        nz0[s] = nz;
+        rows += n[s];
+        nz += rowptr[s][n[s]];
+    }
+    bt->rows_total = rows;
+    bt->nnz_total = nz;
+    bt->row0 = row0;
+    // host staging of the concatenated CSR (validated)
+    std::vector<int> hrp((size_t)rows + count), hcol((size_t)nz);
+    std::vector<double> hval((size_t)nz);
+    for (int s = 0; s < count; s++) {
+        memcpy(&hrp[row0[s] + s], rowptr[s], sizeof(int) * (n[s] + 1));
+        const int e = rowptr[s][n[s]];
+        for (int k = 0; k < e; k++) {
+            const int c = colidx[s][k];
+            if (c < 0 || c >= n[s]) {
+                delete bt;
+                set_last_error("mf_batch_create: system %d column %d outside [0, %d)", s, c, n[s]);
+                return MF_ERR_INVALID_ARG;
+            }
+        }
+        memcpy(&hcol[nz0[s]], colidx[s], sizeof(int) * e);
+        memcpy(&hval[nz0[s]], val[s], sizeof(double) * e);
+    }
+    std::vector<int> order(count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return n[a] > n[b]; });
+    auto fail = [&](cudaError_t e) {
+        set_last_error("mf_batch_create: %s", cudaGetErrorString(e));
+        mf_batch_destroy(bt);
+        return e == cudaErrorMemoryAllocation ? MF_ERR_NO_MEMORY : MF_ERR_CUDA;
+    };
+    cudaError_t e = cudaSuccess;
+#define BT_ALLOC(p, bytes) \
+    if (e == cudaSuccess) e = cudaMalloc((void **)&(p), (bytes))
+    BT_ALLOC(bt->d_order, sizeof(int) * count);
+    BT_ALLOC(bt->d_n, sizeof(int) * count);
+    BT_ALLOC(bt->d_row0, sizeof(long long) * count);
+    BT_ALLOC(bt->d_nz0, sizeof(long long) * count);
+    BT_ALLOC(bt->d_rowptr, sizeof(int) * (rows + count));
+    BT_ALLOC(bt->d_col, sizeof(int) * (nz + 4));
+    BT_ALLOC(bt->d_val, sizeof(double) * (nz + 2));
+    BT_ALLOC(bt->d_val32, sizeof(float) * (nz + 4));
+    BT_ALLOC(bt->d_iters, sizeof(int) * count);
+    BT_ALLOC(bt->d_refs, sizeof(int) * count);
+    BT_ALLOC(bt->d_status, sizeof(int) * count);
+    BT_ALLOC(bt->d_relres, sizeof(double) * count * 2);
+    BT_ALLOC(bt->d_queue, sizeof(int) * 4);
+#undef BT_ALLOC
+    if (e == cudaSuccess) e = cudaMemcpy(bt->d_order, order.data(), sizeof(int) * count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bt->d_n, n, sizeof(int) * count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bt->d_row0, row0.data(), sizeof(long long) * count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bt->d_nz0, nz0.data(), sizeof(long long) * count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bt->d_rowptr, hrp.data(), sizeof(int) * (rows + count), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && nz) e = cudaMemcpy(bt->d_col, hcol.data(), sizeof(int) * nz, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && nz) e = cudaMemcpy(bt->d_val, hval.data(), sizeof(double) * nz, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && nz) {
+        k_to_f32<<<1184, 256>>>(nz, bt->d_val, bt->d_val32);
+        note_launch();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return fail(e);
+    *out = bt;
+    return MF_OK;
+}
+
+mf_status mf_batch_destroy(mf_batch bt)
+{
+    if (!bt) return MF_OK;
+    if (bt->graph) cudaGraphExecDestroy(bt->graph);
+    void *bufs[] = {bt->d_order, bt->d_n, bt->d_row0, bt->d_nz0, bt->d_rowptr, bt->d_col, bt->d_val, bt->d_val32,
+                    bt->d_iters, bt->d_refs, bt->d_status, bt->d_relres, bt->work, bt->d_queue};
+    for (void *p : bufs)
+        if (p) cudaFree(p);
+    delete bt;
+    return MF_OK;
+}
+
+mf_status mf_batch_info(mf_batch bt, long long *rows_total, long long *nnz_total, const long long **row_offsets)
+{
+    if (!bt) return MF_ERR_INVALID_ARG;
+    if (rows_total) *rows_total = bt->rows_total;
+    if (nnz_total) *nnz_total = bt->nnz_total;
+    if (row_offsets) *row_offsets = bt->row0.data();
+    return MF_OK;
+}
+
+static mf_status batch_work(mf_batch bt, bool mixed)
+{
+    const size_t rows = (size_t)bt->rows_total + 16;
+    const size_t need = rows * 8 * 5 + 1024;
+    (void)mixed;
+    if (bt->work_bytes >= need) return MF_OK;
+    if (bt->work) cudaFree(bt->work);
+    bt->work = nullptr;
+    bt->work_bytes = 0;
+    MF_CUDA(cudaMalloc(&bt->work, need));
+    bt->work_bytes = need;
+    return MF_OK;
+}
+
+static mf_status batch_enqueue(mf_batch bt, const double *b, double *x, const mf_solve_opts &o, int lanes,
+                               int cluster, cudaStream_t s)
+{
+    const bool mixed = o.policy != MF_POLICY_FP64;
+    MF_TRY(batch_work(bt, mixed));
+    const size_t rows = (size_t)bt->rows_total + 16;
+    char *w = (char *)bt->work;
+    BatchArgs a;
+    a.count = bt->count;
+    a.order = bt->d_order;
+    a.n = bt->d_n;
+    a.row0 = bt->d_row0;
+    a.nz0 = bt->d_nz0;
+    a.rowptr = bt->d_rowptr;
+    a.col = bt->d_col;
+    a.val = bt->d_val;
+    a.val32 = bt->d_val32;
+    a.b = b;
+    a.x = x;
+    a.r = w;
+    a.p0 = w + rows * 8;
+    a.p1 = w + rows * 16;
+    a.q = w + rows * 24;
+    a.xlo = w + rows * 32;
+    a.queue = bt->d_queue;
+    a.iters = bt->d_iters;
+    a.refs = bt->d_refs;
+    a.status = bt->d_status;
+    a.relres = bt->d_relres;
+    a.maxiter = o.maxiter;
+    a.tol = o.tol;
+    a.delta = (o.refine_delta > 0 && o.refine_delta < 1) ? o.refine_delta : 0.1;
+    MF_CUDA(cudaMemsetAsync(bt->d_queue, 0, sizeof(int), s));
+    if (mixed) MF_TRY(launch_batched_l<true>(lanes, a, cluster, s));
+    else MF_TRY(launch_batched_l<false>(lanes, a, cluster, s));
+    k_batch_resid<<<std::min(bt->count, 1184), 256, 0, s>>>(bt->count, bt->d_n, bt->d_row0, bt->d_nz0, bt->d_rowptr,
+                                                           bt->d_col, bt->d_val, b, x, bt->d_relres + bt->count);
+    note_launch();
+    MF_CUDA(cudaGetLastError());
+    return MF_OK;
+}
+
+mf_status mf_batch_tune(mf_batch bt, const double *b, double *x, const mf_solve_opts *opts, int *lanes_out,
+                        int *cluster_out, void *stream);
+
+mf_status mf_batch_cg_solve(mf_batch bt, const double *b, double *x, const mf_solve_opts *opts, int use_graph,
+                            mf_batch_report *report, void *stream)
+{
+    if (!bt || !b || !x) return MF_ERR_INVALID_ARG;
+    mf_solve_opts o;
+    mf_solve_opts_default(&o);
+    if (opts) o = *opts;
+    if (o.tol <= 0 || o.maxiter <= 0) {
+        set_last_error("batched CG needs tol > 0 and maxiter > 0");
+        return MF_ERR_INVALID_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    int lanes = bt->tuned_lanes ? bt->tuned_lanes : 8;
+    int cluster = bt->tuned_cluster ? bt->tuned_cluster : 4;
+    if (const char *e = getenv("MF_BATCH_LANES")) lanes = atoi(e);
+    if (const char *e = getenv("MF_BATCH_CLUSTER")) cluster = atoi(e);
+    if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) lanes = 8;
+    if (cluster < 1 || cluster > 8) cluster = 4;
+    cudaEvent_t e0, e1;
+    MF_CUDA(cudaEventCreate(&e0));
+    MF_CUDA(cudaEventCreate(&e1));
+    MF_CUDA(cudaEventRecord(e0, s));
+    const int key[6] = {lanes, cluster, o.policy, (int)(o.tol * 1e15), o.maxiter, 1};
+    if (use_graph) {
+        // one graph per (buffers, configuration): replayed on later calls
+        if (!bt->graph || bt->graph_b != b || bt->graph_x != x || memcmp(key, bt->graph_key, sizeof(key))) {
+            if (bt->graph) cudaGraphExecDestroy(bt->graph);
+            bt->graph = nullptr;
+            cudaStream_t cs;
+            MF_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+            cudaGraph_t g;
+            MF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+            mf_status st = batch_enqueue(bt, b, x, o, lanes, cluster, cs);
+            cudaError_t ce = cudaStreamEndCapture(cs, &g);
+            cudaStreamDestroy(cs);
+            if (st != MF_OK) return st;
+            MF_CUDA(ce);
+            MF_CUDA(cudaGraphInstantiate(&bt->graph, g, 0));
+            cudaGraphDestroy(g);
+            bt->graph_b = b;
+            bt->graph_x = x;
+            memcpy(bt->graph_key, key, sizeof(key));
+        }
+        MF_CUDA(cudaGraphLaunch(bt->graph, s));
+    } else {
+        MF_TRY(batch_enqueue(bt, b, x, o, lanes, cluster, s));
+    }
+    MF_CUDA(cudaEventRecord(e1, s));
+    MF_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const int count = bt->count;
+    std::vector<int> it(count), rf(count), stt(count);
+    std::vector<double> rr(count * 2);
+    MF_CUDA(cudaMemcpy(it.data(), bt->d_iters, sizeof(int) * count, cudaMemcpyDeviceToHost));
+    MF_CUDA(cudaMemcpy(rf.data(), bt->d_refs, sizeof(int) * count, cudaMemcpyDeviceToHost));
+    MF_CUDA(cudaMemcpy(stt.data(), bt->d_status, sizeof(int) * count, cudaMemcpyDeviceToHost));
+    MF_CUDA(cudaMemcpy(rr.data(), bt->d_relres, sizeof(double) * count * 2, cudaMemcpyDeviceToHost));
+    mf_status worst = MF_OK;
+    long long iters = 0;
+    double maxrr = 0;
+    int maxit = 0, refs = 0, failed = 0;
+    for (int k = 0; k < count; k++) {
+        iters += it[k];
+        maxit = std::max(maxit, it[k]);
+        refs += rf[k];
+        maxrr = std::max(maxrr, rr[count + k]);
+        if (stt[k] != MF_OK) {
+            failed++;
+            if (worst == MF_OK) worst = (mf_status)stt[k];
+        }
+    }
+    if (report) {
+        report->systems = count;
+        report->failed = failed;
+        report->iterations_total = iters;
+        report->iterations_max = maxit;
+        report->refinements_total = refs;
+        report->relres_true_max = maxrr;
+        report->kernel_ms = ms;
+        report->lanes_per_row = lanes;
+        report->cluster_ctas = cluster;
+        report->status = worst;
+    }
+    if (worst != MF_OK) set_last_error("%d of %d systems did not converge", failed, count);
+    return worst;
+}
+
+mf_status mf_batch_results(mf_batch bt, int *iterations, double *relres_true)
+{
+    if (!bt) return MF_ERR_INVALID_ARG;
+    if (iterations) MF_CUDA(cudaMemcpy(iterations, bt->d_iters, sizeof(int) * bt->count, cudaMemcpyDeviceToHost));
+    if (relres_true)
+        MF_CUDA(cudaMemcpy(relres_true, bt->d_relres + bt->count, sizeof(double) * bt->count, cudaMemcpyDeviceToHost));
+    return MF_OK;
+}
+
+// Autotuner: times every (lanes per row, cluster size) pair on this batch
+// and keeps the fastest; the choice is returned and kept on the handle.
+mf_status mf_batch_tune(mf_batch bt, const double *b, double *x, const mf_solve_opts *opts, int *lanes_out,
+                        int *cluster_out, void *stream)
+{
+    if (!bt || !b || !x) return MF_ERR_INVALID_ARG;
+    mf_solve_opts o;
+    mf_solve_opts_default(&o);
+    if (opts) o = *opts;
+    const int lanes_c[] = {4, 8, 16, 32};
+    const int clus_c[] = {1, 2, 4, 8};
+    float best = 1e30f;
+    int bl = 8, bc = 4;
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int li : lanes_c)
+        for (int ci : clus_c) {
+            cudaEvent_t e0, e1;
+            MF_CUDA(cudaEventCreate(&e0));
+            MF_CUDA(cudaEventCreate(&e1));
+            MF_CUDA(cudaEventRecord(e0, s));
+            mf_status st = batch_enqueue(bt, b, x, o, li, ci, s);
+            MF_CUDA(cudaEventRecord(e1, s));
+            MF_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            if (st == MF_OK && ms < best) {
+                best = ms;
+                bl = li;
+                bc = ci;
+            }
+        }
+    bt->tuned_lanes = bl;
+    bt->tuned_cluster = bc;
+    if (lanes_out) *lanes_out = bl;
+    if (cluster_out) *cluster_out = bc;
+    return MF_OK;
+}
+
+mf_status mf_batch_set_schedule(mf_batch bt, int lanes, int cluster)
+{
+    if (!bt || (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) || cluster < 1 || cluster > 8)
+        return MF_ERR_INVALID_ARG;
+    bt->tuned_lanes = lanes;
+    bt->tuned_cluster = cluster;
+    return MF_OK;
+}
+
+}  // extern "C"

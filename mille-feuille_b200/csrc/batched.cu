@@ -246,11 +246,35 @@ __global__ void __launch_bounds__(BNT) k_batched_cg(BatchArgs a)
 }
 
 template <int L, bool MIX>
-mf_status launch_batched(const BatchArgs &a, int cluster, cudaStream_t s)
+int batched_ctas(int count, int cluster)
 {
-    int dev = 0, sms = 0;
+    int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batched_cg<L, MIX>, BNT, 0);
+    int ctas = sms * (per > 0 ? per : 1);
+    ctas = (ctas / cluster) * cluster;
+    const int want = count * cluster;
+    if (ctas > want) ctas = want;
+    if (ctas < cluster) ctas = cluster;
+    return ctas;
+}
+
+template <bool MIX>
+int batched_ctas_l(int lanes, int count, int cluster)
+{
+    switch (lanes) {
+    case 4: return batched_ctas<4, MIX>(count, cluster);
+    case 8: return batched_ctas<8, MIX>(count, cluster);
+    case 16: return batched_ctas<16, MIX>(count, cluster);
+    default: return batched_ctas<32, MIX>(count, cluster);
+    }
+}
+
+// ctas: computed before any stream capture (batched_ctas)
+template <int L, bool MIX>
+mf_status launch_batched(const BatchArgs &a, int cluster, int ctas, cudaStream_t s)
+{
     cudaLaunchConfig_t cfg;
     memset(&cfg, 0, sizeof(cfg));
     cudaLaunchAttribute attr[1];
@@ -263,13 +287,6 @@ mf_status launch_batched(const BatchArgs &a, int cluster, cudaStream_t s)
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     // enough clusters to fill the GPU (the work queue balances them)
-    int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batched_cg<L, MIX>, BNT, 0);
-    int ctas = sms * (per > 0 ? per : 1);
-    ctas = (ctas / cluster) * cluster;
-    const int want = a.count * cluster;
-    if (ctas > want) ctas = want;
-    if (ctas < cluster) ctas = cluster;
     cfg.gridDim = dim3(ctas);
     note_launch();
     MF_CUDA(cudaLaunchKernelEx(&cfg, k_batched_cg<L, MIX>, a));
@@ -277,13 +294,13 @@ mf_status launch_batched(const BatchArgs &a, int cluster, cudaStream_t s)
 }
 
 template <bool MIX>
-mf_status launch_batched_l(int lanes, const BatchArgs &a, int cluster, cudaStream_t s)
+mf_status launch_batched_l(int lanes, const BatchArgs &a, int cluster, int ctas, cudaStream_t s)
 {
     switch (lanes) {
-    case 4: return launch_batched<4, MIX>(a, cluster, s);
-    case 8: return launch_batched<8, MIX>(a, cluster, s);
-    case 16: return launch_batched<16, MIX>(a, cluster, s);
-    default: return launch_batched<32, MIX>(a, cluster, s);
+    case 4: return launch_batched<4, MIX>(a, cluster, ctas, s);
+    case 8: return launch_batched<8, MIX>(a, cluster, ctas, s);
+    case 16: return launch_batched<16, MIX>(a, cluster, ctas, s);
+    default: return launch_batched<32, MIX>(a, cluster, ctas, s);
     }
 }
 
@@ -444,11 +461,12 @@ static mf_status batch_work(mf_batch bt, bool mixed)
     return MF_OK;
 }
 
+// Enqueues one batched solve.  Nothing here allocates or queries the device:
+// batch_work() and batched_ctas_l() run before (outside any stream capture).
 static mf_status batch_enqueue(mf_batch bt, const double *b, double *x, const mf_solve_opts &o, int lanes,
-                               int cluster, cudaStream_t s)
+                               int cluster, int ctas, cudaStream_t s)
 {
     const bool mixed = o.policy != MF_POLICY_FP64;
-    MF_TRY(batch_work(bt, mixed));
     const size_t rows = (size_t)bt->rows_total + 16;
     char *w = (char *)bt->work;
     BatchArgs a;
@@ -477,8 +495,8 @@ static mf_status batch_enqueue(mf_batch bt, const double *b, double *x, const mf
     a.tol = o.tol;
     a.delta = (o.refine_delta > 0 && o.refine_delta < 1) ? o.refine_delta : 0.1;
     MF_CUDA(cudaMemsetAsync(bt->d_queue, 0, sizeof(int), s));
-    if (mixed) MF_TRY(launch_batched_l<true>(lanes, a, cluster, s));
-    else MF_TRY(launch_batched_l<false>(lanes, a, cluster, s));
+    if (mixed) MF_TRY(launch_batched_l<true>(lanes, a, cluster, ctas, s));
+    else MF_TRY(launch_batched_l<false>(lanes, a, cluster, ctas, s));
     k_batch_resid<<<std::min(bt->count, 1184), 256, 0, s>>>(bt->count, bt->d_n, bt->d_row0, bt->d_nz0, bt->d_rowptr,
                                                            bt->d_col, bt->d_val, b, x, bt->d_relres + bt->count);
     note_launch();
@@ -507,6 +525,9 @@ mf_status mf_batch_cg_solve(mf_batch bt, const double *b, double *x, const mf_so
     if (const char *e = getenv("MF_BATCH_CLUSTER")) cluster = atoi(e);
     if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) lanes = 8;
     if (cluster < 1 || cluster > 8) cluster = 4;
+    const bool mixed = o.policy != MF_POLICY_FP64;
+    MF_TRY(batch_work(bt, mixed));
+    const int ctas = mixed ? batched_ctas_l<true>(lanes, bt->count, cluster) : batched_ctas_l<false>(lanes, bt->count, cluster);
     cudaEvent_t e0, e1;
     MF_CUDA(cudaEventCreate(&e0));
     MF_CUDA(cudaEventCreate(&e1));
@@ -521,11 +542,15 @@ mf_status mf_batch_cg_solve(mf_batch bt, const double *b, double *x, const mf_so
             MF_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
             cudaGraph_t g;
             MF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-            mf_status st = batch_enqueue(bt, b, x, o, lanes, cluster, cs);
+            mf_status st = batch_enqueue(bt, b, x, o, lanes, cluster, ctas, cs);
             cudaError_t ce = cudaStreamEndCapture(cs, &g);
             cudaStreamDestroy(cs);
-            if (st != MF_OK) return st;
-            MF_CUDA(ce);
+            if (st != MF_OK || ce != cudaSuccess) {
+                if (ce == cudaSuccess) cudaGraphDestroy(g);
+                cudaGetLastError();
+                if (st != MF_OK) return st;
+                MF_CUDA(ce);
+            }
             MF_CUDA(cudaGraphInstantiate(&bt->graph, g, 0));
             cudaGraphDestroy(g);
             bt->graph_b = b;
@@ -534,7 +559,7 @@ mf_status mf_batch_cg_solve(mf_batch bt, const double *b, double *x, const mf_so
         }
         MF_CUDA(cudaGraphLaunch(bt->graph, s));
     } else {
-        MF_TRY(batch_enqueue(bt, b, x, o, lanes, cluster, s));
+        MF_TRY(batch_enqueue(bt, b, x, o, lanes, cluster, ctas, s));
     }
     MF_CUDA(cudaEventRecord(e1, s));
     MF_CUDA(cudaEventSynchronize(e1));
@@ -602,13 +627,16 @@ mf_status mf_batch_tune(mf_batch bt, const double *b, double *x, const mf_solve_
     float best = 1e30f;
     int bl = 8, bc = 4;
     cudaStream_t s = (cudaStream_t)stream;
+    const bool mixed = o.policy != MF_POLICY_FP64;
+    MF_TRY(batch_work(bt, mixed));
     for (int li : lanes_c)
         for (int ci : clus_c) {
+            const int ctas = mixed ? batched_ctas_l<true>(li, bt->count, ci) : batched_ctas_l<false>(li, bt->count, ci);
             cudaEvent_t e0, e1;
             MF_CUDA(cudaEventCreate(&e0));
             MF_CUDA(cudaEventCreate(&e1));
             MF_CUDA(cudaEventRecord(e0, s));
-            mf_status st = batch_enqueue(bt, b, x, o, li, ci, s);
+            mf_status st = batch_enqueue(bt, b, x, o, li, ci, ctas, s);
             MF_CUDA(cudaEventRecord(e1, s));
             MF_CUDA(cudaEventSynchronize(e1));
             float ms = 0;

@@ -123,6 +123,14 @@ mf_status mf_encode_column_index(mf_matrix m, void *stream);
  * sequential sum over the row's entries, tiles added in column order. */
 mf_status mf_spmv(mf_matrix m, const double *x, double *y, void *stream);
 
+/* FP64 true relative residual ||b - A x|| / ||b|| of a square system (the
+ * reference's post-solve check, src/main-cg.cu:978-1011): out (device) gets
+ * out[0] = relative residual, out[1] = ||b - A x||, out[2] = ||b||.  Rows of
+ * A x in blockspmv_cpu's order; per-strip partials summed in a fixed order,
+ * so the value is identical on every call.  Scratch: 16 bytes per 16-row
+ * strip, allocated on the handle at the first call. */
+mf_status mf_residual_norm(mf_matrix m, const double *b, const double *x, double *out, void *stream);
+
 typedef enum mf_policy {
     MF_POLICY_FP64 = 0,    /* plain FP64 tiles and vectors */
     MF_POLICY_STATIC = 1,  /* value-range tile classes, FP32 accumulate,

@@ -66,6 +66,9 @@ struct mf_matrix_s {
     size_t pay_bytes = 0, pay_used = 0;
     int packed_policy = -1;
     int policy_loaded = 0;     // a learned policy is attached
+    // per-strip partials of mf_residual_norm
+    double *d_resid = nullptr;
+    size_t resid_bytes = 0;
     // device staging of b and x for the host-buffer solve entry points
     double *host_io = nullptr;
     size_t host_io_n = 0;
@@ -80,6 +83,9 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
 mf_status strip_partition(mf_matrix m, int ctas, cudaStream_t s);
 // spmv.cu
 mf_status spmv_fp64(const MfTiles &A, const double *x, double *y, cudaStream_t s);
+// residual.cu: per-strip partials (2 doubles per strip) then a fixed-order sum
+mf_status residual_norm(const MfTiles &A, const double *b, const double *x, double *part, double *out,
+                        cudaStream_t s);
 // workspace
 mf_status ensure_work(mf_matrix m, size_t bytes);
 }  // namespace mf

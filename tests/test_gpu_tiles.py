@@ -151,3 +151,26 @@ def test_gpu_config_sized_tiles_match_oracle(mf):
     finally:
         ol.free_oracle_tiles(t)
         M.close()
+
+
+@pytest.mark.parametrize("name", ["lap2d_32", "poisson3d_12", "convdiff_10", "ragged_rect", "empty_rows"])
+def test_gpu_residual_norm_matches_oracle(mf, mats, name):
+    """mf_residual_norm (the reference's FP64 post-solve check) against the
+    CPU oracle's sequential FP64 residual, on square test matrices."""
+    import torch
+
+    A = mats[name]
+    if A.n_rows != A.n_cols:
+        pytest.skip("square systems only")
+    M = mf.Matrix(host(mf, A))
+    rng = np.random.default_rng(3)
+    x = rng.uniform(-1, 1, A.n_cols)
+    b = rng.uniform(-1, 1, A.n_rows)
+    out = torch.zeros(3, dtype=torch.float64, device="cuda")
+    mf.check(mf.lib().mf_residual_norm(M.h, torch.from_numpy(b).cuda().data_ptr(),
+                                       torch.from_numpy(x).cuda().data_ptr(), out.data_ptr(), None))
+    got = out.cpu().numpy()
+    want = ol.oracle_true_relres(A, b, x)
+    assert abs(got[0] - want) <= 1e-13 * max(1.0, want)
+    assert abs(got[2] - np.linalg.norm(b)) <= 1e-12 * np.linalg.norm(b)
+    M.close()

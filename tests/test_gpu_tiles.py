@@ -167,8 +167,8 @@ def test_gpu_residual_norm_matches_oracle(mf, mats, name):
     x = rng.uniform(-1, 1, A.n_cols)
     b = rng.uniform(-1, 1, A.n_rows)
     out = torch.zeros(3, dtype=torch.float64, device="cuda")
-    mf.check(mf.lib().mf_residual_norm(M.h, torch.from_numpy(b).cuda().data_ptr(),
-                                       torch.from_numpy(x).cuda().data_ptr(), out.data_ptr(), None))
+    db, dx = torch.from_numpy(b).cuda(), torch.from_numpy(x).cuda()  # held alive across the call
+    mf.check(mf.lib().mf_residual_norm(M.h, db.data_ptr(), dx.data_ptr(), out.data_ptr(), None))
     got = out.cpu().numpy()
     want = ol.oracle_true_relres(A, b, x)
     assert abs(got[0] - want) <= 1e-13 * max(1.0, want)

@@ -131,6 +131,19 @@ mf_status mf_spmv(mf_matrix m, const double *x, double *y, void *stream);
  * strip, allocated on the handle at the first call. */
 mf_status mf_residual_norm(mf_matrix m, const double *b, const double *x, double *out, void *stream);
 
+/* Same result as mf_residual_norm, for callers that may not allocate device
+ * memory on this path (device memory sized once at start-up, memory owned by
+ * the caller's own allocator, or no tolerance for the device-wide
+ * synchronisation cudaMalloc/cudaFree can cause).  No counterpart in the
+ * reference.  It allocates nothing: its scratch is a fixed 1 MiB array in the
+ * library's device image, so it accepts matrices of at most 1,048,576 rows
+ * (65,536 strips) and rejects larger ones with MF_ERR_INVALID_ARG.  The first
+ * call on a device looks up that array's device address (once per device);
+ * make that first call before any stream capture.  All calls on a device
+ * share the array: calls that overlap on the GPU race and must be ordered by
+ * the caller. */
+mf_status mf_residual_norm_noalloc(mf_matrix m, const double *b, const double *x, double *out, void *stream);
+
 typedef enum mf_policy {
     MF_POLICY_FP64 = 0,    /* plain FP64 tiles and vectors */
     MF_POLICY_STATIC = 1,  /* value-range tile classes, FP32 accumulate,

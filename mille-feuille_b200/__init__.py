@@ -95,6 +95,7 @@ def lib() -> C.CDLL:
         L.mf_encode_column_index.argtypes = [vp, vp]
         L.mf_spmv.argtypes = [vp, vp, vp, vp]
         L.mf_residual_norm.argtypes = [vp, vp, vp, vp, vp]
+        L.mf_residual_norm_noalloc.argtypes = [vp, vp, vp, vp, vp]
         L.mf_solve_opts_default.argtypes = [C.POINTER(SolveOpts)]
         L.mf_solve_opts_default.restype = None
         L.mf_cg_solve.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport), vp, vp]

@@ -206,6 +206,41 @@ mf_status mf_bicgstab_solve_host(mf_matrix m, const double *b_host, double *x_ho
                                  const mf_solve_opts *opts, mf_solve_report *report);
 
 /* ---------------------------------------------------------------------- */
+/* Learned precision policy                                                */
+/* ---------------------------------------------------------------------- */
+
+/* A small MLP (16 tile features -> 32 -> 32 -> 4 classes int8-or-bypass /
+ * fp16 / fp32 / fp64; BF16 weights, FP32 accumulation) that picks every
+ * tile's class at each checkpoint of a MF_POLICY_LEARNED CG solve.  No
+ * reference counterpart: it replaces the reference's fixed rule
+ * (src/main-cg-mixed.cu:415-460), which stays available as MF_POLICY_RULE. */
+typedef struct mf_policy_s *mf_learned;
+
+int mf_policy_param_count(void);
+mf_status mf_policy_create(uint64_t seed, mf_learned *out);
+mf_status mf_policy_destroy(mf_learned p);
+/* Weights as float (BF16 values), layout W1[32][16], b1[32], W2[32][32],
+ * b2[32], W3[4][32], b3[4]. */
+mf_status mf_policy_get_params(mf_learned p, float *host, int count);
+mf_status mf_policy_set_params(mf_learned p, const float *host, int count);
+mf_status mf_policy_save(mf_learned p, const char *path);
+mf_status mf_policy_load(const char *path, mf_learned *out);
+/* Runs a plain FP64 CG solve of m (b on the device) and, every
+ * checkpoint_every iterations, adds (features, label) samples of about one
+ * tile in sample_stride to the training set (at most max_samples in all). */
+mf_status mf_policy_collect(mf_learned p, mf_matrix m, const double *b, int checkpoint_every, int sample_stride,
+                            long long max_samples, long long *samples_out);
+mf_status mf_policy_label_counts(mf_learned p, long long counts[4]);
+/* Adam on the softmax cross-entropy of the collected samples. */
+mf_status mf_policy_train(mf_learned p, int epochs, int batch, float lr, uint64_t seed, double *loss_first,
+                          double *loss_last);
+/* Gradient of the mean loss over n given samples (host X[n][16], Y[n]) at
+ * the current weights, without an update (for gradient checks). */
+mf_status mf_policy_eval_grad(mf_learned p, const float *X, const int *Y, int n, float *grad, double *loss);
+/* MF_POLICY_LEARNED solves of m use p (NULL detaches). */
+mf_status mf_matrix_attach_policy(mf_matrix m, mf_learned p);
+
+/* ---------------------------------------------------------------------- */
 /* Batched solves                                                          */
 /* ---------------------------------------------------------------------- */
 

@@ -119,6 +119,18 @@ def lib() -> C.CDLL:
         L.mf_batch_results.argtypes = [vp, vp, vp]
         L.mf_batch_tune.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(C.c_int), C.POINTER(C.c_int), vp]
         L.mf_batch_set_schedule.argtypes = [vp, C.c_int, C.c_int]
+        L.mf_policy_param_count.restype = C.c_int
+        L.mf_policy_create.argtypes = [C.c_uint64, C.POINTER(vp)]
+        L.mf_policy_destroy.argtypes = [vp]
+        L.mf_policy_get_params.argtypes = [vp, vp, C.c_int]
+        L.mf_policy_set_params.argtypes = [vp, vp, C.c_int]
+        L.mf_policy_save.argtypes = [vp, C.c_char_p]
+        L.mf_policy_load.argtypes = [C.c_char_p, C.POINTER(vp)]
+        L.mf_policy_collect.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_longlong, C.POINTER(C.c_longlong)]
+        L.mf_policy_label_counts.argtypes = [vp, vp]
+        L.mf_policy_train.argtypes = [vp, C.c_int, C.c_int, C.c_float, C.c_uint64, dp, dp]
+        L.mf_policy_eval_grad.argtypes = [vp, vp, vp, C.c_int, vp, dp]
+        L.mf_matrix_attach_policy.argtypes = [vp, vp]
         gen = [ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp)]
         L.mf_synth_laplace2d.argtypes = [C.c_int, C.c_int] + gen
         L.mf_synth_poisson3d_scaled.argtypes = [C.c_int, C.c_uint64] + gen
@@ -265,6 +277,11 @@ class Matrix:
     def encode_column_index(self):
         check(lib().mf_encode_column_index(self.h, None))
 
+    def attach_policy(self, policy):
+        """Uses `policy` (a Policy, or None to detach) for MF_POLICY_LEARNED."""
+        check(lib().mf_matrix_attach_policy(self.h, None if policy is None else policy.h))
+        self._policy = policy
+
     def solve_host(self, b, method="cg", **opts):
         """CG (or BiCGSTAB) with host b/x through mf_*_solve_host; returns
         (x, report)."""
@@ -330,3 +347,74 @@ class Batch:
         la, cl = C.c_int(), C.c_int()
         check(lib().mf_batch_tune(self.h, db_ptr, dx_ptr, C.byref(o), C.byref(la), C.byref(cl), None))
         return la.value, cl.value
+
+
+class Policy:
+    """The learned per-tile precision policy (mf_learned handle)."""
+
+    def __init__(self, seed=0, _handle=None):
+        if _handle is None:
+            _handle = C.c_void_p()
+            check(lib().mf_policy_create(seed, C.byref(_handle)))
+        self.h = _handle
+
+    @classmethod
+    def load(cls, path):
+        h = C.c_void_p()
+        check(lib().mf_policy_load(str(path).encode(), C.byref(h)))
+        return cls(_handle=h)
+
+    @staticmethod
+    def param_count():
+        return lib().mf_policy_param_count()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mf_policy_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        w = np.zeros(self.param_count(), np.float32)
+        check(lib().mf_policy_get_params(self.h, w.ctypes.data, w.size))
+        return w
+
+    def set_params(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        check(lib().mf_policy_set_params(self.h, w.ctypes.data, w.size))
+
+    def save(self, path):
+        check(lib().mf_policy_save(self.h, str(path).encode()))
+
+    def collect(self, matrix, b_dev_ptr, checkpoint_every=10, sample_stride=1, max_samples=1 << 20):
+        """Appends samples from an FP64 solve of matrix with device rhs; returns the sample count."""
+        n = C.c_longlong()
+        check(lib().mf_policy_collect(self.h, matrix.h, b_dev_ptr, checkpoint_every, sample_stride, max_samples,
+                                      C.byref(n)))
+        return n.value
+
+    def label_counts(self):
+        c = np.zeros(4, np.int64)
+        check(lib().mf_policy_label_counts(self.h, c.ctypes.data))
+        return c
+
+    def train(self, epochs=5, batch=1024, lr=3e-3, seed=0):
+        """Adam over the collected samples; returns (first batch loss, last epoch mean loss)."""
+        l0, l1 = C.c_double(), C.c_double()
+        check(lib().mf_policy_train(self.h, epochs, batch, lr, seed, C.byref(l0), C.byref(l1)))
+        return l0.value, l1.value
+
+    def eval_grad(self, X, Y):
+        """Mean cross-entropy loss and its gradient at the current weights."""
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.ascontiguousarray(Y, np.int32)
+        g = np.zeros(self.param_count(), np.float32)
+        loss = C.c_double()
+        check(lib().mf_policy_eval_grad(self.h, X.ctypes.data, Y.ctypes.data, len(Y), g.ctypes.data,
+                                        C.byref(loss)))
+        return loss.value, g

@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(NT, MINB) k_cg(CgArgs a)
         rho = rho_new;
         if (!MIX) relres_true = sqrt(rho) / nb;
         if (a.hist && g == 0 && threadIdx.x == 0) a.hist[it] = sqrt(rho) / nb;
-        if (refined && a.exit_on_refine) {
+        if ((refined && a.exit_on_refine) || (a.checkpoint_every > 0 && it % a.checkpoint_every == 0)) {
             exit_reason = EXIT_CHECKPOINT;
             break;
         }

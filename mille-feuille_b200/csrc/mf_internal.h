@@ -66,6 +66,11 @@ struct mf_matrix_s {
     size_t pay_bytes = 0, pay_used = 0;
     int packed_policy = -1;
     int policy_loaded = 0;     // a learned policy is attached
+    struct mf_policy_s *policy = nullptr;
+    void *d_pol = nullptr;     // policy workspace (static tile features, segment statistics)
+    size_t pol_bytes = 0;
+    int pol_static_ready = 0, pol_have_prev = 0;
+    float pol_prev_relres = 0.f;
     // per-strip partials of mf_residual_norm
     double *d_resid = nullptr;
     size_t resid_bytes = 0;

@@ -209,12 +209,3 @@ mf_status rule_working_classes(mf_matrix m, const void *p_new, const void *p_old
 }
 
 }  // namespace mf
-
-namespace mf {
-// Placeholder until the learned policy is loaded: keeps the current classes.
-mf_status learned_working_classes(mf_matrix, SolverWork &, const void *, const void *, unsigned char *, cudaStream_t)
-{
-    set_last_error("learned policy not loaded");
-    return MF_ERR_UNSUPPORTED;
-}
-}  // namespace mf

@@ -10,7 +10,8 @@
 namespace mf {
 
 static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, double *x, const mf_solve_opts &o,
-                                  mf_solve_report &rep, double *history, cudaStream_t s)
+                                  mf_solve_report &rep, double *history, cudaStream_t s,
+                                  const TraceHook *hook = nullptr)
 {
     const bool mixed = o.policy != MF_POLICY_FP64;
     const int G = bicg ? bicgstab_grid(m, mixed) : solver_grid(m, mixed);
@@ -31,6 +32,7 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
             m->packed_policy = MF_POLICY_STATIC;
         }
     }
+    if (o.policy == MF_POLICY_LEARNED) m->pol_have_prev = 0;  // no history from an earlier solve
     CgArgs a;
     memset(&a, 0, sizeof(a));
     a.A = m->v;
@@ -64,6 +66,7 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
     a.delta = o.refine_delta > 0 && o.refine_delta < 1 ? o.refine_delta : 0.1;
     // checkpoints (policy updates between launches) for CG's dynamic policies
     a.exit_on_refine = (!bicg && mixed && o.policy != MF_POLICY_STATIC) ? 1 : 0;
+    a.checkpoint_every = (hook && !bicg) ? hook->every : 0;
     a.budget_ns = (unsigned long long)(o.wait_budget_s * 1e9);
     a.start = 1;
     a.timing = o.phase_times ? w.timing : nullptr;
@@ -80,7 +83,7 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
         if (bicg) MF_TRY(launch_bicgstab(mixed, a, G, s));
         else MF_TRY(launch_cg(mixed, a, G, s));
         launches++;
-        if (!a.exit_on_refine) break;
+        if (!a.exit_on_refine && a.checkpoint_every == 0) break;
         MF_CUDA(cudaMemcpyAsync(st, w.state, sizeof(st), cudaMemcpyDeviceToHost, s));
         MF_CUDA(cudaMemcpyAsync(&h_status, w.status, sizeof(int), cudaMemcpyDeviceToHost, s));
         MF_CUDA(cudaStreamSynchronize(s));
@@ -90,6 +93,11 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
         const int it = (int)st[S_ITERS];
         const void *pnew = (it & 1) ? w.p1 : w.p0;  // written by the last iteration
         const void *pold = (it & 1) ? w.p0 : w.p1;
+        if (hook) MF_TRY(hook->fn(hook->ctx, m, w, pnew, pold, it, st[S_RELRES], s));
+        if (o.policy == MF_POLICY_FP64 || o.policy == MF_POLICY_STATIC) {
+            a.start = 0;
+            continue;
+        }
         if (o.policy == MF_POLICY_RULE) {
             MF_TRY(rule_working_classes(m, pnew, pold, m->d_wcls, s));
         } else {
@@ -169,6 +177,12 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
                    double *history, cudaStream_t s)
 {
     return persistent_solve(false, m, b, x, o, rep, history, s);
+}
+
+mf_status cg_solve_traced(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,
+                          const TraceHook *hook, cudaStream_t s)
+{
+    return persistent_solve(false, m, b, x, o, rep, nullptr, s, hook);
 }
 
 mf_status bicgstab_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,

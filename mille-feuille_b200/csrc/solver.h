@@ -50,6 +50,7 @@ struct CgArgs {
     int fixed;                     // 1: run exactly maxiter iterations
     double delta;                  // reliable-update trigger
     int exit_on_refine;            // 1: return after each reliable update
+    int checkpoint_every;          // > 0: return every this many iterations
     unsigned long long budget_ns;  // bound of every grid-wide wait
     int start;                     // 1: initialise x, r, p and the state
     unsigned long long *timing;    // optional [G][8] per-CTA phase nanoseconds
@@ -66,6 +67,18 @@ struct SolverWork {
 };
 
 mf_status solver_resources(mf_matrix m, int G, SolverWork &w);
+
+// Called at every checkpoint of a solve run with trace collection: the
+// solver state (p of the last iteration in p_new, the previous p in p_old,
+// q = A p_new, r) is in `w`.
+struct TraceHook {
+    int every;
+    mf_status (*fn)(void *ctx, mf_matrix m, SolverWork &w, const void *p_new, const void *p_old, int it,
+                    double relres, cudaStream_t s);
+    void *ctx;
+};
+mf_status cg_solve_traced(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,
+                          const TraceHook *hook, cudaStream_t s);
 // chunks.cu: chunk table for the current partition; payload offsets refresh
 mf_status build_chunks(mf_matrix m, cudaStream_t s);
 mf_status refresh_chunk_payload(mf_matrix m, cudaStream_t s);

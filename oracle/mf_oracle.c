@@ -510,3 +510,65 @@ int orc_bicgstab(int n, const int *rp, const int *ci, const double *v, const dou
     free(r); free(rh); free(p); free(vv); free(s); free(t);
     return it;
 }
+
+/* ---- MLP policy oracle: 16 -> 32 -> 32 -> 4, ReLU, softmax cross-entropy.
+ * Weights layout W1[32][16], b1[32], W2[32][32], b2[32], W3[4][32], b3[4]
+ * (the learned policy of the library; no reference counterpart).  Returns
+ * the mean loss over n samples and its gradient, in double precision. */
+double orc_mlp_grad(const float *w, const float *X, const int *Y, int n, double *grad)
+{
+    enum { NF = 16, H1 = 32, H2 = 32, NO = 4 };
+    const int OW1 = 0, OB1 = H1 * NF, OW2 = OB1 + H1, OB2 = OW2 + H2 * H1, OW3 = OB2 + H2, OB3 = OW3 + NO * H2;
+    const int NP = OB3 + NO;
+    for (int p = 0; p < NP; p++) grad[p] = 0;
+    double loss = 0;
+    for (int s = 0; s < n; s++) {
+        const float *x = X + (size_t)s * NF;
+        double h1[H1], h2[H2], o[NO], dl[NO], d2[H2], d1[H1];
+        for (int j = 0; j < H1; j++) {
+            double a = w[OB1 + j];
+            for (int k = 0; k < NF; k++) a += (double)w[OW1 + j * NF + k] * x[k];
+            h1[j] = a > 0 ? a : 0;
+        }
+        for (int j = 0; j < H2; j++) {
+            double a = w[OB2 + j];
+            for (int k = 0; k < H1; k++) a += (double)w[OW2 + j * H1 + k] * h1[k];
+            h2[j] = a > 0 ? a : 0;
+        }
+        double mx = -1e300;
+        for (int o_ = 0; o_ < NO; o_++) {
+            double a = w[OB3 + o_];
+            for (int k = 0; k < H2; k++) a += (double)w[OW3 + o_ * H2 + k] * h2[k];
+            o[o_] = a;
+            if (a > mx) mx = a;
+        }
+        double z = 0;
+        for (int k = 0; k < NO; k++) z += exp(o[k] - mx);
+        const int y = Y[s] & 3;
+        loss += -(o[y] - mx - log(z));
+        for (int k = 0; k < NO; k++) dl[k] = (exp(o[k] - mx) / z - (k == y ? 1.0 : 0.0)) / n;
+        for (int j = 0; j < H2; j++) {
+            double a = 0;
+            for (int k = 0; k < NO; k++) a += (double)w[OW3 + k * H2 + j] * dl[k];
+            d2[j] = h2[j] > 0 ? a : 0;
+        }
+        for (int j = 0; j < H1; j++) {
+            double a = 0;
+            for (int k = 0; k < H2; k++) a += (double)w[OW2 + k * H1 + j] * d2[k];
+            d1[j] = h1[j] > 0 ? a : 0;
+        }
+        for (int j = 0; j < H1; j++) {
+            for (int k = 0; k < NF; k++) grad[OW1 + j * NF + k] += d1[j] * x[k];
+            grad[OB1 + j] += d1[j];
+        }
+        for (int j = 0; j < H2; j++) {
+            for (int k = 0; k < H1; k++) grad[OW2 + j * H1 + k] += d2[j] * h1[k];
+            grad[OB2 + j] += d2[j];
+        }
+        for (int o_ = 0; o_ < NO; o_++) {
+            for (int k = 0; k < H2; k++) grad[OW3 + o_ * H2 + k] += dl[o_] * h2[k];
+            grad[OB3 + o_] += dl[o_];
+        }
+    }
+    return loss / n;
+}

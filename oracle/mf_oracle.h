@@ -84,6 +84,10 @@ double orc_true_relres(int n, const int *rowptr, const int *colidx, const double
  * uncompressed in-tile column array (the arrays the GPU path uses). */
 void orc_tiled_spmv(const orc_tiles *t, int rowA, const double *x, double *y);
 
+/* MLP policy (16 -> 32 -> 32 -> 4): mean softmax cross-entropy over n
+ * samples and its gradient, double precision. */
+double orc_mlp_grad(const float *w, const float *X, const int *Y, int n, double *grad);
+
 #ifdef __cplusplus
 }
 #endif

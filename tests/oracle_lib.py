@@ -100,6 +100,9 @@ def oracle() -> C.CDLL:
         lib.orc_bicgstab.restype = C.c_int
         lib.orc_true_relres.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
         lib.orc_true_relres.restype = C.c_double
+        lib.orc_mlp_grad.argtypes = [_f32p, _f32p, np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS"), C.c_int,
+                                     _f64p]
+        lib.orc_mlp_grad.restype = C.c_double
         _orc = lib
     return _orc
 

@@ -170,3 +170,27 @@ def test_oracle_bicgstab_on_convdiff(mf):
     it, x, rr = ol.oracle_bicgstab(Ac, b, 2000, 1e-9)
     assert rr <= 1e-9
     assert ol.oracle_true_relres(Ac, b, x) < 1e-8
+
+
+NPARAM = 16 * 32 + 32 + 32 * 32 + 32 + 4 * 32 + 4
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The policy oracle's analytic gradient against central differences."""
+    lib = ol.oracle()
+    rng = np.random.default_rng(21)
+    w = (rng.normal(size=NPARAM) * 0.3).astype(np.float32)
+    X = rng.normal(size=(40, 16)).astype(np.float32)
+    Y = rng.integers(0, 4, size=40).astype(np.int32)
+    g = np.zeros(NPARAM)
+    lib.orc_mlp_grad(w, X, Y, 40, g)
+    for p in rng.choice(NPARAM, size=60, replace=False):
+        h = 1e-3
+        wp, wm = w.astype(np.float64).copy(), w.astype(np.float64).copy()
+        wp[p] += h
+        wm[p] -= h
+        gg = np.zeros(NPARAM)
+        lp = lib.orc_mlp_grad(wp.astype(np.float32), X, Y, 40, gg)
+        lm = lib.orc_mlp_grad(wm.astype(np.float32), X, Y, 40, gg)
+        fd = (lp - lm) / ((np.float32(wp[p]) - np.float32(wm[p])))
+        assert abs(fd - g[p]) <= 2e-3 * max(1.0, abs(g[p])) + 1e-4, (p, fd, g[p])

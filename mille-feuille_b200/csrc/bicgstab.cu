@@ -115,7 +115,8 @@ __global__ void __launch_bounds__(NT, MINB) k_bicgstab(CgArgs a)
     double rnorm = a.start ? rmax : st[S_RELRES] * nb;
     double relres_true = rnorm / nb;
     while (gc.ok) {
-        if (!a.fixed && rnorm <= a.tol * nb) {
+        // an exactly zero residual ends a fixed-count run too
+        if ((!a.fixed && rnorm <= a.tol * nb) || rnorm == 0.0) {
             exit_reason = EXIT_CONVERGED;
             break;
         }
@@ -234,7 +235,7 @@ __global__ void __launch_bounds__(NT, MINB) k_bicgstab(CgArgs a)
         rho = rho_new;
         if (a.hist && g == 0 && threadIdx.x == 0) a.hist[it] = rnorm / nb;
     }
-    if (MIX && exit_reason != EXIT_CONVERGED && gc.ok) {
+    if (MIX && exit_reason != EXIT_CHECKPOINT && gc.ok) {
         for (int i = row0 + threadIdx.x; i < row1; i += NT) {
             a.xhi[i] = a.xhi[i] + (double)xlo[i];
             xlo[i] = (VT)0;

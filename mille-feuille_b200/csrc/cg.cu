@@ -101,7 +101,9 @@ __global__ void __launch_bounds__(NT, MINB) k_cg(CgArgs a)
         tmark = now_;                                     \
     }
     while (gc.ok) {
-        if (!a.fixed && sqrt(rho) <= a.tol * nb) {
+        // an exactly zero residual ends a fixed-count run too (the next
+        // step would divide 0 by 0)
+        if ((!a.fixed && sqrt(rho) <= a.tol * nb) || rho == 0.0) {
             exit_reason = EXIT_CONVERGED;
             break;
         }
@@ -215,8 +217,8 @@ __global__ void __launch_bounds__(NT, MINB) k_cg(CgArgs a)
         }
     }
 #undef MF_MARK
-    if (MIX && exit_reason != EXIT_CONVERGED && exit_reason != EXIT_CHECKPOINT && gc.ok) {
-        // leaving with an unflushed FP32 correction: fold it into x
+    if (MIX && exit_reason != EXIT_CHECKPOINT && gc.ok) {
+        // fold any unflushed FP32 correction into x (zero after a refinement)
         for (int i = row0 + threadIdx.x; i < row1; i += NT) {
             a.xhi[i] = a.xhi[i] + (double)xlo[i];
             xlo[i] = (VT)0;

@@ -88,6 +88,7 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
 mf_status strip_partition(mf_matrix m, int ctas, cudaStream_t s);
 // spmv.cu
 mf_status spmv_fp64(const MfTiles &A, const double *x, double *y, cudaStream_t s);
+mf_status spmv_fp64_cidx(const MfTiles &A, const unsigned char *cidx, const double *x, double *y, cudaStream_t s);
 // residual.cu: per-strip partials (2 doubles per strip) then a fixed-order sum
 mf_status residual_norm(const MfTiles &A, const double *b, const double *x, double *part, double *out,
                         cudaStream_t s);

@@ -11,9 +11,17 @@ DECL = re.compile(r"^\s*(?:const\s+)?(?:unsigned\s+)?[A-Za-z_][\w]*\s*\**\s*\b([
                   re.M | re.S)
 
 
-def declared_functions():
+# headers whose functions live in the solver entry libraries rather than libmf.so
+SOLVER_HEADERS = ("Mille-feuille-cg.h", "Mille-feuille-bicg.h")
+
+
+def declared_functions(headers=None):
     names = set()
     for h in sorted((ROOT / "include").glob("*.h")):
+        if headers is not None and h.name not in headers:
+            continue
+        if headers is None and h.name in SOLVER_HEADERS:
+            continue
         text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
         text = re.sub(r"//[^\n]*", "", text)
         for m in DECL.finditer(text):
@@ -46,3 +54,35 @@ def test_invalid_arguments_rejected_without_device(mf):
     assert st == 1  # MF_ERR_INVALID_ARG
     st = mf.lib().mf_matrix_export(None, b"tile_ptr", None, 0)
     assert st == 1
+
+
+@pytest.mark.parametrize("libname", ["libmf_solvers.so", "libmf_solvers_mixed.so"])
+def test_solver_entry_libraries_export_reference_names(mf, libname):
+    """cg_solve_inc/sync/reduce and bicgstab/_sync/_inc, as declared in
+    Mille-feuille-cg.h and Mille-feuille-bicg.h."""
+    names = declared_functions(SOLVER_HEADERS)
+    assert set(names) == {"cg_solve_inc", "cg_solve_sync", "cg_solve_reduce", "bicgstab", "bicgstab_sync",
+                          "bicgstab_inc"}
+    lib = ctypes.CDLL(str(ROOT / "mille-feuille_b200" / "lib" / libname))
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_tile_matrix_layout_matches_reference_field_order():
+    """Tile_matrix keeps the reference's 69 fields in order (src/format.h:14-86)
+    and appends mf_handle."""
+    import dropin
+
+    f = dropin.tile_fields()
+    assert len(f) == 70 and f[-1] == ("mf_handle", True)
+    names = [n for n, _ in f]
+    assert names[:6] == ["tilem", "tilen", "tilenum", "tile_ptr", "tile_columnidx", "tile_nnz"]
+    assert names.index("csrsize") == names.index("csr_compressedIdx") + 1
+    ref = ROOT.parent / "reference" / "src" / "format.h"
+    if ref.exists():
+        body = ref.read_text()
+        body = body[body.index("typedef struct\n{"): body.index("} Tile_matrix;")]
+        import re as _re
+
+        ref_names = _re.findall(r"\b([A-Za-z_]\w*);", body)
+        assert ref_names == names[:-1]

@@ -16,14 +16,17 @@
 // the next SpMV starts.  Mixed precision follows the CG solver: packed
 // per-tile classes, FP32 vectors and accumulation, FP64 dot products and
 // FP64 reliable updates of the residual.
+#include <type_traits>
+
 #include "persist.cuh"
 
 namespace mf {
 namespace {
 using namespace persist;
 
-__device__ __forceinline__ void grid_sum2(const CgArgs &a, double l0, double l1, int slot, GridCtx &gc,
-                                          SolverSmem &S, double &o0, double &o1)
+template <class SM>
+__device__ __forceinline__ void grid_sum2(const CgArgs &a, double l0, double l1, int slot, GridCtx &gc, SM &S,
+                                          double &o0, double &o1)
 {
     const int G = gridDim.x;
     const double c0 = block_sum<NT>(l0, S.warp);
@@ -33,45 +36,39 @@ __device__ __forceinline__ void grid_sum2(const CgArgs &a, double l0, double l1,
         a.partials[(slot + 1) * G + blockIdx.x] = c1;
     }
     gc.epoch++;
-    gc.ok = gc.ok && grid_barrier_sharded(a.bar, gc.epoch, a.status, a.budget_ns);
-    __shared__ double s_two[2];
-    if (threadIdx.x < 32) {
-        const double s0 = warp_sum_partials(a.partials + slot * G, G);
-        const double s1 = warp_sum_partials(a.partials + (slot + 1) * G, G);
-        if (threadIdx.x == 0) {
-            s_two[0] = s0;
-            s_two[1] = s1;
-        }
-    }
-    __syncthreads();
-    o0 = s_two[0];
-    o1 = s_two[1];
+    gc.ok = gc.ok && grid_barrier_fast(a.bar, gc.epoch, a.status, a.budget_ns);
+    o0 = block_sum_partials<NT>(a.partials + slot * G, G, S.warp);
+    o1 = block_sum_partials<NT>(a.partials + (slot + 1) * G, G, S.warp);
 }
 
-template <bool MIX>
-__global__ void __launch_bounds__(NT, MINB) k_bicgstab(CgArgs a)
+template <bool MIX, int LAY>
+__global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_bicgstab(CgArgs a)
 {
     using VT = typename VecT<MIX>::T;
+    using SM = typename std::conditional<LAY == 0, SolverSmem, SlotSmem>::type;
     constexpr int PK = MIX ? 1 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SolverSmem &S = *reinterpret_cast<SolverSmem *>(smem_raw);
+    SM &S = *reinterpret_cast<SM *>(smem_raw);
     const MfTiles &A = a.A;
     const int g = blockIdx.x;
     const int sb0 = a.part[g], se0 = a.part[g + 1];
-    const int cb = a.cta_chunk[g], ce = a.cta_chunk[g + 1];
+    const int cb = LAY == 0 ? a.cta_chunk[g] : a.scta_chunk[g], ce = LAY == 0 ? a.cta_chunk[g + 1] : a.scta_chunk[g + 1];
     const int row0 = sb0 * MF_TILE, row1 = min(se0 * MF_TILE, A.rows);
     VT *r = (VT *)a.r, *rh = (VT *)a.rhat, *t = (VT *)a.t, *xlo = (VT *)a.xlo;
     GridCtx gc;
     gc.epoch = 0;
     gc.ok = true;
-    gc.use[0] = gc.use[1] = 0;
+    gc.use[0] = gc.use[1] = gc.use[2] = gc.use[3] = 0;
     double *st = a.state;
     if (threadIdx.x == 0) {
-        mbar_init(&S.bar[0], 1);
-        mbar_init(&S.bar[1], 1);
+        for (int i = 0; i < (LAY == 0 ? 2 : NSTG); i++) mbar_init(&S.bar[i], 1);
         mbar_fence_init();
     }
-    for (int c = cb + threadIdx.x; c < ce && c - cb < RECS; c += NT) S.recs[c - cb] = a.chunks[c];
+    if constexpr (LAY == 0) {
+        for (int c = cb + threadIdx.x; c < ce && c - cb < RECS; c += NT) S.recs[c - cb] = a.chunks[c];
+    } else {
+        for (int c = cb + threadIdx.x; c < ce && c - cb < SRECS; c += NT) S.recs[c - cb] = a.schunks[c];
+    }
     __syncthreads();
 
     double rho, beta, nb, rmax, alpha, omega;
@@ -144,7 +141,7 @@ __global__ void __launch_bounds__(NT, MINB) k_bicgstab(CgArgs a)
             vnew[i] = vi;
             loc = __dadd_rn(loc, __dmul_rn((double)rh[i], (double)vi));
         };
-        if (!spmv_chunks<PK>(a, S, gc, cb, ce, psrc, aout, nullptr)) gc.ok = false;
+        if (!spmv_any<PK, LAY>(a, S, gc, cb, ce, sb0, se0, psrc, aout, nullptr)) gc.ok = false;
         double rv, dummy;
         grid_sum2(a, loc, 0.0, 2, gc, S, rv, dummy);
         if (!gc.ok) break;
@@ -170,7 +167,7 @@ __global__ void __launch_bounds__(NT, MINB) k_bicgstab(CgArgs a)
             lts = __dadd_rn(lts, __dmul_rn((double)ti, (double)si));
             ltt = __dadd_rn(ltt, __dmul_rn((double)ti, (double)ti));
         };
-        if (!spmv_chunks<PK>(a, S, gc, cb, ce, ssrc, tout, nullptr)) gc.ok = false;
+        if (!spmv_any<PK, LAY>(a, S, gc, cb, ce, sb0, se0, ssrc, tout, nullptr)) gc.ok = false;
         double ts, tt;
         grid_sum2(a, lts, ltt, 4, gc, S, ts, tt);
         if (!gc.ok) break;
@@ -213,7 +210,7 @@ __global__ void __launch_bounds__(NT, MINB) k_bicgstab(CgArgs a)
                 l1 = __dadd_rn(l1, __dmul_rn((double)rh[i], (double)rv2));
                 l2 = __dadd_rn(l2, __dmul_rn((double)rv2, (double)rv2));
             };
-            if (!spmv_chunks<0>(a, S, gc, cb, ce, xsrc, rout, nullptr)) gc.ok = false;
+            if (!spmv_any<0, LAY>(a, S, gc, cb, ce, sb0, se0, xsrc, rout, nullptr)) gc.ok = false;
             grid_sum2(a, l1, l2, 0, gc, S, rho_new, rrn);
             if (!gc.ok) break;
             rnorm = sqrt(rrn);
@@ -255,7 +252,7 @@ __global__ void __launch_bounds__(NT, MINB) k_bicgstab(CgArgs a)
     }
 }
 
-template <bool MIX>
+template <bool MIX, int LAY>
 int max_ctas_bicg()
 {
     static int cached = -1;
@@ -263,9 +260,9 @@ int max_ctas_bicg()
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const size_t dyn = sizeof(SolverSmem);
-        cudaFuncSetAttribute(k_bicgstab<MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bicgstab<MIX>, NT, dyn);
+        const size_t dyn = LAY == 0 ? sizeof(SolverSmem) : sizeof(SlotSmem);
+        cudaFuncSetAttribute(k_bicgstab<MIX, LAY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bicgstab<MIX, LAY>, NT, dyn);
         cached = sms * (per > 0 ? per : 1);
     }
     return cached;
@@ -273,9 +270,10 @@ int max_ctas_bicg()
 
 }  // namespace
 
-int bicgstab_grid(mf_matrix m, bool mixed)
+int bicgstab_grid(mf_matrix m, bool mixed, bool slots)
 {
-    int maxc = mixed ? max_ctas_bicg<true>() : max_ctas_bicg<false>();
+    int maxc = slots ? (mixed ? max_ctas_bicg<true, 1>() : max_ctas_bicg<false, 1>())
+                     : (mixed ? max_ctas_bicg<true, 0>() : max_ctas_bicg<false, 0>());
     if (const char *e = getenv("MF_SOLVER_CTAS")) {
         const int v = atoi(e);
         if (v > 0 && v < maxc) maxc = v;
@@ -287,16 +285,20 @@ int bicgstab_grid(mf_matrix m, bool mixed)
 
 mf_status launch_bicgstab(bool mixed, CgArgs &a, int G, cudaStream_t s)
 {
-    const size_t dyn = sizeof(SolverSmem);
     void *args[] = {&a};
     note_launch();
-    if (mixed) {
-        max_ctas_bicg<true>();
-        MF_CUDA(cudaLaunchCooperativeKernel((const void *)k_bicgstab<true>, dim3(G), dim3(NT), args, dyn, s));
+    const void *fn;
+    size_t dyn;
+    if (a.sslot) {
+        dyn = sizeof(SlotSmem);
+        if (mixed) max_ctas_bicg<true, 1>(), fn = (const void *)k_bicgstab<true, 1>;
+        else max_ctas_bicg<false, 1>(), fn = (const void *)k_bicgstab<false, 1>;
     } else {
-        max_ctas_bicg<false>();
-        MF_CUDA(cudaLaunchCooperativeKernel((const void *)k_bicgstab<false>, dim3(G), dim3(NT), args, dyn, s));
+        dyn = sizeof(SolverSmem);
+        if (mixed) max_ctas_bicg<true, 0>(), fn = (const void *)k_bicgstab<true, 0>;
+        else max_ctas_bicg<false, 0>(), fn = (const void *)k_bicgstab<false, 0>;
     }
+    MF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(NT), args, dyn, s));
     return MF_OK;
 }
 

@@ -28,36 +28,42 @@
 //     by refine_delta, the FP32 correction is added to the FP64 solution and
 //     r is replaced by the FP64 true residual b - A x computed from the FP64
 //     payload.  Convergence is only declared on that FP64 true residual.
+#include <type_traits>
+
 #include "persist.cuh"
 
 namespace mf {
 namespace {
 using namespace persist;
 
-template <bool MIX>
-__global__ void __launch_bounds__(NT, MINB) k_cg(CgArgs a)
+template <bool MIX, int LAY>
+__global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_cg(CgArgs a)
 {
     using VT = typename VecT<MIX>::T;
+    using SM = typename std::conditional<LAY == 0, SolverSmem, SlotSmem>::type;
     constexpr int PK = MIX ? 1 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SolverSmem &S = *reinterpret_cast<SolverSmem *>(smem_raw);
+    SM &S = *reinterpret_cast<SM *>(smem_raw);
     const MfTiles &A = a.A;
     const int g = blockIdx.x;
     const int sb0 = a.part[g], se0 = a.part[g + 1];
-    const int cb = a.cta_chunk[g], ce = a.cta_chunk[g + 1];
+    const int cb = LAY == 0 ? a.cta_chunk[g] : a.scta_chunk[g], ce = LAY == 0 ? a.cta_chunk[g + 1] : a.scta_chunk[g + 1];
     const int row0 = sb0 * MF_TILE, row1 = min(se0 * MF_TILE, A.rows);
     VT *r = (VT *)a.r, *q = (VT *)a.q, *xlo = (VT *)a.xlo;
     GridCtx gc;
     gc.epoch = 0;
     gc.ok = true;
-    gc.use[0] = gc.use[1] = 0;
+    gc.use[0] = gc.use[1] = gc.use[2] = gc.use[3] = 0;
     double *st = a.state;
     if (threadIdx.x == 0) {
-        mbar_init(&S.bar[0], 1);
-        mbar_init(&S.bar[1], 1);
+        for (int i = 0; i < (LAY == 0 ? 2 : NSTG); i++) mbar_init(&S.bar[i], 1);
         mbar_fence_init();
     }
-    for (int c = cb + threadIdx.x; c < ce && c - cb < RECS; c += NT) S.recs[c - cb] = a.chunks[c];
+    if constexpr (LAY == 0) {
+        for (int c = cb + threadIdx.x; c < ce && c - cb < RECS; c += NT) S.recs[c - cb] = a.chunks[c];
+    } else {
+        for (int c = cb + threadIdx.x; c < ce && c - cb < SRECS; c += NT) S.recs[c - cb] = a.schunks[c];
+    }
     __syncthreads();
 
     double rho, beta, nb, rmax;
@@ -130,7 +136,7 @@ __global__ void __launch_bounds__(NT, MINB) k_cg(CgArgs a)
             q[i] = qi;
             loc = __dadd_rn(loc, __dmul_rn((double)pn, (double)qi));
         };
-        if (!spmv_chunks<PK>(a, S, gc, cb, ce, psrc, aout, timed ? tph : nullptr)) gc.ok = false;
+        if (!spmv_any<PK, LAY>(a, S, gc, cb, ce, sb0, se0, psrc, aout, timed ? tph : nullptr)) gc.ok = false;
         MF_MARK(0);
         const double pq = grid_sum(a, loc, 2, gc, S);
         MF_MARK(1);
@@ -198,7 +204,7 @@ __global__ void __launch_bounds__(NT, MINB) k_cg(CgArgs a)
                 r[i] = rv;
                 loc = __dadd_rn(loc, __dmul_rn((double)rv, (double)rv));
             };
-            if (!spmv_chunks<0>(a, S, gc, cb, ce, xsrc, rout, nullptr)) gc.ok = false;
+            if (!spmv_any<0, LAY>(a, S, gc, cb, ce, sb0, se0, xsrc, rout, nullptr)) gc.ok = false;
             rho_new = grid_sum(a, loc, 1, gc, S);
             if (!gc.ok) break;
             rmax = sqrt(rho_new);
@@ -274,7 +280,13 @@ __global__ void k_resid_final(int nblk, const double *__restrict__ part, double 
     }
 }
 
-template <bool MIX>
+template <int LAY>
+constexpr size_t smem_bytes()
+{
+    return LAY == 0 ? sizeof(SolverSmem) : sizeof(SlotSmem);
+}
+
+template <bool MIX, int LAY>
 int max_ctas_for()
 {
     static int cached = -1;
@@ -282,9 +294,9 @@ int max_ctas_for()
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const size_t dyn = sizeof(SolverSmem);
-        cudaFuncSetAttribute(k_cg<MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg<MIX>, NT, dyn);
+        const size_t dyn = smem_bytes<LAY>();
+        cudaFuncSetAttribute(k_cg<MIX, LAY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg<MIX, LAY>, NT, dyn);
         cached = sms * (per > 0 ? per : 1);
     }
     return cached;
@@ -337,9 +349,10 @@ mf_status solver_resources(mf_matrix m, int G, SolverWork &w)
     return MF_OK;
 }
 
-int solver_grid(mf_matrix m, bool mixed)
+int solver_grid(mf_matrix m, bool mixed, bool slots)
 {
-    int maxc = mixed ? max_ctas_for<true>() : max_ctas_for<false>();
+    int maxc = slots ? (mixed ? max_ctas_for<true, 1>() : max_ctas_for<false, 1>())
+                     : (mixed ? max_ctas_for<true, 0>() : max_ctas_for<false, 0>());
     if (const char *e = getenv("MF_SOLVER_CTAS")) {
         const int v = atoi(e);
         if (v > 0 && v < maxc) maxc = v;
@@ -369,16 +382,20 @@ mf_status true_residual(mf_matrix m, const double *b, const double *x, SolverWor
 
 mf_status launch_cg(bool mixed, CgArgs &a, int G, cudaStream_t s)
 {
-    const size_t dyn = sizeof(SolverSmem);
     void *args[] = {&a};
     note_launch();
-    if (mixed) {
-        max_ctas_for<true>();
-        MF_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg<true>, dim3(G), dim3(NT), args, dyn, s));
+    const void *fn;
+    size_t dyn;
+    if (a.sslot) {
+        dyn = smem_bytes<1>();
+        if (mixed) max_ctas_for<true, 1>(), fn = (const void *)k_cg<true, 1>;
+        else max_ctas_for<false, 1>(), fn = (const void *)k_cg<false, 1>;
     } else {
-        max_ctas_for<false>();
-        MF_CUDA(cudaLaunchCooperativeKernel((const void *)k_cg<false>, dim3(G), dim3(NT), args, dyn, s));
+        dyn = smem_bytes<0>();
+        if (mixed) max_ctas_for<true, 0>(), fn = (const void *)k_cg<true, 0>;
+        else max_ctas_for<false, 0>(), fn = (const void *)k_cg<false, 0>;
     }
+    MF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(NT), args, dyn, s));
     return MF_OK;
 }
 

@@ -136,6 +136,53 @@ __device__ __forceinline__ bool grid_barrier_sharded(unsigned long long *ctr, un
     return s_ok != 0;
 }
 
+__device__ __forceinline__ unsigned long long atom_add_acq_rel_u64(unsigned long long *p, unsigned long long v)
+{
+    unsigned long long old;
+    asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+    return old;
+}
+
+// Grid-wide barrier with sharded arrival and one-way ordering: the arrival
+// is an acquire-release atomic (it publishes every write the CTA made before
+// the preceding __syncthreads, and the last arrival of a group carries its
+// group's writes on to the top counter), the spin is an acquire load.  No
+// full fences: one L2 round trip to arrive, one per poll.  Same counters and
+// epochs as grid_barrier_sharded.  A CTA that gives up (budget, or another
+// CTA's error status seen while spinning) returns false.
+__device__ __forceinline__ bool grid_barrier_fast(unsigned long long *ctr, unsigned long long epoch, int *status,
+                                                  unsigned long long budget_ns)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned G = gridDim.x;
+        const unsigned sub = blockIdx.x & 7u;
+        const unsigned long long gsize = (G - sub + 7u) / 8u;
+        const unsigned long long ng = G < 8u ? G : 8u;
+        const unsigned long long old = atom_add_acq_rel_u64(ctr + 16 * sub, 1ull);
+        if (old + 1ull == epoch * gsize) atom_add_acq_rel_u64(ctr + 128, 1ull);
+        if (ld_acquire_u64(ctr + 128) < epoch * ng) {
+            const unsigned long long t0 = globaltimer_ns();
+            unsigned spins = 0;
+            while (ld_acquire_u64(ctr + 128) < epoch * ng) {
+                if (((++spins) & 31u) == 0u) {
+                    if (ld_volatile_i32(status) != DEV_OK) { ok = 0; break; }
+                    if (globaltimer_ns() - t0 > budget_ns) {
+                        atomicCAS(status, DEV_OK, DEV_TIMEOUT);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 // Deterministic CTA reduction of one double per thread: warp butterfly, then
 // the warp results summed in warp order.  All threads get the result.
 template <int NT>
@@ -173,6 +220,27 @@ __device__ __forceinline__ double warp_sum_partials(const double *part, int coun
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     return s;
+}
+
+// Deterministic sum of `count` per-CTA partials by a whole CTA (same order
+// in every CTA): thread t sums entries t, t + NT, ... (loads issued
+// together), then the fixed block tree.  All threads get the result.
+template <int NT>
+__device__ __forceinline__ double block_sum_partials(const double *part, int count, double *s_warp)
+{
+    double s = 0.0;
+    constexpr int B = 4;
+    for (int i0 = threadIdx.x; i0 < count; i0 += NT * B) {
+        double v[B];
+#pragma unroll
+        for (int u = 0; u < B; u++) {
+            const int i = i0 + NT * u;
+            v[u] = (i < count) ? __ldcg(part + i) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < B; u++) s += v[u];
+    }
+    return block_sum<NT>(s, s_warp);
 }
 
 }  // namespace mf

@@ -71,6 +71,18 @@ struct mf_matrix_s {
     size_t pol_bytes = 0;
     int pol_static_ready = 0, pol_have_prev = 0;
     float pol_prev_relres = 0.f;
+    // row-slot execution layout of the persistent solvers (slots.cu)
+    int slots_state = 0;       // 0 not built, 1 built, -1 not describable
+    long long nslots = 0;
+    int *d_sslot = nullptr;
+    uint16_t *d_smeta = nullptr;
+    double *d_sval = nullptr;
+    unsigned *d_shdr = nullptr;
+    unsigned char *d_spay = nullptr;
+    int slot_policy = -1;      // policy whose classes the slot payload holds
+    int *d_scta_chunk = nullptr;   // slot chunk table of the current partition
+    void *d_schunks = nullptr;
+    int schunk_ctas = 0, nschunks = 0;
     // per-strip partials of mf_residual_norm
     double *d_resid = nullptr;
     size_t resid_bytes = 0;

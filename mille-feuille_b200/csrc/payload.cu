@@ -138,8 +138,8 @@ __global__ void k_seg_change(int nseg, int n, const VT *__restrict__ pn, const V
             pm = fabsf((float)pn[j]);
         }
         for (int o = 8; o > 0; o >>= 1) {
-            dp = fmaxf(dp, __shfl_xor_sync(0xffffffffu, dp, o, 16));
-            pm = fmaxf(pm, __shfl_xor_sync(0xffffffffu, pm, o, 16));
+            dp = fmaxf(dp, __shfl_xor_sync(0xFFFFu << (threadIdx.x & 16), dp, o, 16));
+            pm = fmaxf(pm, __shfl_xor_sync(0xFFFFu << (threadIdx.x & 16), pm, o, 16));
         }
         if (lane == 0) {
             seg_dp[s] = dp;

@@ -18,6 +18,14 @@ constexpr int NT = CH_STRIPS * MF_TILE;  // one half-warp per strip of a chunk
 #define MF_CG_MINB 3
 #endif
 constexpr int MINB = MF_CG_MINB;  // CTAs per SM the registers allow
+#ifndef MF_SLOT_MINB
+#define MF_SLOT_MINB 3
+#endif
+#ifndef MF_SLOT_U
+#define MF_SLOT_U 4
+#endif
+constexpr int SMINB = MF_SLOT_MINB;  // CTAs per SM of the row-slot kernels
+constexpr int SLOT_U = MF_SLOT_U;    // slots loaded before any is used
 constexpr int RECS = 64;                    // chunk records cached in shared memory
 
 // Byte layout of one shared-memory stage (every region 16-byte aligned,
@@ -50,6 +58,42 @@ struct __align__(16) SolverSmem {
     double res;
 };
 
+// Shared memory of the kernels that run from the row-slot layout: two
+// stages, each holding one slot chunk (strip slot offsets, tile pointers,
+// tile columns, slot words, then FP64 values or the mixed slot headers and
+// payload).  Every region is 16-byte aligned and sized for the largest
+// 16-byte-rounded range it receives.
+constexpr int SOFF_SSLOT = 0;
+constexpr int SOFF_TPTR = 112;
+constexpr int SOFF_TCOL = 224;
+constexpr int SOFF_META = SOFF_TCOL + SC_TILES * 4 + 32;
+constexpr int SOFF_DATA = SOFF_META + SC_SLOTS * MF_TILE * 2 + 32;
+constexpr int SOFF_PAY = SOFF_DATA + SC_SLOTS * 4 + 32;  // mixed payload after the slot headers
+constexpr int SSTAGE_BYTES = SOFF_DATA + SC_SLOTS * MF_TILE * 8 + 32;
+static_assert(SOFF_META % 16 == 0 && SOFF_DATA % 16 == 0 && SOFF_PAY % 16 == 0 && SSTAGE_BYTES % 16 == 0,
+              "slot stage regions must be 16-byte aligned");
+static_assert(SOFF_PAY + SC_SLOTS * 64 + 32 <= SSTAGE_BYTES, "mixed payload must fit the stage");
+
+struct SlotHdr {
+    SlotChunk rec;
+    int sh_sslot, sh_tptr, sh_tcol, sh_meta, sh_data, sh_pay;
+};
+
+#ifndef MF_SLOT_STAGES
+#define MF_SLOT_STAGES 2
+#endif
+constexpr int NSTG = MF_SLOT_STAGES;  // slot chunks in flight per CTA
+constexpr int SRECS = 64;  // slot chunk records cached in shared memory
+
+struct __align__(16) SlotSmem {
+    unsigned char stage[NSTG][SSTAGE_BYTES];
+    SlotHdr hdr[NSTG];
+    SlotChunk recs[SRECS];
+    uint64_t bar[NSTG];
+    double warp[NT / 32];
+    double res;
+};
+
 template <bool MIX>
 struct VecT {
     using T = double;
@@ -62,28 +106,24 @@ struct VecT<true> {
 struct GridCtx {
     unsigned long long epoch;
     bool ok;
-    unsigned use[2];  // completed uses of each stage (mbarrier phase parity)
+    unsigned use[4];  // completed uses of each stage (mbarrier phase parity)
 };
 
-__device__ __forceinline__ double grid_sum(const CgArgs &a, double local, int slot, GridCtx &gc, SolverSmem &S)
+template <class SM>
+__device__ __forceinline__ double grid_sum(const CgArgs &a, double local, int slot, GridCtx &gc, SM &S)
 {
     const int G = gridDim.x;
     double cta = block_sum<NT>(local, S.warp);
     if (threadIdx.x == 0) a.partials[slot * G + blockIdx.x] = cta;
     gc.epoch++;
-    gc.ok = gc.ok && grid_barrier_sharded(a.bar, gc.epoch, a.status, a.budget_ns);
-    if (threadIdx.x < 32) {
-        double s = warp_sum_partials(a.partials + slot * G, G);
-        if (threadIdx.x == 0) S.res = s;
-    }
-    __syncthreads();
-    return S.res;
+    gc.ok = gc.ok && grid_barrier_fast(a.bar, gc.epoch, a.status, a.budget_ns);
+    return block_sum_partials<NT>(a.partials + slot * G, G, S.warp);
 }
 
 __device__ __forceinline__ void grid_sync(const CgArgs &a, GridCtx &gc)
 {
     gc.epoch++;
-    gc.ok = gc.ok && grid_barrier_sharded(a.bar, gc.epoch, a.status, a.budget_ns);
+    gc.ok = gc.ok && grid_barrier_fast(a.bar, gc.epoch, a.status, a.budget_ns);
 }
 
 // Offset of tile t's u8 row pointers in Blockcsr_Ptr (csrptr_offset without
@@ -325,6 +365,194 @@ __device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb,
     }
 #undef MF_SUB
     return ok;
+}
+
+// One row from the row-slot layout.  mt, vd / hd point at the row's first
+// slot word / value / slot header; consecutive slots are MF_TILE elements
+// (words, values) or one header apart.  pay + (header >> 2) * 16 is a slot's
+// payload.  FP64 (PK 0): per-tile partial sums in the reference's order,
+// products and sums rounded separately (bit-identical to blockspmv_cpu);
+// mixed (PK 1): the slot's format decoded to FP32, fused multiply-add
+// accumulation in row order.  U slots are loaded before any is used.
+template <int PK, class Src>
+__device__ __forceinline__ double slot_row(const unsigned short *mt, const double *vd, const unsigned *hd,
+                                           const unsigned char *pay, const int *tcol, int K, int row, int hl, Src src,
+                                           double &xown, bool &has_own)
+{
+    using XT = decltype(src(0));
+    constexpr int U = SLOT_U;
+    double yd = 0.0, part = 0.0;
+    float yf = 0.f;
+    int prevj = -1;
+    has_own = false;
+    for (int kk = 0; kk < K; kk += U) {
+        unsigned short m[U];
+        double v[U];
+        float f[U];
+        int col[U];
+        XT xv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = kk + u;
+            const bool in = k < K;
+            m[u] = in ? mt[k * MF_TILE] : (unsigned short)0xFFFF;
+            if constexpr (PK == 0) {
+                v[u] = in ? vd[k * MF_TILE] : 0.0;
+            } else {
+                f[u] = 0.f;
+                if (in) {
+                    const unsigned h = hd[k];
+                    const unsigned char *d = pay + (size_t)(h >> 2) * 16;
+                    const unsigned fm = h & 3u;
+                    if (fm == 0u) f[u] = ((const float *)d)[hl];
+                    else if (fm == 1u) f[u] = __half2float(((const __half *)d)[hl]);
+                    else if (fm == 2u) f[u] = (float)((const signed char *)d)[hl];
+                    else m[u] = 0xFFFF;  // every tile of this slot is bypassed
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) col[u] = (m[u] != 0xFFFF) ? tcol[m[u] >> 4] * MF_TILE + (m[u] & 15) : -1;
+#pragma unroll
+        for (int u = 0; u < U; u++) xv[u] = (col[u] >= 0) ? src(col[u]) : (XT)0;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (col[u] < 0) continue;
+            if (col[u] == row) {
+                xown = (double)xv[u];
+                has_own = true;
+            }
+            if constexpr (PK == 0) {
+                const int j = m[u] >> 4;
+                if (j != prevj) {
+                    yd = __dadd_rn(yd, part);
+                    part = 0.0;
+                    prevj = j;
+                }
+                part = __dadd_rn(part, __dmul_rn((double)xv[u], v[u]));
+            } else {
+                yf = fmaf(f[u], (float)xv[u], yf);
+            }
+        }
+    }
+    if constexpr (PK == 0) return __dadd_rn(yd, part);
+    else return (double)yf;
+}
+
+// Thread 0: stage slot chunk c into stage k.
+template <int PK>
+__device__ void issue_slot_chunk(const CgArgs &a, SlotSmem &S, int c, int k)
+{
+    const int cb = a.scta_chunk[blockIdx.x];
+    const SlotChunk r = (c - cb < SRECS) ? S.recs[c - cb] : a.schunks[c];
+    SlotHdr &h = S.hdr[k];
+    h.rec = r;
+    unsigned char *st = S.stage[k];
+    const long long m0 = 2ll * MF_TILE * r.k0, m1 = 2ll * MF_TILE * r.k1;
+    unsigned total = range_bytes(4ll * r.s0, 4ll * (r.s1 + 1)) * 2;
+    if (!r.direct) {
+        total += range_bytes(4ll * r.t0, 4ll * r.t1) + range_bytes(m0, m1);
+        if (PK == 0) total += range_bytes(8ll * MF_TILE * r.k0, 8ll * MF_TILE * r.k1);
+        else total += range_bytes(4ll * r.k0, 4ll * (r.k1 + 1)) + range_bytes(r.y0, r.y1);
+    }
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&S.bar[k], total);
+    add_range(st + SOFF_SSLOT, (const unsigned char *)a.sslot, 4ll * r.s0, 4ll * (r.s1 + 1), &S.bar[k], h.sh_sslot);
+    add_range(st + SOFF_TPTR, (const unsigned char *)a.A.tile_ptr, 4ll * r.s0, 4ll * (r.s1 + 1), &S.bar[k],
+              h.sh_tptr);
+    if (r.direct) return;
+    add_range(st + SOFF_TCOL, (const unsigned char *)a.A.tile_columnidx, 4ll * r.t0, 4ll * r.t1, &S.bar[k],
+              h.sh_tcol);
+    add_range(st + SOFF_META, (const unsigned char *)a.smeta, m0, m1, &S.bar[k], h.sh_meta);
+    if (PK == 0) {
+        add_range(st + SOFF_DATA, (const unsigned char *)a.sval, 8ll * MF_TILE * r.k0, 8ll * MF_TILE * r.k1, &S.bar[k],
+                  h.sh_data);
+    } else {
+        add_range(st + SOFF_DATA, (const unsigned char *)a.shdr, 4ll * r.k0, 4ll * (r.k1 + 1), &S.bar[k], h.sh_data);
+        add_range(st + SOFF_PAY, a.spay, r.y0, r.y1, &S.bar[k], h.sh_pay);
+    }
+}
+
+// y = A src over this CTA's slot chunks [cb, ce); out(s, r, y, xown,
+// has_own) receives every row.  Two chunks in flight: while the CTA
+// computes chunk c from shared memory (one half-warp per strip, one lane per
+// row), the bulk copies of chunk c + 1 are landing; chunk c + 2 is issued as
+// soon as the stage of c is free.  Returns false when a bounded wait expired.
+template <int PK, class Src, class Out>
+__device__ bool spmv_slots(const CgArgs &a, SlotSmem &S, GridCtx &gc, int cb, int ce, Src src, Out &out)
+{
+    const MfTiles &A = a.A;
+    const int tid = threadIdx.x, hw = tid >> 4, hl = tid & 15;
+    if (tid == 0)
+        for (int j = 0; j < NSTG && cb + j < ce; j++) issue_slot_chunk<PK>(a, S, cb + j, j);
+    __syncthreads();
+    bool ok = true;
+    for (int c = cb; c < ce; c++) {
+        const int k = (c - cb) % NSTG;
+        if (!mbar_wait_bounded(&S.bar[k], gc.use[k] & 1u, a.status, a.budget_ns)) {
+            ok = false;
+            // the later stages may still have copies in flight: wait for
+            // them (bounded) before leaving so no copy lands in freed memory
+            for (int j = 1; j < NSTG && c + j < ce; j++) {
+                const int kj = (c + j - cb) % NSTG;
+                mbar_wait_bounded(&S.bar[kj], gc.use[kj] & 1u, a.status, a.budget_ns);
+            }
+            break;
+        }
+        gc.use[k]++;
+        const SlotHdr &h = S.hdr[k];
+        const SlotChunk &rec = h.rec;
+        const unsigned char *st = S.stage[k];
+        const int *ssl = (const int *)(st + SOFF_SSLOT + h.sh_sslot);
+        const int *tpt = (const int *)(st + SOFF_TPTR + h.sh_tptr);
+        if (rec.direct) {
+            // one strip too large for a stage: its rows straight from global memory
+            const int s = rec.s0;
+            const int rowlen = (s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE;
+            if (hw == 0 && hl < rowlen) {
+                const int k0 = ssl[0], K = ssl[1] - k0;
+                const size_t e0 = (size_t)k0 * MF_TILE + hl;
+                double xown = 0.0;
+                bool own = false;
+                const double y = slot_row<PK>(a.smeta + e0, a.sval + e0, a.shdr + k0, a.spay,
+                                              A.tile_columnidx + tpt[0], K, s * MF_TILE + hl, hl, src, xown, own);
+                out(s, hl, y, xown, own);
+            }
+        } else {
+            const int s = rec.s0 + hw;
+            if (s < rec.s1) {
+                const int rowlen = (s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE;
+                if (hl < rowlen) {
+                    const int kA = ssl[hw] - rec.k0, K = ssl[hw + 1] - ssl[hw];
+                    const unsigned short *mt = (const unsigned short *)(st + SOFF_META + h.sh_meta) + kA * MF_TILE + hl;
+                    const double *vd = (const double *)(st + SOFF_DATA + h.sh_data) + kA * MF_TILE + hl;
+                    const unsigned *hd = (const unsigned *)(st + SOFF_DATA + h.sh_data) + kA;
+                    const unsigned char *pay = st + SOFF_PAY + h.sh_pay - rec.y0;
+                    const int *tcl = (const int *)(st + SOFF_TCOL + h.sh_tcol) + (tpt[hw] - rec.t0);
+                    double xown = 0.0;
+                    bool own = false;
+                    const double y = slot_row<PK>(mt, vd, hd, pay, tcl, K, s * MF_TILE + hl, hl, src, xown, own);
+                    out(s, hl, y, xown, own);
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && c + NSTG < ce) issue_slot_chunk<PK>(a, S, c + NSTG, k);
+    }
+    return ok;
+}
+
+// The SpMV of the layout the kernel was built for (LAY 0: staged tile
+// chunks, LAY 1: row slots).
+template <int PK, int LAY, class SM, class Src, class Out>
+__device__ __forceinline__ bool spmv_any(const CgArgs &a, SM &S, GridCtx &gc, int cb, int ce, int sb, int se,
+                                         Src src, Out &out, unsigned long long *tph)
+{
+    if constexpr (LAY == 0) {
+        return spmv_chunks<PK>(a, S, gc, cb, ce, src, out, tph);
+    } else {
+        return spmv_slots<PK>(a, S, gc, cb, ce, src, out);
+    }
 }
 
 }  // namespace persist

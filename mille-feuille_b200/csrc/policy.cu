@@ -69,9 +69,9 @@ __global__ void k_seg_stats(int nseg, int n, const VT *__restrict__ pn, const VT
             rr = fabsf((float)r[j]);
         }
         for (int o = 8; o > 0; o >>= 1) {
-            p = fmaxf(p, __shfl_xor_sync(0xffffffffu, p, o, 16));
-            dp = fmaxf(dp, __shfl_xor_sync(0xffffffffu, dp, o, 16));
-            rr = fmaxf(rr, __shfl_xor_sync(0xffffffffu, rr, o, 16));
+            p = fmaxf(p, __shfl_xor_sync(0xFFFFu << (threadIdx.x & 16), p, o, 16));
+            dp = fmaxf(dp, __shfl_xor_sync(0xFFFFu << (threadIdx.x & 16), dp, o, 16));
+            rr = fmaxf(rr, __shfl_xor_sync(0xFFFFu << (threadIdx.x & 16), rr, o, 16));
         }
         if (lane == 0) {
             sp[s] = p;

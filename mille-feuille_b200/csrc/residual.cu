@@ -28,8 +28,8 @@ __global__ void __launch_bounds__(256) k_resid_strips(MfTiles A, const double *_
         }
 #pragma unroll
         for (int o = 8; o > 0; o >>= 1) {
-            d2 += __shfl_xor_sync(0xffffffffu, d2, o, 16);
-            b2 += __shfl_xor_sync(0xffffffffu, b2, o, 16);
+            d2 += __shfl_xor_sync(0xFFFFu << (threadIdx.x & 16), d2, o, 16);
+            b2 += __shfl_xor_sync(0xFFFFu << (threadIdx.x & 16), b2, o, 16);
         }
         if (r == 0) {
             part[2 * s] = d2;

@@ -14,22 +14,38 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
                                   const TraceHook *hook = nullptr)
 {
     const bool mixed = o.policy != MF_POLICY_FP64;
-    const int G = bicg ? bicgstab_grid(m, mixed) : solver_grid(m, mixed);
-    if (m->part_ctas != G || !m->d_chunks) {
+    // execution layout: row slots unless disabled or not describable
+    const char *lay = getenv("MF_SOLVER_LAYOUT");
+    const bool want_slots = !(lay && !strcmp(lay, "tiles"));
+    if (want_slots) MF_TRY(build_slots(m, s));
+    const bool slots = want_slots && m->slots_state == 1;
+    const int G = bicg ? bicgstab_grid(m, mixed, slots) : solver_grid(m, mixed, slots);
+    if (m->part_ctas != G || (!slots && !m->d_chunks)) {
         MF_TRY(strip_partition(m, G, s));
-        MF_TRY(build_chunks(m, s));
+        if (!slots) MF_TRY(build_chunks(m, s));
         m->packed_policy = -1;  // chunk payload offsets must be refreshed
     }
+    if (slots) MF_TRY(build_slot_chunks(m, G, s));
     SolverWork w;
     MF_TRY(solver_resources(m, G, w));
     const int T = m->v.tilenum;
+    // repack the payload of the layout in use for the classes in d_wcls
+    auto repack = [&](int policy) -> mf_status {
+        MF_TRY(pack_payload(m, m->d_wcls, s));  // also counts the algorithmic payload bytes
+        if (slots) {
+            MF_TRY(pack_slots(m, m->d_wcls, s));
+            m->slot_policy = policy;
+        } else {
+            MF_TRY(refresh_chunk_payload(m, s));
+            m->packed_policy = policy;
+        }
+        return MF_OK;
+    };
     if (mixed) {
         if (!m->d_wcls) MF_CUDA(cudaMalloc(&m->d_wcls, (size_t)T + 16));
-        if (m->packed_policy != MF_POLICY_STATIC) {
+        if ((slots ? m->slot_policy : m->packed_policy) != MF_POLICY_STATIC) {
             MF_TRY(static_working_classes(m, m->d_wcls, s));
-            MF_TRY(pack_payload(m, m->d_wcls, s));
-            MF_TRY(refresh_chunk_payload(m, s));
-            m->packed_policy = MF_POLICY_STATIC;
+            MF_TRY(repack(MF_POLICY_STATIC));
         }
     }
     if (o.policy == MF_POLICY_LEARNED) m->pol_have_prev = 0;  // no history from an earlier solve
@@ -41,6 +57,15 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
     a.chunks = (const ChunkRec *)m->d_chunks;
     a.last_tile_begin = m->last_tile_begin;
     a.last_rowlen = m->v.rows - (m->v.tilem - 1) * MF_TILE;
+    if (slots) {
+        a.sslot = m->d_sslot;
+        a.smeta = m->d_smeta;
+        a.sval = m->d_sval;
+        a.shdr = m->d_shdr;
+        a.spay = m->d_spay;
+        a.scta_chunk = m->d_scta_chunk;
+        a.schunks = (const SlotChunk *)m->d_schunks;
+    }
     a.pay = m->d_pay;
     a.poff = m->d_poff;
     a.wcls = m->d_wcls;
@@ -103,9 +128,7 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
         } else {
             MF_TRY(learned_working_classes(m, w, pnew, pold, m->d_wcls, s));
         }
-        MF_TRY(pack_payload(m, m->d_wcls, s));
-        MF_TRY(refresh_chunk_payload(m, s));
-        m->packed_policy = o.policy;
+        MF_TRY(repack(o.policy));
         a.start = 0;
     }
     MF_CUDA(cudaEventRecord(e1, s));

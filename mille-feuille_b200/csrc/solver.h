@@ -23,6 +23,19 @@ struct ChunkRec {
     int pad;
 };
 
+// A chunk of the row-slot layout: consecutive strips of one CTA whose slot
+// words, values (or mixed payload) and tile columns fit one shared-memory
+// stage.  A strip too large for a stage on its own is a one-strip chunk with
+// `direct` set (computed from global memory).
+constexpr int SC_STRIPS = 16, SC_SLOTS = 128, SC_TILES = 256;
+struct SlotChunk {
+    int s0, s1;            // strips [s0, s1)
+    int k0, k1;            // slots [k0, k1)
+    int t0, t1;            // tiles [t0, t1)
+    int direct, pad;
+    long long y0, y1;      // mixed payload bytes [y0, y1)
+};
+
 // Persistent solver state kept in device memory between launches.
 enum : int { S_RHO = 0, S_BETA, S_NB, S_RMAX, S_ITERS, S_REFS, S_EXIT, S_RELRES, S_ALPHA, S_OMEGA, S_COUNT };
 // Why a launch returned.
@@ -56,6 +69,14 @@ struct CgArgs {
     unsigned long long *timing;    // optional [G][8] per-CTA phase nanoseconds
     int last_tile_begin;           // first tile of the last strip
     int last_rowlen;               // rows of the last strip
+    // row-slot layout (null when the kernel runs from tile chunks)
+    const int *sslot;              // [tilem+1] first slot of each strip
+    const uint16_t *smeta;         // [slots*16] tile-in-strip << 4 | in-tile column
+    const double *sval;            // [slots*16] FP64 values
+    const unsigned *shdr;          // mixed: [slots] payload offset (16 B) << 2 | format
+    const unsigned char *spay;     // mixed: slot payload
+    const int *scta_chunk;         // [G+1] slot-chunk range of each CTA
+    const SlotChunk *schunks;
 };
 
 struct SolverWork {
@@ -82,10 +103,14 @@ mf_status cg_solve_traced(mf_matrix m, const double *b, double *x, const mf_solv
 // chunks.cu: chunk table for the current partition; payload offsets refresh
 mf_status build_chunks(mf_matrix m, cudaStream_t s);
 mf_status refresh_chunk_payload(mf_matrix m, cudaStream_t s);
-int solver_grid(mf_matrix m, bool mixed);
+int solver_grid(mf_matrix m, bool mixed, bool slots);
 mf_status launch_cg(bool mixed, CgArgs &a, int G, cudaStream_t s);
 mf_status launch_bicgstab(bool mixed, CgArgs &a, int G, cudaStream_t s);
-int bicgstab_grid(mf_matrix m, bool mixed);
+int bicgstab_grid(mf_matrix m, bool mixed, bool slots);
+// slots.cu: the row-slot layout (built once; state -1 = not describable)
+mf_status build_slots(mf_matrix m, cudaStream_t s);
+mf_status pack_slots(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s);
+mf_status build_slot_chunks(mf_matrix m, int G, cudaStream_t s);
 mf_status true_residual(mf_matrix m, const double *b, const double *x, SolverWork &w, double *relres, cudaStream_t s);
 // payload.cu
 mf_status pack_payload(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s);

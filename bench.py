@@ -1,23 +1,35 @@
 #!/usr/bin/env python
 """Benchmark: CG solves/s to relative residual 1e-10 on one B200.
 
-Workload (default): the 3D 7-point 128^3 configuration (n = 2,097,152,
-nnz = 14,581,760; off-diagonals -(f_i+f_j)/2 with f = 10^U[-3,0], diagonal
-row |sum| + 1e-3, b = A x*, x* ~ U[-1,1], seed 1).  One step = one full solve
-from x0 = 0 to ||b - A x|| / ||b|| <= 1e-10 with the matrix resident in HBM.
+Workloads (--workload):
+  poisson3d (default) 3D 7-point 128^3 (n = 2,097,152, nnz = 14,581,760;
+                  off-diagonals -(f_i+f_j)/2 with f = 10^U[-3,0], diagonal
+                  row |sum| + 1e-3, b = A x*, x* ~ U[-1,1], seed 1), solved
+                  with tile mixed precision and FP64 refinement (--policy
+                  static); the plain FP64 tiled solve of the same system is
+                  timed in the same run (fp64 key).  One step = one solve
+                  from x0 = 0 to ||b - A x|| / ||b|| <= 1e-10, matrix
+                  resident in HBM.
+  batched         512 random SPD systems, n ~ log-uniform[1k, 64k], seeds
+                  100-611, one graph-captured batched launch per step; the
+                  plain FP64 tiled solves of the same systems one after
+                  another are timed beside it (fp64 key).
+  convdiff        BiCGSTAB on the 96^3 convection-diffusion system to 1e-9.
+  aniso           160^3 anisotropic diffusion (seed 3) with a learned policy
+                  file (--policy-file), the rule policy and plain FP64.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mf|reference]
 
 --impl mf        this library (value: device-resident solves; e2e: the
-                 host-buffer C-ABI call mf_cg_solve_host, b in and x out
-                 through pinned host memory every step)
+                 host-buffer call, b in and x out through pinned host memory
+                 every step)
 --impl reference the reference's own CPU tiled path (Tile_create +
                  blockspmv_cpu from the reference sources, with a CG loop
-                 around it), timed on the host cores on a bounded sample
+                 around it) on the default workload, timed on the host cores
+                 on a bounded sample
 
 N > 1 runs independent replicas, one per GPU (a single system does not
-shard), timed with CUDA events and reported as the max over
-ranks.
+shard), timed with CUDA events and reported as the max over ranks.
 """
 from __future__ import annotations
 
@@ -205,6 +217,271 @@ def run_reference(args):
     return 0
 
 
+def _timed(stream, fn, steps):
+    """Device time of `steps` calls of fn (CUDA events on the launching stream)."""
+    import torch
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        fn()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1)
+
+
+def _max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def tiles_of(A):
+    """Number of non-empty 16x16 tiles of a host CSR matrix."""
+    rows = np.repeat(np.arange(A.n_rows, dtype=np.int64), np.diff(A.rowptr))
+    key = (rows // 16) * ((A.n_cols + 15) // 16) + A.colidx.astype(np.int64) // 16
+    return int(np.unique(key).size)
+
+
+def workload_single(args, mf, world, local):
+    """poisson3d / convdiff / aniso: one system, device-resident solves."""
+    import torch
+
+    L = mf.lib()
+    method = "bicgstab" if args.workload == "convdiff" else "cg"
+    if args.workload == "poisson3d":
+        A = mf.synth_poisson3d_scaled(GRID, SEED)
+        seed, tol, name = SEED, TOL, f"poisson3d_scaled_{GRID}^3 CG to 1e-10"
+    elif args.workload == "convdiff":
+        A = mf.synth_convdiff3d(96)
+        seed, tol, name = 2, 1e-9, "convdiff3d_96^3 BiCGSTAB to 1e-9"
+    else:
+        A = mf.synth_aniso3d(160, 3)
+        seed, tol, name = 3, TOL, "aniso3d_160^3 (lognormal k, sigma 2, corr 8, k_z x100) CG to 1e-10"
+    xs = mf.synth_xstar(seed, A.n_rows)
+    b = A.matvec(xs)
+    t0 = time.perf_counter()
+    M = mf.Matrix(A)
+    torch.cuda.synchronize()
+    setup_ms = (time.perf_counter() - t0) * 1e3
+    pol = None
+    if args.policy == "learned":
+        if not args.policy_file:
+            raise SystemExit("--policy learned needs --policy-file")
+        pol = mf.Policy.load(args.policy_file)
+        M.attach_policy(pol)
+    n = A.n_rows
+    db = torch.from_numpy(b).cuda()
+    dx = torch.zeros(n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    fn_dev = L.mf_bicgstab_solve if method == "bicgstab" else L.mf_cg_solve
+    fn_host = L.mf_bicgstab_solve_host if method == "bicgstab" else L.mf_cg_solve_host
+
+    def opts_for(policy):
+        if args.iters:
+            return mf.solve_opts(tol=-1.0, maxiter=args.iters, policy=policy)
+        return mf.solve_opts(tol=tol, maxiter=50000, policy=policy)
+
+    def make_solve(policy, rep):
+        o = opts_for(policy)
+
+        def solve():
+            st = fn_dev(M.h, db.data_ptr(), dx.data_ptr(), C.byref(o), C.byref(rep), None, stream.cuda_stream)
+            if st != 0:
+                mf.check(st)
+        return solve
+
+    rep = mf.SolveReport()
+    solve = make_solve(args.policy, rep)
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize()
+    _barrier(world)
+    torch.cuda.synchronize()
+    launches0 = L.mf_kernel_launches()
+    kernel_ms, iters, bytes_moved = [], [], []
+
+    def step():
+        solve()
+        kernel_ms.append(rep.kernel_ms)
+        iters.append(rep.iterations)
+        bytes_moved.append(rep.bytes_moved)
+
+    with ClockSampler(local) as clk:
+        ms = _timed(stream, step, args.steps)
+    launches = L.mf_kernel_launches() - launches0
+    ms = _max_over_ranks(ms, world)
+    value = args.steps * world / (ms * 1e-3)
+    result = {"rep": rep, "ms": ms, "value": value, "launches": launches, "clocks": clk.summary(),
+              "kernel_ms": kernel_ms, "iters": iters, "bytes_moved": bytes_moved}
+    if args.profile:
+        return result, None
+    relres_true = rep.relres_true
+    x_err = float(torch.max(torch.abs(dx.cpu() - torch.from_numpy(xs))).item())
+    info = {"workload": name, "n": n, "nnz": A.nnz, "seed": seed, "policy": args.policy,
+            "iterations": int(statistics.mean(iters)), "refinements": int(rep.refinements),
+            "relres_true": relres_true, "max_abs_err_vs_xstar": x_err, "setup_ms": setup_ms,
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (matrix > 126 MB L2); no flush"}
+    # the plain FP64 tiled solve of the same system, same box, same run
+    if args.policy != "fp64" and not args.iters:
+        rep64 = mf.SolveReport()
+        s64 = make_solve("fp64", rep64)
+        s64()
+        torch.cuda.synchronize()
+        _barrier(world)
+        k = max(3, args.steps // 2)
+        ms64 = _max_over_ranks(_timed(stream, s64, k), world)
+        info["fp64"] = {"value": k * world / (ms64 * 1e-3), "unit": UNIT, "iterations": rep64.iterations,
+                        "relres_true": rep64.relres_true, "steps": k}
+        if args.workload == "aniso" and args.policy == "learned":
+            repr_ = mf.SolveReport()
+            sr = make_solve("rule", repr_)
+            sr()
+            torch.cuda.synchronize()
+            msr = _max_over_ranks(_timed(stream, sr, k), world)
+            info["rule"] = {"value": k * world / (msr * 1e-3), "unit": UNIT, "iterations": repr_.iterations,
+                            "relres_true": repr_.relres_true, "steps": k}
+    # e2e: the host-buffer C-ABI call, pinned b in and x out every step
+    o = opts_for(args.policy)
+    b_pin = torch.from_numpy(b).pin_memory()
+    x_pin = torch.zeros(n, dtype=torch.float64).pin_memory()
+    erep = mf.SolveReport()
+    fn_host(M.h, b_pin.data_ptr(), x_pin.data_ptr(), C.byref(o), C.byref(erep))
+    torch.cuda.synchronize()
+    _barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st = fn_host(M.h, b_pin.data_ptr(), x_pin.data_ptr(), C.byref(o), C.byref(erep))
+        if st != 0:
+            mf.check(st)
+    torch.cuda.synchronize()
+    e2e_s = _max_over_ranks(time.perf_counter() - t0, world)
+    result["e2e"] = {"value": args.steps * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
+                     "d2h_bytes_per_step": 8 * n}
+    mean_ms = statistics.mean(kernel_ms)
+    per_launch = statistics.mean(bytes_moved)
+    kname = ("k_bicgstab" if method == "bicgstab" else "k_cg") + ("_fp64" if args.policy == "fp64" else "_mixed")
+    result["roofline_in"] = (per_launch, mean_ms, kname, statistics.mean(iters))
+    result["dtype"] = "f64" if args.policy == "fp64" else "mixed(f32/f16/i8 tiles, f32 accumulate, f64 refinement)"
+    result["cpu"] = (A, b) if args.workload == "poisson3d" else None
+    M.close()
+    return result, info
+
+
+def workload_batched(args, mf, world, local):
+    """512 random SPD systems in one graph-captured batched launch."""
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+
+    L = mf.lib()
+    N = 512
+    with ThreadPoolExecutor(16) as ex:
+        systems = list(ex.map(lambda k: mf.synth_random_spd(100 + k), range(N)))
+        xs = list(ex.map(lambda k: mf.synth_xstar(100 + k, systems[k].n_rows), range(N)))
+    bs = [A.matvec(x) for A, x in zip(systems, xs)]
+    t0 = time.perf_counter()
+    B = mf.Batch(systems)
+    setup_ms = (time.perf_counter() - t0) * 1e3
+    bstack = B.stack(bs)
+    db = torch.from_numpy(bstack).cuda()
+    dx = torch.zeros_like(db)
+    stream = torch.cuda.current_stream()
+    o = mf.solve_opts(tol=TOL, maxiter=50000, policy=args.policy)
+    rep = mf.BatchReport()
+
+    def solve():
+        st = L.mf_batch_cg_solve(B.h, db.data_ptr(), dx.data_ptr(), C.byref(o), 1, C.byref(rep),
+                                 stream.cuda_stream)
+        if st != 0:
+            mf.check(st)
+
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize()
+    _barrier(world)
+    launches0 = L.mf_kernel_launches()
+    kernel_ms = []
+
+    def step():
+        solve()
+        kernel_ms.append(rep.kernel_ms)
+
+    with ClockSampler(local) as clk:
+        ms = _timed(stream, step, args.steps)
+    launches = L.mf_kernel_launches() - launches0
+    ms = _max_over_ranks(ms, world)
+    its, rr = B.results()
+    value = N * args.steps * world / (ms * 1e-3)
+    result = {"rep": rep, "ms": ms, "value": value, "launches": launches, "clocks": clk.summary()}
+    if args.profile:
+        return result, None
+    # algorithmic bytes of the launch: per system and iteration, the FP64
+    # tiled SpMV (or its FP32 counterpart) plus the CG vector streams
+    sb = 8 if args.policy == "fp64" else 4
+    vb = 72 if args.policy == "fp64" else 36
+    alg = 0
+    for A, it in zip(systems, its):
+        alg += int(it) * (A.nnz * (sb + 1) + 24 * tiles_of(A) + 16 * A.n_rows + vb * A.n_rows)
+    info = {"workload": "batched random SPD x512 (n ~ log-uniform[1k,64k], seeds 100-611) CG to 1e-10",
+            "systems": N, "rows_total": int(sum(A.n_rows for A in systems)),
+            "nnz_total": int(sum(A.nnz for A in systems)), "policy": args.policy,
+            "iterations_mean": float(its.mean()), "iterations_max": int(its.max()),
+            "relres_true_max": float(rep.relres_true_max), "failed": int(rep.failed), "setup_ms": setup_ms,
+            "lanes_per_row": int(rep.lanes_per_row), "cluster_ctas": int(rep.cluster_ctas),
+            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2; no flush"}
+    # the plain FP64 tiled solves of the same systems, one after another
+    if not args.no_fp64_baseline:
+        dbs = [torch.from_numpy(bv).cuda() for bv in bs]
+        mats = [mf.Matrix(A) for A in systems]
+        o64 = mf.solve_opts(tol=TOL, maxiter=50000, policy="fp64")
+        r64 = mf.SolveReport()
+        xk = torch.zeros(max(A.n_rows for A in systems), dtype=torch.float64, device="cuda")
+
+        def seq():
+            for M_, d in zip(mats, dbs):
+                L.mf_cg_solve(M_.h, d.data_ptr(), xk.data_ptr(), C.byref(o64), C.byref(r64), None,
+                              stream.cuda_stream)
+
+        seq()
+        torch.cuda.synchronize()
+        ms64 = _max_over_ranks(_timed(stream, seq, 1), world)
+        info["fp64"] = {"value": N * world / (ms64 * 1e-3), "unit": UNIT,
+                        "what": "the same 512 systems solved one after another by the plain FP64 tiled CG"}
+        for M_ in mats:
+            M_.close()
+    # e2e: stacked b from pinned host memory, solve, x back, every step
+    b_pin = torch.from_numpy(bstack).pin_memory()
+    x_pin = torch.zeros_like(b_pin).pin_memory()
+    _barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        db.copy_(b_pin, non_blocking=True)
+        solve()
+        x_pin.copy_(dx, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_s = _max_over_ranks(time.perf_counter() - t0, world)
+    result["e2e"] = {"value": N * args.steps * world / e2e_s, "unit": UNIT,
+                     "h2d_bytes_per_step": 8 * len(bstack), "d2h_bytes_per_step": 8 * len(bstack)}
+    result["roofline_in"] = (alg, statistics.mean(kernel_ms), "k_batched_cg", None)
+    result["dtype"] = "f64" if args.policy == "fp64" else "mixed(f32 values, f32 accumulate, f64 refinement)"
+    result["cpu"] = None
+    B.close()
+    return result, info
+
+
 def run_mf(args):
     import torch
     import torch.distributed as dist
@@ -220,110 +497,35 @@ def run_mf(args):
     import __graft_entry__ as ge
 
     mf = ge.load_package()
-    L = mf.lib()
-    A, xs, b = build_problem(mf)
-    t0 = time.perf_counter()
-    M = mf.Matrix(A)
-    torch.cuda.synchronize()
-    setup_ms = (time.perf_counter() - t0) * 1e3
-    n = A.n_rows
-    db = torch.from_numpy(b).cuda()
-    dx = torch.zeros(n, dtype=torch.float64, device="cuda")
-    stream = torch.cuda.current_stream()
-    if args.iters:
-        opts = mf.solve_opts(tol=-1.0, maxiter=args.iters, policy=args.policy)
+    if args.workload == "batched":
+        res, info = workload_batched(args, mf, world, local)
     else:
-        opts = mf.solve_opts(tol=TOL, maxiter=20000, policy=args.policy)
-    rep = mf.SolveReport()
-
-    def solve():
-        st = L.mf_cg_solve(M.h, db.data_ptr(), dx.data_ptr(), C.byref(opts), C.byref(rep), None, stream.cuda_stream)
-        if st != 0:
-            mf.check(st)
-
-    for _ in range(args.warmup):
-        solve()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = L.mf_kernel_launches()
-    kernel_ms, iters, bytes_moved = [], [], []
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            solve()
-            kernel_ms.append(rep.kernel_ms)
-            iters.append(rep.iterations)
-            bytes_moved.append(rep.bytes_moved)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    launches = L.mf_kernel_launches() - launches0
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = args.steps * world / (ms * 1e-3)
+        res, info = workload_single(args, mf, world, local)
     if args.profile:
         if rank == 0:
-            print(json.dumps({"profile_run": True, "ms_per_step": ms / args.steps, "iterations": rep.iterations,
-                              "kernel_ms": rep.kernel_ms, "launches": int(launches)}))
-        M.close()
+            print(json.dumps({"profile_run": True, "ms_per_step": res["ms"] / args.steps,
+                              "launches": int(res["launches"])}))
         if world > 1:
             dist.destroy_process_group()
         return 0
-    relres_true = rep.relres_true
-    x_err = float(torch.max(torch.abs(dx.cpu() - torch.from_numpy(xs))).item())
-
-    # e2e: the host-buffer C-ABI call, pinned b in and x out every step
-    b_pin = torch.from_numpy(b).pin_memory()
-    x_pin = torch.zeros(n, dtype=torch.float64).pin_memory()
-    erep = mf.SolveReport()
-    for _ in range(1):
-        L.mf_cg_solve_host(M.h, b_pin.data_ptr(), x_pin.data_ptr(), C.byref(opts), C.byref(erep))
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        st = L.mf_cg_solve_host(M.h, b_pin.data_ptr(), x_pin.data_ptr(), C.byref(opts), C.byref(erep))
-        if st != 0:
-            mf.check(st)
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = args.steps * world / e2e_s
-
     peak, peak_kind = load_peaks()
-    mean_ms = statistics.mean(kernel_ms)
-    per_launch_bytes = statistics.mean(bytes_moved)
-    achieved = per_launch_bytes / (mean_ms * 1e-3) / 1e9
-    kname = "k_cg_fp64" if args.policy == "fp64" else "k_cg_mixed"
+    per_launch, mean_ms, kname, mean_iters = res["roofline_in"]
+    achieved = per_launch / (mean_ms * 1e-3) / 1e9
     tr = ncu_traffic(kname)
-    traffic = None if tr is None else tr["dram_bytes_per_iteration"] * statistics.mean(iters)
+    traffic = None
+    if tr is not None and mean_iters is not None:
+        traffic = tr["dram_bytes_per_iteration"] * mean_iters
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_kind": peak_kind, "kernel": kname,
-                "algorithmic_bytes_per_launch": per_launch_bytes, "launch_ms": mean_ms}
+                "algorithmic_bytes_per_launch": per_launch, "launch_ms": mean_ms}
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.policy == "fp64" else "mixed(f16/f32 tiles, f32 accumulate, f64 refinement)",
-        "data": "synthetic",
-        "config": {"workload": f"poisson3d_scaled_{GRID}^3 CG to 1e-10", "n": n, "nnz": A.nnz, "seed": SEED,
-                   "policy": args.policy, "iterations": int(statistics.mean(iters)), "relres_true": relres_true,
-                   "max_abs_err_vs_xstar": x_err, "setup_ms": setup_ms, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (matrix ~200 MB vs 126 MB L2); no flush"},
-        "roofline": roofline,
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
-        "gpu_launches": int(launches),
-        "clocks": clk.summary(),
+        "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": res["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": res["dtype"], "data": "synthetic", "config": info, "roofline": roofline,
+        "e2e": res["e2e"], "gpu_launches": int(res["launches"]), "clocks": res["clocks"],
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and res["cpu"] is not None:
+        A, b = res["cpu"]
         cpu = CpuReference(A, b)
         if cpu.ref is not None:
             k = cpu.auto_iters(15.0)
@@ -336,7 +538,6 @@ def run_mf(args):
                                               f"not timed"}
     if rank == 0:
         print(json.dumps(line))
-    M.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
@@ -348,7 +549,10 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mf", "reference"], default="mf")
-    ap.add_argument("--policy", default="fp64", choices=["fp64", "static", "rule", "learned"])
+    ap.add_argument("--workload", default="poisson3d", choices=["poisson3d", "batched", "convdiff", "aniso"])
+    ap.add_argument("--policy", default="static", choices=["fp64", "static", "rule", "learned"])
+    ap.add_argument("--policy-file", default=None, help="learned policy (mf_policy_save format)")
+    ap.add_argument("--no-fp64-baseline", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="device solves only (no e2e, clocks or CPU baseline): the command profiled with ncu")

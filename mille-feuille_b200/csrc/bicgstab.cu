@@ -16,6 +16,7 @@
 // the next SpMV starts.  Mixed precision follows the CG solver: packed
 // per-tile classes, FP32 vectors and accumulation, FP64 dot products and
 // FP64 reliable updates of the residual.
+#include <algorithm>
 #include <type_traits>
 
 #include "persist.cuh"
@@ -279,6 +280,8 @@ int bicgstab_grid(mf_matrix m, bool mixed, bool slots)
         if (v > 0 && v < maxc) maxc = v;
     }
     int want = ceil_div(m->v.tilem, CH_STRIPS);
+    // strips with long rows: enough CTAs for the slots, not only the strips
+    if (slots && m->nslots > 0) want = std::max<long long>(want, (m->nslots + SC_SLOTS - 1) / SC_SLOTS);
     if (want < 1) want = 1;
     return want < maxc ? want : maxc;
 }

@@ -28,6 +28,7 @@
 //     by refine_delta, the FP32 correction is added to the FP64 solution and
 //     r is replaced by the FP64 true residual b - A x computed from the FP64
 //     payload.  Convergence is only declared on that FP64 true residual.
+#include <algorithm>
 #include <type_traits>
 
 #include "persist.cuh"
@@ -358,6 +359,8 @@ int solver_grid(mf_matrix m, bool mixed, bool slots)
         if (v > 0 && v < maxc) maxc = v;
     }
     int want = ceil_div(m->v.tilem, CH_STRIPS);
+    // strips with long rows: enough CTAs for the slots, not only the strips
+    if (slots && m->nslots > 0) want = std::max<long long>(want, (m->nslots + SC_SLOTS - 1) / SC_SLOTS);
     if (want < 1) want = 1;
     return want < maxc ? want : maxc;
 }

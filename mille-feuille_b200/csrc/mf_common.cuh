@@ -229,7 +229,7 @@ template <int NT>
 __device__ __forceinline__ double block_sum_partials(const double *part, int count, double *s_warp)
 {
     double s = 0.0;
-    constexpr int B = 4;
+    constexpr int B = 2;
     for (int i0 = threadIdx.x; i0 < count; i0 += NT * B) {
         double v[B];
 #pragma unroll

@@ -89,6 +89,8 @@ struct __align__(16) SlotSmem {
     unsigned char stage[NSTG][SSTAGE_BYTES];
     SlotHdr hdr[NSTG];
     SlotChunk recs[SRECS];
+    double py[NT], px[NT];  // per-thread partial row sums / own p values (strips shared by half-warps)
+    unsigned char pown[NT];
     uint64_t bar[NSTG];
     double warp[NT / 32];
     double res;
@@ -313,7 +315,8 @@ __device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb,
     bool ok = true;
     for (int c = cb; c < ce; c++) {
         const int k = (c - cb) & 1;
-        if (!mbar_wait_bounded(&S.bar[k], gc.use[k] & 1u, a.status, a.budget_ns)) {
+        // CTA-wide vote on the bounded wait so that every thread leaves together
+        if (!__syncthreads_and(mbar_wait_bounded(&S.bar[k], gc.use[k] & 1u, a.status, a.budget_ns))) {
             ok = false;
             // the other stage may still have a copy in flight: wait for it
             // (bounded) before leaving so no copy lands in freed memory
@@ -439,12 +442,17 @@ __device__ __forceinline__ double slot_row(const unsigned short *mt, const doubl
     else return (double)yf;
 }
 
+__device__ __forceinline__ SlotChunk slot_rec(const CgArgs &a, const SlotSmem &S, int cb, int c)
+{
+    return (c - cb < SRECS) ? S.recs[c - cb] : a.schunks[c];
+}
+
 // Thread 0: stage slot chunk c into stage k.
 template <int PK>
 __device__ void issue_slot_chunk(const CgArgs &a, SlotSmem &S, int c, int k)
 {
     const int cb = a.scta_chunk[blockIdx.x];
-    const SlotChunk r = (c - cb < SRECS) ? S.recs[c - cb] : a.schunks[c];
+    const SlotChunk r = slot_rec(a, S, cb, c);
     SlotHdr &h = S.hdr[k];
     h.rec = r;
     unsigned char *st = S.stage[k];
@@ -474,10 +482,14 @@ __device__ void issue_slot_chunk(const CgArgs &a, SlotSmem &S, int c, int k)
 }
 
 // y = A src over this CTA's slot chunks [cb, ce); out(s, r, y, xown,
-// has_own) receives every row.  Two chunks in flight: while the CTA
-// computes chunk c from shared memory (one half-warp per strip, one lane per
-// row), the bulk copies of chunk c + 1 are landing; chunk c + 2 is issued as
-// soon as the stage of c is free.  Returns false when a bounded wait expired.
+// has_own) receives every row.  Chunks stream through NSTG shared-memory
+// stages: while the CTA computes one chunk (one half-warp per strip, one
+// lane per row), the bulk copies of the next ones are landing; a stage is
+// refilled as soon as the CTA is done with it.  Every thread waits for its
+// chunk's data itself; a thread whose bounded wait expired computes nothing,
+// and the barrier closing the chunk votes, so that the whole CTA leaves
+// together -- after waiting (bounded) for the copies still in flight, so
+// that none lands in freed shared memory.  Returns false when a wait expired.
 template <int PK, class Src, class Out>
 __device__ bool spmv_slots(const CgArgs &a, SlotSmem &S, GridCtx &gc, int cb, int ce, Src src, Out &out)
 {
@@ -486,45 +498,27 @@ __device__ bool spmv_slots(const CgArgs &a, SlotSmem &S, GridCtx &gc, int cb, in
     if (tid == 0)
         for (int j = 0; j < NSTG && cb + j < ce; j++) issue_slot_chunk<PK>(a, S, cb + j, j);
     __syncthreads();
-    bool ok = true;
     for (int c = cb; c < ce; c++) {
         const int k = (c - cb) % NSTG;
-        if (!mbar_wait_bounded(&S.bar[k], gc.use[k] & 1u, a.status, a.budget_ns)) {
-            ok = false;
-            // the later stages may still have copies in flight: wait for
-            // them (bounded) before leaving so no copy lands in freed memory
-            for (int j = 1; j < NSTG && c + j < ce; j++) {
-                const int kj = (c + j - cb) % NSTG;
-                mbar_wait_bounded(&S.bar[kj], gc.use[kj] & 1u, a.status, a.budget_ns);
-            }
-            break;
-        }
+        const bool w = mbar_wait_bounded(&S.bar[k], gc.use[k] & 1u, a.status, a.budget_ns);
         gc.use[k]++;
         const SlotHdr &h = S.hdr[k];
         const SlotChunk &rec = h.rec;
-        const unsigned char *st = S.stage[k];
-        const int *ssl = (const int *)(st + SOFF_SSLOT + h.sh_sslot);
-        const int *tpt = (const int *)(st + SOFF_TPTR + h.sh_tptr);
-        if (rec.direct) {
-            // one strip too large for a stage: its rows straight from global memory
-            const int s = rec.s0;
-            const int rowlen = (s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE;
-            if (hw == 0 && hl < rowlen) {
-                const int k0 = ssl[0], K = ssl[1] - k0;
-                const size_t e0 = (size_t)k0 * MF_TILE + hl;
-                double xown = 0.0;
-                bool own = false;
-                const double y = slot_row<PK>(a.smeta + e0, a.sval + e0, a.shdr + k0, a.spay,
-                                              A.tile_columnidx + tpt[0], K, s * MF_TILE + hl, hl, src, xown, own);
-                out(s, hl, y, xown, own);
-            }
-        } else {
+        // the header is valid whether or not the data arrived (written before
+        // the copies were issued), so L and the barriers below are uniform
+        const int L = rec.lanes;
+        if (L == 1) {
+            // one half-warp per strip, one lane per row, from the stage
             const int s = rec.s0 + hw;
-            if (s < rec.s1) {
+            if (w && s < rec.s1) {
                 const int rowlen = (s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE;
                 if (hl < rowlen) {
+                    const unsigned char *st = S.stage[k];
+                    const int *ssl = (const int *)(st + SOFF_SSLOT + h.sh_sslot);
+                    const int *tpt = (const int *)(st + SOFF_TPTR + h.sh_tptr);
                     const int kA = ssl[hw] - rec.k0, K = ssl[hw + 1] - ssl[hw];
-                    const unsigned short *mt = (const unsigned short *)(st + SOFF_META + h.sh_meta) + kA * MF_TILE + hl;
+                    const unsigned short *mt =
+                        (const unsigned short *)(st + SOFF_META + h.sh_meta) + kA * MF_TILE + hl;
                     const double *vd = (const double *)(st + SOFF_DATA + h.sh_data) + kA * MF_TILE + hl;
                     const unsigned *hd = (const unsigned *)(st + SOFF_DATA + h.sh_data) + kA;
                     const unsigned char *pay = st + SOFF_PAY + h.sh_pay - rec.y0;
@@ -535,11 +529,69 @@ __device__ bool spmv_slots(const CgArgs &a, SlotSmem &S, GridCtx &gc, int cb, in
                     out(s, hl, y, xown, own);
                 }
             }
+        } else {
+            // L half-warps per strip, each on a contiguous part of its slots;
+            // the parts' sums are added in order
+            const int j = hw / L, part = hw % L;
+            const int s = rec.s0 + j;
+            const bool row_ok = w && s < rec.s1 && hl < ((s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE);
+            double y = 0.0, xown = 0.0;
+            bool own = false;
+            if (row_ok) {
+                const unsigned char *st = S.stage[k];
+                const int *ssl = (const int *)(st + SOFF_SSLOT + h.sh_sslot);
+                const int *tpt = (const int *)(st + SOFF_TPTR + h.sh_tptr);
+                const int K = ssl[j + 1] - ssl[j];
+                const int kb = K * part / L, ke = K * (part + 1) / L;
+                const int row = s * MF_TILE + hl;
+                if (rec.direct) {
+                    // one strip too large for a stage: read from global memory
+                    const int k0 = ssl[0] + kb;
+                    const size_t e0 = (size_t)k0 * MF_TILE + hl;
+                    y = slot_row<PK>(a.smeta + e0, a.sval + e0, a.shdr + k0, a.spay, A.tile_columnidx + tpt[0],
+                                     ke - kb, row, hl, src, xown, own);
+                } else {
+                    const int kA = ssl[j] - rec.k0 + kb;
+                    const unsigned short *mt =
+                        (const unsigned short *)(st + SOFF_META + h.sh_meta) + kA * MF_TILE + hl;
+                    const double *vd = (const double *)(st + SOFF_DATA + h.sh_data) + kA * MF_TILE + hl;
+                    const unsigned *hd = (const unsigned *)(st + SOFF_DATA + h.sh_data) + kA;
+                    const unsigned char *pay = st + SOFF_PAY + h.sh_pay - rec.y0;
+                    const int *tcl = (const int *)(st + SOFF_TCOL + h.sh_tcol) + (tpt[j] - rec.t0);
+                    y = slot_row<PK>(mt, vd, hd, pay, tcl, ke - kb, row, hl, src, xown, own);
+                }
+            }
+            S.py[tid] = y;
+            S.px[tid] = xown;
+            S.pown[tid] = own ? 1 : 0;
+            __syncthreads();
+            if (row_ok && part == 0) {
+                double yy = 0.0, xo = 0.0;
+                bool ow = false;
+                for (int q = 0; q < L; q++) {
+                    const int t = ((j * L + q) << 4) | hl;
+                    yy = __dadd_rn(yy, S.py[t]);
+                    if (!ow && S.pown[t]) {
+                        ow = true;
+                        xo = S.px[t];
+                    }
+                }
+                out(s, hl, yy, xo, ow);
+            }
         }
-        __syncthreads();
+        if (!__syncthreads_and(w)) {
+            // chunks c+1 .. c+NSTG-1 may still be landing
+            for (int jj = 1; jj < NSTG && c + jj < ce; jj++) {
+                const int kj = (c + jj - cb) % NSTG;
+                mbar_wait_bounded(&S.bar[kj], gc.use[kj] & 1u, a.status, a.budget_ns);
+                gc.use[kj]++;
+            }
+            __syncthreads();
+            return false;
+        }
         if (tid == 0 && c + NSTG < ce) issue_slot_chunk<PK>(a, S, c + NSTG, k);
     }
-    return ok;
+    return true;
 }
 
 // The SpMV of the layout the kernel was built for (LAY 0: staged tile

@@ -174,22 +174,31 @@ __global__ void k_slot_pack(MfTiles A, const int *__restrict__ sslot, const unsi
     }
 }
 
-// Greedy chunking of one CTA's strips (the same walk counts and fills).
-__device__ __forceinline__ int slot_walk(int s, int se, const int *sslot, const int *tile_ptr, bool &direct)
+// Greedy chunking of one CTA's strips (the same walk counts and fills): a
+// chunk grows while its strips fit the stage and 16 / lanes(max K) half-warp
+// groups.
+__device__ __forceinline__ int slot_walk(int s, int se, const int *sslot, const int *tile_ptr, bool &direct,
+                                         int &lanes)
 {
     const int s0 = s;
+    int kmax = 0;
     direct = false;
-    while (s < se && s - s0 < SC_STRIPS) {
+    while (s < se) {
+        const int K = sslot[s + 1] - sslot[s];
+        const int km = K > kmax ? K : kmax;
         const int nk = sslot[s + 1] - sslot[s0], nt = tile_ptr[s + 1] - tile_ptr[s0];
-        if (nk > SC_SLOTS || nt > SC_TILES) {
+        if (s - s0 + 1 > SC_STRIPS / slot_lanes(km) || nk > SC_SLOTS || nt > SC_TILES) {
             if (s == s0) {
                 direct = true;
+                kmax = km;
                 s++;
             }
             break;
         }
+        kmax = km;
         s++;
     }
+    lanes = direct ? 16 : slot_lanes(kmax);
     return s;
 }
 
@@ -204,8 +213,9 @@ __global__ void k_slot_chunk_count(int G, const int *__restrict__ part, const in
         int c = 0, s = part[g];
         const int se = part[g + 1];
         bool d;
+        int l;
         while (s < se) {
-            s = slot_walk(s, se, sslot, tile_ptr, d);
+            s = slot_walk(s, se, sslot, tile_ptr, d, l);
             c++;
         }
         cnt[g] = c;
@@ -221,7 +231,8 @@ __global__ void k_slot_chunk_fill(int G, const int *__restrict__ part, const int
         const int se = part[g + 1];
         while (s < se) {
             bool d;
-            const int s1 = slot_walk(s, se, sslot, tile_ptr, d);
+            int l;
+            const int s1 = slot_walk(s, se, sslot, tile_ptr, d, l);
             SlotChunk r;
             r.s0 = s;
             r.s1 = s1;
@@ -230,7 +241,7 @@ __global__ void k_slot_chunk_fill(int G, const int *__restrict__ part, const int
             r.t0 = tile_ptr[s];
             r.t1 = tile_ptr[s1];
             r.direct = d ? 1 : 0;
-            r.pad = 0;
+            r.lanes = l;
             r.y0 = r.y1 = 0;
             rec[c++] = r;
             s = s1;

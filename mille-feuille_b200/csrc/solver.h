@@ -25,16 +25,25 @@ struct ChunkRec {
 
 // A chunk of the row-slot layout: consecutive strips of one CTA whose slot
 // words, values (or mixed payload) and tile columns fit one shared-memory
-// stage.  A strip too large for a stage on its own is a one-strip chunk with
-// `direct` set (computed from global memory).
+// stage.  `lanes` half-warps share each strip (1, 2, 4, 8 or 16; a chunk has
+// 16 / lanes strips at most): each takes a contiguous part of the strip's
+// slots, and the parts' sums are added in order.  A strip too large for a
+// stage on its own is a one-strip chunk with `direct` set (16 half-warps,
+// read from global memory).
 constexpr int SC_STRIPS = 16, SC_SLOTS = 128, SC_TILES = 256;
 struct SlotChunk {
     int s0, s1;            // strips [s0, s1)
     int k0, k1;            // slots [k0, k1)
     int t0, t1;            // tiles [t0, t1)
-    int direct, pad;
+    int direct, lanes;
     long long y0, y1;      // mixed payload bytes [y0, y1)
 };
+
+// Half-warps per strip for a strip of K slots: about 8 slots each.
+__host__ __device__ __forceinline__ int slot_lanes(int K)
+{
+    return K <= 8 ? 1 : K <= 16 ? 2 : K <= 32 ? 4 : K <= 64 ? 8 : 16;
+}
 
 // Persistent solver state kept in device memory between launches.
 enum : int { S_RHO = 0, S_BETA, S_NB, S_RMAX, S_ITERS, S_REFS, S_EXIT, S_RELRES, S_ALPHA, S_OMEGA, S_COUNT };

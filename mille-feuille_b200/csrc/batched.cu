@@ -90,24 +90,69 @@ __device__ __forceinline__ double cluster_sum(cg::cluster_group &cl, double v, d
     return s;
 }
 
-// L lanes per row: lanes stride over the row's entries; the partials are
-// combined with a fixed xor tree, so every run gives the same bits.
+// L lanes per row: lanes stride over the row's entries (BU entries per lane
+// loaded before any is used); the partials are combined with a fixed xor
+// tree, so every run gives the same bits.  Two rows per lane group are in
+// flight at once (i1 < 0: none).
+constexpr int BU = 4;
+
 template <int L, bool MIX, class Src>
-__device__ __forceinline__ double row_dot(const int *__restrict__ rp, const int *__restrict__ col,
-                                          const double *__restrict__ val, const float *__restrict__ val32, int i,
-                                          int lane, Src src)
+__device__ __forceinline__ void row_dot2(const int *__restrict__ rp, const int *__restrict__ col,
+                                         const double *__restrict__ val, const float *__restrict__ val32, int i0, int i1,
+                                         int lane, Src src, double &y0, double &y1)
 {
-    const int a = (i >= 0) ? rp[i] : 0, e = (i >= 0) ? rp[i + 1] : 0;
-    double s = 0.0;
-    float sf = 0.0f;
-    for (int k = a + lane; k < e; k += L) {
-        if (MIX) sf = fmaf(__ldcs(val32 + k), (float)src(__ldcs(col + k)), sf);
-        else s = fma(__ldcs(val + k), (double)src(__ldcs(col + k)), s);
-    }
-    if (MIX) s = (double)sf;
+    using XT = decltype(src(0));
+    const int a0 = (i0 >= 0) ? rp[i0] : 0, e0 = (i0 >= 0) ? rp[i0 + 1] : 0;
+    const int a1 = (i1 >= 0) ? rp[i1] : 0, e1 = (i1 >= 0) ? rp[i1 + 1] : 0;
+    double s0 = 0.0, s1 = 0.0;
+    float f0 = 0.0f, f1 = 0.0f;
+    const int n0 = e0 - a0, n1 = e1 - a1, nmax = n0 > n1 ? n0 : n1;
+    for (int k = lane; k < nmax; k += L * BU) {
+        int c0[BU], c1[BU];
+        double v0[BU], v1[BU];
+        float w0[BU], w1[BU];
 #pragma unroll
-    for (int o = L / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, L);
-    return s;
+        for (int u = 0; u < BU; u++) {
+            const int kk = k + u * L;
+            const bool in0 = kk < n0, in1 = kk < n1;
+            c0[u] = in0 ? __ldcs(col + a0 + kk) : -1;
+            c1[u] = in1 ? __ldcs(col + a1 + kk) : -1;
+            if (MIX) {
+                w0[u] = in0 ? __ldcs(val32 + a0 + kk) : 0.0f;
+                w1[u] = in1 ? __ldcs(val32 + a1 + kk) : 0.0f;
+            } else {
+                v0[u] = in0 ? __ldcs(val + a0 + kk) : 0.0;
+                v1[u] = in1 ? __ldcs(val + a1 + kk) : 0.0;
+            }
+        }
+        XT x0[BU], x1[BU];
+#pragma unroll
+        for (int u = 0; u < BU; u++) {
+            x0[u] = c0[u] >= 0 ? src(c0[u]) : (XT)0;
+            x1[u] = c1[u] >= 0 ? src(c1[u]) : (XT)0;
+        }
+#pragma unroll
+        for (int u = 0; u < BU; u++) {
+            if (MIX) {
+                f0 = fmaf(w0[u], (float)x0[u], f0);
+                f1 = fmaf(w1[u], (float)x1[u], f1);
+            } else {
+                s0 = fma(v0[u], (double)x0[u], s0);
+                s1 = fma(v1[u], (double)x1[u], s1);
+            }
+        }
+    }
+    if (MIX) {
+        s0 = (double)f0;
+        s1 = (double)f1;
+    }
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o, L);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o, L);
+    }
+    y0 = s0;
+    y1 = s1;
 }
 
 template <int L, bool MIX>
@@ -174,14 +219,24 @@ __global__ void __launch_bounds__(BNT) k_batched_cg(BatchArgs a)
             };
             double loc = 0.0;
             // the trip count is the same for every lane (shuffles inside)
-            for (int base = ra; base < rb; base += GPB) {
-                const int i = base + grp < rb ? base + grp : -1;
-                const double y = row_dot<L, MIX>(rp, col, val, val32, i, lane, psrc);
-                if (lane == 0 && i >= 0) {
-                    const VT pn = psrc(i);
-                    pnew[i] = pn;
-                    q[i] = (VT)y;
-                    loc += (double)pn * (double)(VT)y;
+            for (int base = ra; base < rb; base += 2 * GPB) {
+                const int i0 = base + grp < rb ? base + grp : -1;
+                const int i1 = base + GPB + grp < rb ? base + GPB + grp : -1;
+                double y0, y1;
+                row_dot2<L, MIX>(rp, col, val, val32, i0, i1, lane, psrc, y0, y1);
+                if (lane == 0) {
+                    if (i0 >= 0) {
+                        const VT pn = psrc(i0);
+                        pnew[i0] = pn;
+                        q[i0] = (VT)y0;
+                        loc += (double)pn * (double)(VT)y0;
+                    }
+                    if (i1 >= 0) {
+                        const VT pn = psrc(i1);
+                        pnew[i1] = pn;
+                        q[i1] = (VT)y1;
+                        loc += (double)pn * (double)(VT)y1;
+                    }
                 }
             }
             const double pq = cluster_sum(cl, loc, &s_slot[2], s_warp);
@@ -215,13 +270,22 @@ __global__ void __launch_bounds__(BNT) k_batched_cg(BatchArgs a)
                 loc = 0.0;
                 const double *xh = x;
                 auto xsrc = [=](int c) -> double { return xh[c]; };
-                for (int base = ra; base < rb; base += GPB) {
-                    const int i = base + grp < rb ? base + grp : -1;
-                    const double y = row_dot<L, false>(rp, col, val, val32, i, lane, xsrc);
-                    if (lane == 0 && i >= 0) {
-                        const VT rv = (VT)(b[i] - y);
-                        r[i] = rv;
-                        loc += (double)rv * (double)rv;
+                for (int base = ra; base < rb; base += 2 * GPB) {
+                    const int i0 = base + grp < rb ? base + grp : -1;
+                    const int i1 = base + GPB + grp < rb ? base + GPB + grp : -1;
+                    double y0, y1;
+                    row_dot2<L, false>(rp, col, val, val32, i0, i1, lane, xsrc, y0, y1);
+                    if (lane == 0) {
+                        if (i0 >= 0) {
+                            const VT rv = (VT)(b[i0] - y0);
+                            r[i0] = rv;
+                            loc += (double)rv * (double)rv;
+                        }
+                        if (i1 >= 0) {
+                            const VT rv = (VT)(b[i1] - y1);
+                            r[i1] = rv;
+                            loc += (double)rv * (double)rv;
+                        }
                     }
                 }
                 rho_new = cluster_sum(cl, loc, &s_slot[1], s_warp);

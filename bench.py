@@ -289,10 +289,12 @@ def workload_single(args, mf, world, local):
     fn_dev = L.mf_bicgstab_solve if method == "bicgstab" else L.mf_cg_solve
     fn_host = L.mf_bicgstab_solve_host if method == "bicgstab" else L.mf_cg_solve_host
 
+    maxiter = 400000 if args.workload == "aniso" else 50000
+
     def opts_for(policy):
         if args.iters:
             return mf.solve_opts(tol=-1.0, maxiter=args.iters, policy=policy)
-        return mf.solve_opts(tol=tol, maxiter=50000, policy=policy)
+        return mf.solve_opts(tol=tol, maxiter=maxiter, policy=policy)
 
     def make_solve(policy, rep):
         o = opts_for(policy)

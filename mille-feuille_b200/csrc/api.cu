@@ -1,6 +1,7 @@
 // api.cu -- the C ABI (include/mf.h): handles, status codes, host/device
 // entry points.  No call aborts; every CUDA error becomes an mf_status.
 #include <atomic>
+#include <mutex>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
@@ -14,6 +15,37 @@ static thread_local char g_err[1024] = "";
 static std::atomic<long long> g_launches{0};
 
 void note_launch(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+cudaError_t pool_malloc_async(void **p, size_t bytes, cudaStream_t s)
+{
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaMallocAsync(p, bytes, s);
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!pools[dev]) {
+            cudaMemPoolProps props;
+            memset(&props, 0, sizeof(props));
+            props.allocType = cudaMemAllocationTypePinned;
+            props.handleTypes = cudaMemHandleTypeNone;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            e = cudaMemPoolCreate(&pools[dev], &props);
+            if (e != cudaSuccess) {
+                pools[dev] = nullptr;
+                return e;
+            }
+            uint64_t keep = 256ull << 20;  // up to 256 MiB stays in the pool across synchronisations
+            cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        pool = pools[dev];
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
 
 void set_last_error(const char *fmt, ...)
 {

@@ -17,6 +17,17 @@ namespace mf {
 void set_last_error(const char *fmt, ...);
 // Counts kernel launches issued by the library (mf_kernel_launches()).
 void note_launch(int k = 1);
+// Stream-ordered temporary allocation from the library's own memory pool of
+// the current device (created on first use; it keeps up to 256 MiB of freed
+// memory across synchronisations instead of returning it each time, so the
+// temporaries of a solve's checkpoints cost no driver allocation).  Free
+// with cudaFreeAsync.
+cudaError_t pool_malloc_async(void **p, size_t bytes, cudaStream_t s);
+template <typename T>
+inline cudaError_t pool_malloc_async(T **p, size_t bytes, cudaStream_t s)
+{
+    return pool_malloc_async((void **)p, bytes, s);
+}
 
 #define MF_CUDA(expr)                                                                     \
     do {                                                                                  \

@@ -87,7 +87,7 @@ mf_status pack_payload(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s)
     const int T = m->v.tilenum;
     if (!m->d_poff) MF_CUDA(cudaMalloc(&m->d_poff, sizeof(unsigned) * (T + 1) + 16));
     int *sizes = nullptr;
-    MF_CUDA(cudaMallocAsync(&sizes, sizeof(int) * (T + 1), s));
+    MF_CUDA(pool_malloc_async(&sizes, sizeof(int) * (T + 1), s));
     k_pack_sizes<<<grid_for(T + 1, 256), 256, 0, s>>>(T, m->d_tile_nnz, d_wcls, sizes);
     note_launch();
     MF_CUDA(cudaGetLastError());
@@ -192,7 +192,7 @@ mf_status rule_working_classes(mf_matrix m, const void *p_new, const void *p_old
     const int T = m->v.tilenum, n = m->v.cols;
     const int nseg = m->v.tilen;
     float *seg = nullptr;
-    MF_CUDA(cudaMallocAsync(&seg, sizeof(float) * nseg + sizeof(unsigned) * 4, s));
+    MF_CUDA(pool_malloc_async(&seg, sizeof(float) * nseg + sizeof(unsigned) * 4, s));
     unsigned *pmax = (unsigned *)(seg + nseg);
     MF_CUDA(cudaMemsetAsync(pmax, 0, sizeof(unsigned), s));
     k_seg_change<float><<<grid_for2((long long)nseg * 16, 256), 256, 0, s>>>(nseg, n, (const float *)p_new,

@@ -13,10 +13,9 @@
 //  10 log10(max|a| max_j|p| / max|q|)/10
 //  11..14 features 6, 7, 8, 9 at the previous checkpoint (history)
 //  15 1 (bias input)
-// Labels (from FP64 solver traces): the lowest class whose rounding error
-// bound for the tile's contribution stays under 2^-22 max|q|:
-//   0 int8 (exact integer tile) or bypass (contribution below the bound),
-//   1 fp16, 2 fp32, 3 fp64.
+// Labels (from FP64 solver traces): the narrowest class whose rounding costs
+// no more than the FP32 rounding of the rows the tile feeds (k_collect):
+//   0 int8 (exact integer tile) or bypass, 1 fp16, 2 fp32 (3 fp64: unused).
 // Training: softmax cross-entropy, per-sample backward in shared memory,
 // per-parameter sums over the samples in a fixed order (deterministic), Adam
 // on FP32 master weights, BF16 copies for the forward pass.
@@ -135,35 +134,58 @@ __device__ __forceinline__ void tile_features(const FeatIn &f, int t, float *x)
     x[15] = 1.f;
 }
 
-// label: lowest class whose error bound for the tile stays under 2^-22 max|q|
+// |A| |p| per row (the magnitude the row's FP32 sum is rounded against).
+__global__ void k_row_absmag(MfTiles A, const double *__restrict__ p, double *__restrict__ mag)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.rows; i += gridDim.x * blockDim.x) {
+        const int bi = i / MF_TILE, r = i % MF_TILE;
+        const int rowlen = (bi == A.tilem - 1) ? A.rows - bi * MF_TILE : MF_TILE;
+        double m = 0.0;
+        for (int t = A.tile_ptr[bi]; t < A.tile_ptr[bi + 1]; t++) {
+            const int off = A.tile_nnz[t], nz = A.tile_nnz[t + 1] - off;
+            const int po = A.csrptr_offset[t];
+            const int lo = A.ptr[po + r], hi = (r == rowlen - 1) ? nz : (int)A.ptr[po + r + 1];
+            const int xo = A.tile_columnidx[t] * MF_TILE;
+            for (int k = lo; k < hi; k++) m += fabs(A.val[off + k]) * fabs(p[xo + A.col[off + k]]);
+        }
+        mag[i] = m;
+    }
+}
+
+// Label of a tile: the narrowest class whose rounding costs no more than the
+// FP32 rounding of the rows it feeds.  With e_r = sum |a||p| over the tile's
+// entries of row r and M_r the same sum over the whole row, storing the tile
+// in fp16 adds about 2^-11 e_r and skipping it adds e_r, against the FP32
+// sum's 2^-24 M_r:  0 (int8-exact tile, or every e_r <= 2^-24 M_r: bypass),
+// 1 (fp16-exact tile, or every e_r <= 2^-13 M_r), 2 (fp32).  Class 3 (fp64)
+// is never needed by the inner FP32 solver.
 template <typename VT>
 __global__ void k_collect(FeatIn f, const double *__restrict__ val, const unsigned char *__restrict__ col,
                           const unsigned char *__restrict__ ptr, int last_tile_begin, int last_rowlen,
-                          const VT *__restrict__ pn, int stride, unsigned salt, float *__restrict__ X,
-                          unsigned char *__restrict__ Y, unsigned long long *__restrict__ count, long long cap)
+                          const VT *__restrict__ pn, const double *__restrict__ mag, int stride, unsigned salt,
+                          float *__restrict__ X, unsigned char *__restrict__ Y, unsigned long long *__restrict__ count,
+                          long long cap)
 {
-    const float qmax = __uint_as_float(f.gmax[2]);
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < f.T; t += gridDim.x * blockDim.x) {
         const unsigned h = (unsigned)t * 2654435761u ^ salt;
         if ((h >> 8) % (unsigned)stride != 0u) continue;
-        // largest row contribution sum |a||p| of the tile
         const int o0 = f.tile_nnz[t], nz = f.tile_nnz[t + 1] - o0;
         const long long po = (t < last_tile_begin) ? 16ll * t : 16ll * last_tile_begin + (long long)(t - last_tile_begin) * last_rowlen;
         const int rowlen = (t < last_tile_begin) ? MF_TILE : last_rowlen;
         const int xo = f.tile_col[t] * MF_TILE;
-        double emax = 0.0;
+        const int row0 = f.tile_row[t] * MF_TILE;
+        double ratio = 0.0;  // max_r e_r / M_r
         for (int r = 0; r < rowlen; r++) {
             const int lo = ptr[po + r], hi = (r == rowlen - 1) ? nz : (int)ptr[po + r + 1];
             double e = 0.0;
             for (int k = lo; k < hi; k++) e += fabs(val[o0 + k]) * fabs((double)pn[xo + col[o0 + k]]);
-            emax = fmax(emax, e);
+            const double M = mag[row0 + r];
+            if (e > 0.0) ratio = fmax(ratio, M > 0.0 ? e / M : 1.0);
         }
-        const double bound = ldexp((double)qmax, -22);
         int lab;
-        if (f.cls[t] == MF_CLASS_INT8 || emax <= bound) lab = 0;
-        else if (ldexp(emax, -11) <= bound) lab = 1;
-        else if (ldexp(emax, -24) <= bound) lab = 2;
-        else lab = 3;
+        if (f.cls[t] == MF_CLASS_INT8 || ratio <= 0x1.0p-24) lab = 0;
+        else if (f.cls[t] == MF_CLASS_FP16 || ratio <= 0x1.0p-13) lab = 1;
+        else lab = 2;
         const unsigned long long slot = atomicAdd(count, 1ull);
         if ((long long)slot >= cap) continue;
         float x[NF];
@@ -217,9 +239,24 @@ __global__ void k_mlp_classify(FeatIn f, const __nv_bfloat16 *__restrict__ wq, u
         float x[NF], h1[H1], h2[H2], o[NO];
         tile_features(f, t, x);
         mlp_forward(s_w, x, h1, h2, o);
-        int best = 0;
-        for (int k = 1; k < NO; k++)
-            if (o[k] > o[best]) best = k;
+        // conservative decision: the narrowest class c the network is 99 %
+        // sure the tile tolerates, P(label <= c) >= 0.99
+        float mx = o[0];
+        for (int k = 1; k < NO; k++) mx = fmaxf(mx, o[k]);
+        float pr[NO], z = 0.f;
+        for (int k = 0; k < NO; k++) {
+            pr[k] = __expf(o[k] - mx);
+            z += pr[k];
+        }
+        int best = NO - 1;
+        float cum = 0.f;
+        for (int k = 0; k < NO; k++) {
+            cum += pr[k];
+            if (cum >= 0.99f * z) {
+                best = k;
+                break;
+            }
+        }
         const int c = f.cls[t];
         int w;
         if (best == 0) w = (c == MF_CLASS_INT8) ? MF_CLASS_INT8 : MF_CLASS_BYPASS;
@@ -468,13 +505,20 @@ static mf_status collect_hook(void *ctx, mf_matrix m, SolverWork &w, const void 
     MF_TRY(checkpoint_stats<double>(m, pw, p_new, p_old, w.r, w.q, s));
     const FeatIn f = feat_in(m, pw, (float)relres);
     unsigned long long *d_cnt = nullptr;
-    MF_CUDA(cudaMallocAsync(&d_cnt, sizeof(unsigned long long), s));
+    MF_CUDA(pool_malloc_async(&d_cnt, sizeof(unsigned long long) + sizeof(double) * ((size_t)m->v.rows + 1), s));
+    double *d_mag = (double *)(d_cnt + 1);
+    if (m->v.rows > 0) {
+        k_row_absmag<<<grid_for4(m->v.rows, 256), 256, 0, s>>>(m->v, (const double *)p_new, d_mag);
+        note_launch();
+        MF_CUDA(cudaGetLastError());
+    }
     const unsigned long long start = (unsigned long long)p->n;
     MF_CUDA(cudaMemcpyAsync(d_cnt, &start, sizeof(start), cudaMemcpyHostToDevice, s));
     if (f.T > 0) {
         k_collect<double><<<grid_for4(f.T, 256), 256, 0, s>>>(
             f, m->d_val, m->d_col, m->d_ptr, m->last_tile_begin, m->v.rows - (m->v.tilem - 1) * MF_TILE,
-            (const double *)p_new, c->stride, c->salt ^ (unsigned)it * 0x9E3779B9u, p->d_x, p->d_y, d_cnt, p->cap);
+            (const double *)p_new, d_mag, c->stride, c->salt ^ (unsigned)it * 0x9E3779B9u, p->d_x, p->d_y, d_cnt,
+            p->cap);
         note_launch();
         MF_CUDA(cudaGetLastError());
     }

@@ -83,7 +83,7 @@ mf_status scan_rec(const int *in, int *out, int n, cudaStream_t s, int *d_total)
         return MF_OK;
     }
     int *tot = nullptr;
-    MF_CUDA(cudaMallocAsync(&tot, sizeof(int) * (blocks + 1), s));
+    MF_CUDA(pool_malloc_async(&tot, sizeof(int) * (blocks + 1), s));
     k_block_totals<<<blocks, SCAN_NT, 0, s>>>(in, n, tot);
     note_launch();
     mf_status st = MF_OK;
@@ -107,7 +107,7 @@ mf_status exclusive_scan_i32(const int *in, int *out, int n, cudaStream_t s, int
         return MF_OK;
     }
     int *d_total = nullptr;
-    if (total_host) MF_CUDA(cudaMallocAsync(&d_total, sizeof(int), s));
+    if (total_host) MF_CUDA(pool_malloc_async(&d_total, sizeof(int), s));
     mf_status st = scan_rec(in, out, n, s, d_total);
     if (total_host) {
         if (st == MF_OK) {

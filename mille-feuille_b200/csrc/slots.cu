@@ -270,7 +270,7 @@ mf_status build_slot_chunks(mf_matrix m, int G, cudaStream_t s)
     m->schunk_ctas = 0;
     MF_CUDA(cudaMalloc(&m->d_scta_chunk, sizeof(int) * (G + 1)));
     int *cnt = nullptr;
-    MF_CUDA(cudaMallocAsync(&cnt, sizeof(int) * (G + 1), s));
+    MF_CUDA(pool_malloc_async(&cnt, sizeof(int) * (G + 1), s));
     k_slot_chunk_count<<<grid_for3(G + 1, 128), 128, 0, s>>>(G, m->d_part, m->d_sslot, m->d_tile_ptr, cnt);
     note_launch();
     MF_CUDA(cudaGetLastError());
@@ -299,7 +299,7 @@ mf_status build_slots(mf_matrix m, cudaStream_t s)
     const int tilem = A.tilem;
     int *d_K = nullptr, *d_flag = nullptr;
     MF_CUDA(cudaMalloc(&m->d_sslot, sizeof(int) * (tilem + 1) + 32));  // slack: 16-byte bulk-copy rounding
-    MF_CUDA(cudaMallocAsync(&d_K, sizeof(int) * (tilem + 1) + sizeof(int), s));
+    MF_CUDA(pool_malloc_async(&d_K, sizeof(int) * (tilem + 1) + sizeof(int), s));
     d_flag = d_K + tilem + 1;
     MF_CUDA(cudaMemsetAsync(d_flag, 0, sizeof(int), s));
     k_slot_count<<<grid_for3((long long)(tilem + 1) * 16, 256), 256, 0, s>>>(A, d_K, d_flag);
@@ -338,7 +338,7 @@ mf_status pack_slots(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s)
     }
     unsigned char *srank = (unsigned char *)(m->d_shdr + ns + 1);
     int *sizes = nullptr;
-    MF_CUDA(cudaMallocAsync(&sizes, sizeof(int) * ((size_t)ns + 1) * 2, s));
+    MF_CUDA(pool_malloc_async(&sizes, sizeof(int) * ((size_t)ns + 1) * 2, s));
     int *soff = sizes + ns + 1;
     k_slot_sizes<<<grid_for3((long long)A.tilem * 16, 256), 256, 0, s>>>(A, m->d_sslot, m->d_smeta, d_wcls, ns, srank,
                                                                         sizes);

@@ -406,7 +406,7 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
 
     size_t acc = 0;
     int *d_err = nullptr;
-    MF_CUDA(cudaMallocAsync(&d_err, sizeof(int) * 8, s));
+    MF_CUDA(pool_malloc_async(&d_err, sizeof(int) * 8, s));
     MF_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int) * 8, s));
     int *d_class_count = d_err + 1;  // [5]
     int *d_maxnz = d_err + 6;
@@ -427,10 +427,10 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
     // pass 1: per tile-row sort
     int *d_perm = nullptr, *d_cnt = nullptr;
     unsigned long long *d_big = nullptr;
-    MF_CUDA(cudaMallocAsync(&d_perm, sizeof(int) * (size_t)(nnz + rp0 + 1), s));
-    MF_CUDA(cudaMallocAsync(&d_cnt, sizeof(int) * (size_t)(tilem + 1), s));
+    MF_CUDA(pool_malloc_async(&d_perm, sizeof(int) * (size_t)(nnz + rp0 + 1), s));
+    MF_CUDA(pool_malloc_async(&d_cnt, sizeof(int) * (size_t)(tilem + 1), s));
     // global sort space only when some tile-row exceeds the shared-memory cap
-    MF_CUDA(cudaMallocAsync(&d_big, sizeof(unsigned long long) * (size_t)(nnz + rp0 + 1), s));
+    MF_CUDA(pool_malloc_async(&d_big, sizeof(unsigned long long) * (size_t)(nnz + rp0 + 1), s));
     MF_TRY(dalloc(&m->d_tile_ptr, tilem + 1, &acc));
     if (tilem > 0) {
         k_sort_tilerows<<<grid_for(tilem, 1) , BUILD_NT, 0, s>>>(tilem, rowA, d_rowptr, d_colidx, d_perm, d_big, d_cnt);
@@ -452,7 +452,7 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
     MF_TRY(dalloc(&m->d_cidx, (nnz + 1) / 2, &acc));
     MF_CUDA(cudaMemsetAsync(m->d_cidx, 0, (size_t)(nnz + 1) / 2 + 1, s));
     int *d_run = nullptr;
-    MF_CUDA(cudaMallocAsync(&d_run, sizeof(int) * (size_t)T * MF_TILE + 16, s));
+    MF_CUDA(pool_malloc_async(&d_run, sizeof(int) * (size_t)T * MF_TILE + 16, s));
     MF_CUDA(cudaMemsetAsync(d_run, 0xff, sizeof(int) * (size_t)T * MF_TILE + 16, s));
     if (tilem > 0) {
         k_fill_tilerows<<<grid_for(tilem, 1), BUILD_NT, 0, s>>>(tilem, rowA, rp0, d_rowptr, d_colidx, d_val, d_val_low,
@@ -519,7 +519,7 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
     int rbb = 0;
     {
         int *d_rc = nullptr;
-        MF_CUDA(cudaMallocAsync(&d_rc, sizeof(int) * (tilem + 1), s));
+        MF_CUDA(pool_malloc_async(&d_rc, sizeof(int) * (tilem + 1), s));
         k_rbb_count<<<grid_for(tilem + 1, 256), 256, 0, s>>>(tilem, m->d_tile_ptr, d_rc, m->d_block_signal);
         note_launch();
         MF_CUDA(cudaGetLastError());
@@ -589,7 +589,7 @@ mf_status strip_partition(mf_matrix m, int ctas, cudaStream_t s)
     const int tilem = m->v.tilem;
     MF_CUDA(cudaMalloc(&m->d_part, sizeof(int) * (ctas + 1)));
     int *d_cost = nullptr;
-    MF_CUDA(cudaMallocAsync(&d_cost, sizeof(int) * (tilem + 1), s));
+    MF_CUDA(pool_malloc_async(&d_cost, sizeof(int) * (tilem + 1), s));
     k_strip_cost<<<grid_for(tilem + 1, 256), 256, 0, s>>>(tilem, m->d_tile_ptr, m->d_tile_nnz, d_cost);
     note_launch();
     MF_CUDA(cudaGetLastError());

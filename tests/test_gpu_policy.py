@@ -61,20 +61,22 @@ def test_learned_requires_attached_policy(mf):
 
 @pytest.fixture(scope="module")
 def trained(mf, torch):
-    """A policy trained on traces of FP64 solves of small anisotropic
-    problems (16^3, seeds 1000..1003)."""
+    """A policy trained on traces of FP64 solves of random SPD systems whose
+    rows mix magnitudes over 8 decades (2000 rows, seeds 1000..1007): the
+    tiles of small entries are the ones an accuracy-preserving label may
+    demote."""
     P = mf.Policy(seed=1)
     total = 0
-    for seed in range(1000, 1004):
-        A = mf.synth_aniso3d(16, seed)
+    for seed in range(1000, 1008):
+        A = mf.synth_random_spd(seed, 2000)
         xs = mf.synth_xstar(seed, A.n_rows)
         b = torch.tensor(A.matvec(xs), dtype=torch.float64, device="cuda")
         M = mf.Matrix(A)
-        total = P.collect(M, b.data_ptr(), checkpoint_every=5, sample_stride=1, max_samples=1 << 20)
+        total = P.collect(M, b.data_ptr(), checkpoint_every=20, sample_stride=2, max_samples=1 << 22)
         torch.cuda.synchronize()
         M.close()
     counts = P.label_counts()
-    l0, l1 = P.train(epochs=20, batch=512, lr=3e-3, seed=7)
+    l0, l1 = P.train(epochs=20, batch=1024, lr=3e-3, seed=7)
     return P, total, counts, l0, l1
 
 
@@ -85,20 +87,25 @@ def test_policy_collect_and_train(trained):
     assert l1 < l0, (l0, l1)
 
 
-def test_learned_solve_reaches_fp64_tolerance(mf, trained):
-    """An unseen instance (seed 2000, 24^3): the LEARNED policy reaches the
-    1e-10 true relative residual, and moves fewer bytes than plain FP64."""
+def test_learned_policy_gain_over_static(mf, trained):
+    """An unseen system (seed 2000, 4000 rows): the LEARNED policy reaches the
+    1e-10 FP64 true relative residual like the STATIC value-range policy
+    (the method without the network) and moves fewer bytes: the network
+    demotes tiles whose contribution is below the rows' FP32 rounding."""
     P = trained[0]
-    A = mf.synth_aniso3d(24, 2000)
+    A = mf.synth_random_spd(2000, 4000)
     xs = mf.synth_xstar(2000, A.n_rows)
     b = A.matvec(xs)
     M = mf.Matrix(A)
     M.attach_policy(P)
-    x, rep = M.solve_host(b, tol=1e-10, maxiter=20000, policy="learned")
+    x, rep = M.solve_host(b, tol=1e-10, maxiter=50000, policy="learned")
     assert rep.status == 0, rep.as_dict()
     assert rep.relres_true <= 1e-10 * (1 + 1e-6)
     assert ol.oracle_true_relres(ol.Csr(A.n_rows, A.n_cols, A.rowptr, A.colidx, A.val), b, x) <= 2e-10
-    x64, rep64 = M.solve_host(b, tol=1e-10, maxiter=20000, policy="fp64")
-    assert rep64.status == 0
-    assert rep.bytes_moved < rep64.bytes_moved
+    xs_, reps = M.solve_host(b, tol=1e-10, maxiter=50000, policy="static")
+    x64, rep64 = M.solve_host(b, tol=1e-10, maxiter=50000, policy="fp64")
+    assert reps.status == 0 and rep64.status == 0
+    per_it = lambda r: r.bytes_moved / max(1, r.iterations)
+    assert per_it(rep) < per_it(reps) < per_it(rep64), (per_it(rep), per_it(reps), per_it(rep64))
+    assert rep.bytes_moved < reps.bytes_moved, (rep.as_dict(), reps.as_dict())
     M.close()

@@ -96,14 +96,28 @@ __device__ __forceinline__ double cluster_sum(cg::cluster_group &cl, double v, d
 // flight at once (i1 < 0: none).
 constexpr int BU = 4;
 
+// Row bounds of the two rows of a step (0, 0 for a missing row).
+struct RowPair {
+    int a0, e0, a1, e1;
+};
+
+__device__ __forceinline__ RowPair row_pair(const int *__restrict__ rp, int i0, int i1)
+{
+    RowPair p;
+    p.a0 = (i0 >= 0) ? rp[i0] : 0;
+    p.e0 = (i0 >= 0) ? rp[i0 + 1] : 0;
+    p.a1 = (i1 >= 0) ? rp[i1] : 0;
+    p.e1 = (i1 >= 0) ? rp[i1 + 1] : 0;
+    return p;
+}
+
 template <int L, bool MIX, class Src>
-__device__ __forceinline__ void row_dot2(const int *__restrict__ rp, const int *__restrict__ col,
-                                         const double *__restrict__ val, const float *__restrict__ val32, int i0, int i1,
-                                         int lane, Src src, double &y0, double &y1)
+__device__ __forceinline__ void row_dot2(const RowPair &rb, const int *__restrict__ col,
+                                         const double *__restrict__ val, const float *__restrict__ val32, int lane,
+                                         Src src, double &y0, double &y1)
 {
     using XT = decltype(src(0));
-    const int a0 = (i0 >= 0) ? rp[i0] : 0, e0 = (i0 >= 0) ? rp[i0 + 1] : 0;
-    const int a1 = (i1 >= 0) ? rp[i1] : 0, e1 = (i1 >= 0) ? rp[i1 + 1] : 0;
+    const int a0 = rb.a0, e0 = rb.e0, a1 = rb.a1, e1 = rb.e1;
     double s0 = 0.0, s1 = 0.0;
     float f0 = 0.0f, f1 = 0.0f;
     const int n0 = e0 - a0, n1 = e1 - a1, nmax = n0 > n1 ? n0 : n1;
@@ -219,11 +233,16 @@ __global__ void __launch_bounds__(BNT) k_batched_cg(BatchArgs a)
             };
             double loc = 0.0;
             // the trip count is the same for every lane (shuffles inside)
+            // row bounds of the next step are loaded while this step computes
+            RowPair nxt = row_pair(rp, ra + grp < rb ? ra + grp : -1, ra + GPB + grp < rb ? ra + GPB + grp : -1);
             for (int base = ra; base < rb; base += 2 * GPB) {
                 const int i0 = base + grp < rb ? base + grp : -1;
                 const int i1 = base + GPB + grp < rb ? base + GPB + grp : -1;
+                const RowPair cur = nxt;
+                const int n0 = base + 2 * GPB + grp, n1 = base + 3 * GPB + grp;
+                nxt = row_pair(rp, n0 < rb ? n0 : -1, n1 < rb ? n1 : -1);
                 double y0, y1;
-                row_dot2<L, MIX>(rp, col, val, val32, i0, i1, lane, psrc, y0, y1);
+                row_dot2<L, MIX>(cur, col, val, val32, lane, psrc, y0, y1);
                 if (lane == 0) {
                     if (i0 >= 0) {
                         const VT pn = psrc(i0);
@@ -274,7 +293,7 @@ __global__ void __launch_bounds__(BNT) k_batched_cg(BatchArgs a)
                     const int i0 = base + grp < rb ? base + grp : -1;
                     const int i1 = base + GPB + grp < rb ? base + GPB + grp : -1;
                     double y0, y1;
-                    row_dot2<L, false>(rp, col, val, val32, i0, i1, lane, xsrc, y0, y1);
+                    row_dot2<L, false>(row_pair(rp, i0, i1), col, val, val32, lane, xsrc, y0, y1);
                     if (lane == 0) {
                         if (i0 >= 0) {
                             const VT rv = (VT)(b[i0] - y0);
@@ -315,6 +334,8 @@ int batched_ctas(int count, int cluster)
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // clusters of 16 CTAs are above the portable size: allowed explicitly
+    if (cluster > 8) cudaFuncSetAttribute(k_batched_cg<L, MIX>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batched_cg<L, MIX>, BNT, 0);
     int ctas = sms * (per > 0 ? per : 1);
     ctas = (ctas / cluster) * cluster;
@@ -584,11 +605,11 @@ mf_status mf_batch_cg_solve(mf_batch bt, const double *b, double *x, const mf_so
     }
     cudaStream_t s = (cudaStream_t)stream;
     int lanes = bt->tuned_lanes ? bt->tuned_lanes : 8;
-    int cluster = bt->tuned_cluster ? bt->tuned_cluster : 4;
+    int cluster = bt->tuned_cluster ? bt->tuned_cluster : 8;
     if (const char *e = getenv("MF_BATCH_LANES")) lanes = atoi(e);
     if (const char *e = getenv("MF_BATCH_CLUSTER")) cluster = atoi(e);
     if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) lanes = 8;
-    if (cluster < 1 || cluster > 8) cluster = 4;
+    if (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16) cluster = 8;
     const bool mixed = o.policy != MF_POLICY_FP64;
     MF_TRY(batch_work(bt, mixed));
     const int ctas = mixed ? batched_ctas_l<true>(lanes, bt->count, cluster) : batched_ctas_l<false>(lanes, bt->count, cluster);
@@ -687,7 +708,7 @@ mf_status mf_batch_tune(mf_batch bt, const double *b, double *x, const mf_solve_
     mf_solve_opts_default(&o);
     if (opts) o = *opts;
     const int lanes_c[] = {4, 8, 16, 32};
-    const int clus_c[] = {1, 2, 4, 8};
+    const int clus_c[] = {1, 2, 4, 8, 16};
     float best = 1e30f;
     int bl = 8, bc = 4;
     cudaStream_t s = (cudaStream_t)stream;
@@ -722,7 +743,8 @@ mf_status mf_batch_tune(mf_batch bt, const double *b, double *x, const mf_solve_
 
 mf_status mf_batch_set_schedule(mf_batch bt, int lanes, int cluster)
 {
-    if (!bt || (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) || cluster < 1 || cluster > 8)
+    if (!bt || (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) ||
+        (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16))
         return MF_ERR_INVALID_ARG;
     bt->tuned_lanes = lanes;
     bt->tuned_cluster = cluster;

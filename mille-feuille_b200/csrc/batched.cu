@@ -643,6 +643,7 @@ mf_status mf_batch_cg_solve(mf_batch bt, const double *b, double *x, const mf_so
             memcpy(bt->graph_key, key, sizeof(key));
         }
         MF_CUDA(cudaGraphLaunch(bt->graph, s));
+        note_launch(2);  // the graph's kernels: the batched CG and the residual check
     } else {
         MF_TRY(batch_enqueue(bt, b, x, o, lanes, cluster, ctas, s));
     }

@@ -279,7 +279,7 @@ mf_status mf_batch_cg_solve(mf_batch bt, const double *b, double *x, const mf_so
 mf_status mf_batch_results(mf_batch bt, int *iterations, double *relres_true);
 /* Autotuner: times each schedule (lanes per row 4/8/16/32 x cluster size
  * 1/2/4/8/16) on this batch, keeps the fastest on the handle.  Default
- * schedule: 8 lanes, clusters of 8 CTAs.  Clusters of 16 CTAs exceed the
+ * schedule: 8 lanes, clusters of 4 CTAs.  Clusters of 16 CTAs exceed the
  * portable cluster size and are enabled explicitly on the kernel. */
 mf_status mf_batch_tune(mf_batch bt, const double *b, double *x, const mf_solve_opts *opts, int *lanes_out,
                         int *cluster_out, void *stream);

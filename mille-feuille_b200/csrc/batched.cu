@@ -23,6 +23,7 @@
 #include <type_traits>
 
 #include "mf_internal.h"
+#include "tma.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -44,6 +45,10 @@ struct mf_batch_s {
     void *work = nullptr;
     size_t work_bytes = 0;
     int *d_queue = nullptr;
+    // row chunks of every system (staged through shared memory by the SpMV)
+    int *d_sc = nullptr;          // [count+1] first chunk of each system
+    int *d_crow = nullptr;        // per system nch+1 chunk row starts (relative rows), at sc[s] + s
+    int *d_cent = nullptr;        // the entries offsets rowptr[crow] of the same chunks
     // CUDA graph of the last solve configuration
     cudaGraphExec_t graph = nullptr;
     const void *graph_b = nullptr;
@@ -68,12 +73,14 @@ struct BatchArgs {
     const double *b;
     double *x;
     void *r, *p0, *p1, *q, *xlo;  // workspace vectors (rows_total each)
+    const int *sc, *crow, *cent;   // row chunks
     int *queue;
     int *iters, *refs, *status;
     double *relres;
     int maxiter;
     double tol;
     double delta;
+    unsigned long long budget_ns;  // bound of every shared-memory stage wait
 };
 
 // Deterministic cluster-wide sum: each CTA reduces its threads in a fixed
@@ -90,11 +97,94 @@ __device__ __forceinline__ double cluster_sum(cg::cluster_group &cl, double v, d
     return s;
 }
 
+// Row chunks staged through shared memory: up to BCR rows and BCE entries
+// per chunk (a longer row is a chunk of its own, read from global memory).
+constexpr int BCE = 2048, BCR = 256;
+constexpr int BOFF_RP = 0;                          // rowptr[r0 .. r1]
+constexpr int BOFF_COL = 1072;                      // columns of the chunk's entries
+constexpr int BOFF_VAL = BOFF_COL + BCE * 4 + 32;   // values (FP64, or FP32 when mixed)
+constexpr int BSTAGE = BOFF_VAL + BCE * 8 + 32;
+static_assert(BOFF_COL % 16 == 0 && BOFF_VAL % 16 == 0 && BSTAGE % 16 == 0, "stage regions 16-byte aligned");
+static_assert((BCR + 1) * 4 + 32 <= BOFF_COL, "row pointers fit");
+
+struct BHdr {
+    int r0, r1, e0, direct;   // rows [r0, r1), first entry e0 (relative to the system)
+    int sh_rp, sh_col, sh_val, pad;
+};
+
+#ifndef MF_BATCH_STAGES
+#define MF_BATCH_STAGES 2
+#endif
+constexpr int BNS = MF_BATCH_STAGES;  // chunks in flight per CTA
+
+struct BSmem {
+    unsigned char stage[BNS][BSTAGE];
+    BHdr hdr[BNS];
+    uint64_t bar[BNS];
+};
+
+__device__ __forceinline__ void b_add_range(unsigned char *dst, const unsigned char *src, long long a0, long long a1,
+                                            uint64_t *bar, int &shift)
+{
+    const long long c0 = a0 & ~15ll, c1 = (a1 + 15) & ~15ll;
+    shift = (int)(a0 - c0);
+    if (c1 > c0) bulk_g2s_hint(dst, src + c0, (unsigned)(c1 - c0), bar, l2_policy_evict_first());
+}
+
+__device__ __forceinline__ unsigned b_range_bytes(long long a0, long long a1)
+{
+    return (unsigned)(((a1 + 15) & ~15ll) - (a0 & ~15ll));
+}
+
+// A chunk's rows [r0, r1) and entries [e0, e1) (relative to its system).
+struct BChunk {
+    int r0, r1, e0, e1;
+};
+
+__device__ __forceinline__ BChunk b_chunk(const BatchArgs &a, int sys, int c)
+{
+    BChunk ch;
+    ch.r0 = a.crow[c + sys];
+    ch.r1 = a.crow[c + 1 + sys];
+    ch.e0 = a.cent[c + sys];
+    ch.e1 = a.cent[c + 1 + sys];
+    return ch;
+}
+
+// Thread 0: stage chunk `ch` of system `sys` into stage k.
+template <bool MIX>
+__device__ void b_issue(const BatchArgs &a, BSmem &S, long long rp_base, long long z0, const BChunk &ch, int k)
+{
+    BHdr &h = S.hdr[k];
+    const int r0 = ch.r0, r1 = ch.r1, e0 = ch.e0, e1 = ch.e1;
+    h.r0 = r0;
+    h.r1 = r1;
+    h.e0 = e0;
+    h.direct = (e1 - e0 > BCE) ? 1 : 0;
+    const int vb = MIX ? 4 : 8;
+    unsigned total = b_range_bytes(4 * (rp_base + r0), 4 * (rp_base + r1 + 1));
+    if (!h.direct) total += b_range_bytes(4 * (z0 + e0), 4 * (z0 + e1)) + b_range_bytes(vb * (z0 + e0), vb * (z0 + e1));
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&S.bar[k], total);
+    unsigned char *st = S.stage[k];
+    b_add_range(st + BOFF_RP, (const unsigned char *)a.rowptr, 4 * (rp_base + r0), 4 * (rp_base + r1 + 1), &S.bar[k],
+                h.sh_rp);
+    if (h.direct) return;
+    b_add_range(st + BOFF_COL, (const unsigned char *)a.col, 4 * (z0 + e0), 4 * (z0 + e1), &S.bar[k], h.sh_col);
+    if (MIX)
+        b_add_range(st + BOFF_VAL, (const unsigned char *)a.val32, 4 * (z0 + e0), 4 * (z0 + e1), &S.bar[k], h.sh_val);
+    else
+        b_add_range(st + BOFF_VAL, (const unsigned char *)a.val, 8 * (z0 + e0), 8 * (z0 + e1), &S.bar[k], h.sh_val);
+}
+
 // L lanes per row: lanes stride over the row's entries (BU entries per lane
 // loaded before any is used); the partials are combined with a fixed xor
 // tree, so every run gives the same bits.  Two rows per lane group are in
 // flight at once (i1 < 0: none).
-constexpr int BU = 4;
+#ifndef MF_BATCH_BU
+#define MF_BATCH_BU 8
+#endif
+constexpr int BU = MF_BATCH_BU;
 
 // Row bounds of the two rows of a step (0, 0 for a missing row).
 struct RowPair {
@@ -111,7 +201,7 @@ __device__ __forceinline__ RowPair row_pair(const int *__restrict__ rp, int i0, 
     return p;
 }
 
-template <int L, bool MIX, class Src>
+template <int L, bool MIX, class Src, bool GLOBAL = true>
 __device__ __forceinline__ void row_dot2(const RowPair &rb, const int *__restrict__ col,
                                          const double *__restrict__ val, const float *__restrict__ val32, int lane,
                                          Src src, double &y0, double &y1)
@@ -129,14 +219,26 @@ __device__ __forceinline__ void row_dot2(const RowPair &rb, const int *__restric
         for (int u = 0; u < BU; u++) {
             const int kk = k + u * L;
             const bool in0 = kk < n0, in1 = kk < n1;
-            c0[u] = in0 ? __ldcs(col + a0 + kk) : -1;
-            c1[u] = in1 ? __ldcs(col + a1 + kk) : -1;
-            if (MIX) {
-                w0[u] = in0 ? __ldcs(val32 + a0 + kk) : 0.0f;
-                w1[u] = in1 ? __ldcs(val32 + a1 + kk) : 0.0f;
-            } else {
-                v0[u] = in0 ? __ldcs(val + a0 + kk) : 0.0;
-                v1[u] = in1 ? __ldcs(val + a1 + kk) : 0.0;
+            if constexpr (GLOBAL) {
+                c0[u] = in0 ? __ldcs(col + a0 + kk) : -1;
+                c1[u] = in1 ? __ldcs(col + a1 + kk) : -1;
+                if (MIX) {
+                    w0[u] = in0 ? __ldcs(val32 + a0 + kk) : 0.0f;
+                    w1[u] = in1 ? __ldcs(val32 + a1 + kk) : 0.0f;
+                } else {
+                    v0[u] = in0 ? __ldcs(val + a0 + kk) : 0.0;
+                    v1[u] = in1 ? __ldcs(val + a1 + kk) : 0.0;
+                }
+            } else {  // staged in shared memory
+                c0[u] = in0 ? col[a0 + kk] : -1;
+                c1[u] = in1 ? col[a1 + kk] : -1;
+                if (MIX) {
+                    w0[u] = in0 ? val32[a0 + kk] : 0.0f;
+                    w1[u] = in1 ? val32[a1 + kk] : 0.0f;
+                } else {
+                    v0[u] = in0 ? val[a0 + kk] : 0.0;
+                    v1[u] = in1 ? val[a1 + kk] : 0.0;
+                }
             }
         }
         XT x0[BU], x1[BU];
@@ -169,14 +271,29 @@ __device__ __forceinline__ void row_dot2(const RowPair &rb, const int *__restric
     y1 = s1;
 }
 
+#ifndef MF_BATCH_MINB
+#define MF_BATCH_MINB 2
+#endif
+
 template <int L, bool MIX>
-__global__ void __launch_bounds__(BNT) k_batched_cg(BatchArgs a)
+__global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
 {
     using VT = typename std::conditional<MIX, float, double>::type;
     cg::cluster_group cl = cg::this_cluster();
     __shared__ double s_warp[BNT / 32];
     __shared__ double s_slot[4];
     __shared__ int s_sys;
+    __shared__ int s_fail;
+    extern __shared__ __align__(16) unsigned char b_smem_raw[];
+    BSmem &S = *reinterpret_cast<BSmem *>(b_smem_raw);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < BNS; k++) mbar_init(&S.bar[k], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    unsigned use[BNS];
+#pragma unroll
+    for (int k = 0; k < BNS; k++) use[k] = 0;
     const unsigned rank = cl.block_rank(), ncta = cl.num_blocks();
     const int tid = threadIdx.x;
     const int lane = tid % L, grp = tid / L;
@@ -198,9 +315,11 @@ __global__ void __launch_bounds__(BNT) k_batched_cg(BatchArgs a)
         double *x = a.x + r0;
         VT *r = (VT *)a.r + r0, *q = (VT *)a.q + r0, *xlo = (VT *)a.xlo + r0;
         VT *pb[2] = {(VT *)a.p0 + r0, (VT *)a.p1 + r0};
-        // this CTA's rows
-        const int per = (n + ncta - 1) / ncta;
-        const int ra = min(n, (int)rank * per), rb = min(n, ra + per);
+        // this CTA's chunks and rows
+        const int sc0 = a.sc[sys], nch = a.sc[sys + 1] - sc0;
+        const int cl0 = sc0 + (int)((long long)nch * rank / ncta), cl1 = sc0 + (int)((long long)nch * (rank + 1) / ncta);
+        const int ra = a.crow[cl0 + sys], rb = a.crow[cl1 + sys];
+        const long long rp_base = r0 + sys;
         double lb = 0.0, lr = 0.0;
         for (int i = ra + tid; i < rb; i += BNT) {
             const double bv = b[i];
@@ -226,39 +345,97 @@ __global__ void __launch_bounds__(BNT) k_batched_cg(BatchArgs a)
             const VT *pold = pb[it & 1];
             VT *pnew = pb[(it & 1) ^ 1];
             const VT bt = (VT)beta;
-            const VT *rr = r;
-            auto psrc = [=](int c) -> VT {
-                if constexpr (MIX) return fmaf(bt, pold[c], rr[c]);
-                else return fma(bt, pold[c], rr[c]);
-            };
+            // p = r + beta p over this CTA's rows, then a cluster barrier: the
+            // SpMV gathers one vector (random column patterns make every
+            // gathered element its own memory request)
+            for (int i = ra + tid; i < rb; i += BNT) {
+                if constexpr (MIX) pnew[i] = fmaf(bt, pold[i], r[i]);
+                else pnew[i] = fma(bt, pold[i], r[i]);
+            }
+            cl.sync();
+            const VT *pn_c = pnew;
+            auto psrc = [=](int c) -> VT { return pn_c[c]; };
             double loc = 0.0;
-            // the trip count is the same for every lane (shuffles inside)
-            // row bounds of the next step are loaded while this step computes
-            RowPair nxt = row_pair(rp, ra + grp < rb ? ra + grp : -1, ra + GPB + grp < rb ? ra + GPB + grp : -1);
-            for (int base = ra; base < rb; base += 2 * GPB) {
-                const int i0 = base + grp < rb ? base + grp : -1;
-                const int i1 = base + GPB + grp < rb ? base + GPB + grp : -1;
-                const RowPair cur = nxt;
-                const int n0 = base + 2 * GPB + grp, n1 = base + 3 * GPB + grp;
-                nxt = row_pair(rp, n0 < rb ? n0 : -1, n1 < rb ? n1 : -1);
-                double y0, y1;
-                row_dot2<L, MIX>(cur, col, val, val32, lane, psrc, y0, y1);
-                if (lane == 0) {
-                    if (i0 >= 0) {
-                        const VT pn = psrc(i0);
-                        pnew[i0] = pn;
-                        q[i0] = (VT)y0;
-                        loc += (double)pn * (double)(VT)y0;
-                    }
-                    if (i1 >= 0) {
-                        const VT pn = psrc(i1);
-                        pnew[i1] = pn;
-                        q[i1] = (VT)y1;
-                        loc += (double)pn * (double)(VT)y1;
+            auto emit = [&](int i, VT pn, double y) {
+                q[i] = (VT)y;
+                loc += (double)pn * (double)(VT)y;
+            };
+            // the CTA's row chunks stream through two shared-memory stages
+            // (bulk copies, completion on an mbarrier); every wait is bounded
+            // and voted CTA-wide, and a failure is voted cluster-wide below
+            bool fail = false;
+            // thread 0 keeps the bounds of the next chunk to issue in registers,
+            // loaded one issue ahead
+            BChunk nxt;
+            if (tid == 0) {
+                for (int j = 0; j < BNS && cl0 + j < cl1; j++) b_issue<MIX>(a, S, rp_base, z0, b_chunk(a, sys, cl0 + j), j);
+                if (cl0 + BNS < cl1) nxt = b_chunk(a, sys, cl0 + BNS);
+            }
+            __syncthreads();
+            for (int c = cl0; c < cl1; c++) {
+                const int k = (c - cl0) % BNS;
+                const bool w = mbar_wait_bounded(&S.bar[k], use[k] & 1u, a.queue + 1, a.budget_ns);
+                use[k]++;
+                if (w) {
+                    const BHdr &h = S.hdr[k];
+                    const unsigned char *st = S.stage[k];
+                    const int *rps = (const int *)(st + BOFF_RP + h.sh_rp);  // rowptr[h.r0 + j]
+                    const int nr = h.r1 - h.r0;
+                    // the trip count is the same for every lane (shuffles inside)
+                    for (int qb = 0; qb < nr; qb += 2 * GPB) {
+                        const int q0 = qb + grp, q1 = qb + GPB + grp;
+                        // the rows' own p values are loaded before the row sums
+                        VT pn0 = (VT)0, pn1 = (VT)0;
+                        if (lane == 0) {
+                            if (q0 < nr) pn0 = psrc(h.r0 + q0);
+                            if (q1 < nr) pn1 = psrc(h.r0 + q1);
+                        }
+                        RowPair rr;
+                        rr.a0 = q0 < nr ? rps[q0] : 0;
+                        rr.e0 = q0 < nr ? rps[q0 + 1] : 0;
+                        rr.a1 = q1 < nr ? rps[q1] : 0;
+                        rr.e1 = q1 < nr ? rps[q1 + 1] : 0;
+                        double y0, y1;
+                        if (h.direct) {
+                            row_dot2<L, MIX, decltype(psrc), true>(rr, col, val, val32, lane, psrc, y0, y1);
+                        } else {
+                            rr.a0 -= h.e0;
+                            rr.e0 -= h.e0;
+                            rr.a1 -= h.e0;
+                            rr.e1 -= h.e0;
+                            row_dot2<L, MIX, decltype(psrc), false>(
+                                rr, (const int *)(st + BOFF_COL + h.sh_col), (const double *)(st + BOFF_VAL + h.sh_val),
+                                (const float *)(st + BOFF_VAL + h.sh_val), lane, psrc, y0, y1);
+                        }
+                        if (lane == 0) {
+                            if (q0 < nr) emit(h.r0 + q0, pn0, y0);
+                            if (q1 < nr) emit(h.r0 + q1, pn1, y1);
+                        }
                     }
                 }
+                if (!__syncthreads_and(w)) {
+                    fail = true;
+                    // the later stages may still be landing
+                    for (int j = 1; j < BNS && c + j < cl1; j++) {
+                        const int kj = (c + j - cl0) % BNS;
+                        mbar_wait_bounded(&S.bar[kj], use[kj] & 1u, a.queue + 1, a.budget_ns);
+                        use[kj]++;
+                    }
+                    break;
+                }
+                if (tid == 0 && c + BNS < cl1) {
+                    b_issue<MIX>(a, S, rp_base, z0, nxt, k);
+                    if (c + BNS + 1 < cl1) nxt = b_chunk(a, sys, c + BNS + 1);
+                }
             }
+            if (tid == 0) s_fail = fail ? 1 : 0;
             const double pq = cluster_sum(cl, loc, &s_slot[2], s_warp);
+            int any_fail = 0;
+            for (unsigned kk = 0; kk < ncta; kk++) any_fail |= *cl.map_shared_rank(&s_fail, kk);
+            if (any_fail) {
+                status = MF_ERR_TIMEOUT;
+                break;
+            }
             if (!(pq != 0.0) || !isfinite(pq)) {
                 status = MF_ERR_BREAKDOWN;
                 break;
@@ -336,7 +513,8 @@ int batched_ctas(int count, int cluster)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     // clusters of 16 CTAs are above the portable size: allowed explicitly
     if (cluster > 8) cudaFuncSetAttribute(k_batched_cg<L, MIX>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batched_cg<L, MIX>, BNT, 0);
+    cudaFuncSetAttribute(k_batched_cg<L, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BSmem));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batched_cg<L, MIX>, BNT, sizeof(BSmem));
     int ctas = sms * (per > 0 ? per : 1);
     ctas = (ctas / cluster) * cluster;
     const int want = count * cluster;
@@ -368,6 +546,7 @@ mf_status launch_batched(const BatchArgs &a, int cluster, int ctas, cudaStream_t
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.blockDim = dim3(BNT);
+    cfg.dynamicSmemBytes = sizeof(BSmem);
     cfg.stream = s;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
@@ -468,6 +647,24 @@ mf_status mf_batch_create(int count, const int *n, const int *const *rowptr, con
         memcpy(&hcol[nz0[s]], colidx[s], sizeof(int) * e);
         memcpy(&hval[nz0[s]], val[s], sizeof(double) * e);
     }
+    // row chunks of each system: at most BCR rows and BCE entries (a longer
+    // row alone); per system nch + 1 row starts and entry offsets
+    std::vector<int> sc(count + 1), crow, cent;
+    for (int s = 0; s < count; s++) {
+        sc[s] = (int)(crow.size() - s);
+        const int *rp = rowptr[s];
+        int r = 0;
+        while (r < n[s]) {
+            crow.push_back(r);
+            cent.push_back(rp[r]);
+            const int r_start = r;
+            r++;
+            while (r < n[s] && r - r_start < BCR && rp[r + 1] - rp[r_start] <= BCE) r++;
+        }
+        crow.push_back(n[s]);
+        cent.push_back(rp[n[s]]);
+    }
+    sc[count] = (int)(crow.size() - count);
     std::vector<int> order(count);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return n[a] > n[b]; });
@@ -483,7 +680,10 @@ mf_status mf_batch_create(int count, const int *n, const int *const *rowptr, con
     BT_ALLOC(bt->d_n, sizeof(int) * count);
     BT_ALLOC(bt->d_row0, sizeof(long long) * count);
     BT_ALLOC(bt->d_nz0, sizeof(long long) * count);
-    BT_ALLOC(bt->d_rowptr, sizeof(int) * (rows + count));
+    BT_ALLOC(bt->d_rowptr, sizeof(int) * (rows + count + 8));  // slack: 16-byte bulk-copy rounding
+    BT_ALLOC(bt->d_sc, sizeof(int) * (count + 1));
+    BT_ALLOC(bt->d_crow, sizeof(int) * crow.size());
+    BT_ALLOC(bt->d_cent, sizeof(int) * cent.size());
     BT_ALLOC(bt->d_col, sizeof(int) * (nz + 4));
     BT_ALLOC(bt->d_val, sizeof(double) * (nz + 2));
     BT_ALLOC(bt->d_val32, sizeof(float) * (nz + 4));
@@ -498,6 +698,9 @@ mf_status mf_batch_create(int count, const int *n, const int *const *rowptr, con
     if (e == cudaSuccess) e = cudaMemcpy(bt->d_row0, row0.data(), sizeof(long long) * count, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(bt->d_nz0, nz0.data(), sizeof(long long) * count, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(bt->d_rowptr, hrp.data(), sizeof(int) * (rows + count), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bt->d_sc, sc.data(), sizeof(int) * (count + 1), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bt->d_crow, crow.data(), sizeof(int) * crow.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bt->d_cent, cent.data(), sizeof(int) * cent.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && nz) e = cudaMemcpy(bt->d_col, hcol.data(), sizeof(int) * nz, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && nz) e = cudaMemcpy(bt->d_val, hval.data(), sizeof(double) * nz, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && nz) {
@@ -516,7 +719,8 @@ mf_status mf_batch_destroy(mf_batch bt)
     if (!bt) return MF_OK;
     if (bt->graph) cudaGraphExecDestroy(bt->graph);
     void *bufs[] = {bt->d_order, bt->d_n, bt->d_row0, bt->d_nz0, bt->d_rowptr, bt->d_col, bt->d_val, bt->d_val32,
-                    bt->d_iters, bt->d_refs, bt->d_status, bt->d_relres, bt->work, bt->d_queue};
+                    bt->d_iters, bt->d_refs, bt->d_status, bt->d_relres, bt->work, bt->d_queue, bt->d_sc,
+                    bt->d_crow, bt->d_cent};
     for (void *p : bufs)
         if (p) cudaFree(p);
     delete bt;
@@ -579,7 +783,11 @@ static mf_status batch_enqueue(mf_batch bt, const double *b, double *x, const mf
     a.maxiter = o.maxiter;
     a.tol = o.tol;
     a.delta = (o.refine_delta > 0 && o.refine_delta < 1) ? o.refine_delta : 0.1;
-    MF_CUDA(cudaMemsetAsync(bt->d_queue, 0, sizeof(int), s));
+    a.budget_ns = (unsigned long long)(o.wait_budget_s * 1e9);
+    a.sc = bt->d_sc;
+    a.crow = bt->d_crow;
+    a.cent = bt->d_cent;
+    MF_CUDA(cudaMemsetAsync(bt->d_queue, 0, sizeof(int) * 2, s));  // queue head, stage-wait status
     if (mixed) MF_TRY(launch_batched_l<true>(lanes, a, cluster, ctas, s));
     else MF_TRY(launch_batched_l<false>(lanes, a, cluster, ctas, s));
     k_batch_resid<<<std::min(bt->count, 1184), 256, 0, s>>>(bt->count, bt->d_n, bt->d_row0, bt->d_nz0, bt->d_rowptr,
@@ -605,11 +813,11 @@ mf_status mf_batch_cg_solve(mf_batch bt, const double *b, double *x, const mf_so
     }
     cudaStream_t s = (cudaStream_t)stream;
     int lanes = bt->tuned_lanes ? bt->tuned_lanes : 8;
-    int cluster = bt->tuned_cluster ? bt->tuned_cluster : 8;
+    int cluster = bt->tuned_cluster ? bt->tuned_cluster : 4;
     if (const char *e = getenv("MF_BATCH_LANES")) lanes = atoi(e);
     if (const char *e = getenv("MF_BATCH_CLUSTER")) cluster = atoi(e);
     if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) lanes = 8;
-    if (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16) cluster = 8;
+    if (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16) cluster = 4;
     const bool mixed = o.policy != MF_POLICY_FP64;
     MF_TRY(batch_work(bt, mixed));
     const int ctas = mixed ? batched_ctas_l<true>(lanes, bt->count, cluster) : batched_ctas_l<false>(lanes, bt->count, cluster);

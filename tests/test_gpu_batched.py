@@ -70,7 +70,7 @@ def test_batched_autotuner_picks_a_schedule(mf, batch):
     db = torch.from_numpy(B.stack(bs)).cuda()
     dx = torch.zeros_like(db)
     lanes, cluster = B.tune(db.data_ptr(), dx.data_ptr(), tol=1e-10, maxiter=20000)
-    assert lanes in (4, 8, 16, 32) and cluster in (1, 2, 4, 8)
+    assert lanes in (4, 8, 16, 32) and cluster in (1, 2, 4, 8, 16)
     st, rep = B.solve_device(db.data_ptr(), dx.data_ptr(), use_graph=1, tol=1e-10, maxiter=20000)
     assert st == 0 and rep.lanes_per_row == lanes and rep.cluster_ctas == cluster
 

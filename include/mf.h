@@ -286,6 +286,14 @@ mf_status mf_batch_tune(mf_batch bt, const double *b, double *x, const mf_solve_
 /* lanes in {4, 8, 16, 32}, cluster in {1, 2, 4, 8, 16}. */
 mf_status mf_batch_set_schedule(mf_batch bt, int lanes, int cluster);
 
+/* Diagnostic: runs the persistent kernels' bounded waits (a grid barrier
+ * whose second epoch nobody completes, an mbarrier nobody arrives at) on 2
+ * CTAs and reports how they ended: results[0] = the device status word
+ * (MF_ERR_TIMEOUT expected), then per CTA {first barrier passed (1), second
+ * barrier passed (0), mbarrier wait expired with MF_ERR_TIMEOUT (1)}.  7
+ * ints.  budget_s in (0, 10].  No reference counterpart. */
+mf_status mf_selftest_bounded_waits(double budget_s, int *results);
+
 /* ---------------------------------------------------------------------- */
 /* Matrix Market input and synthetic matrices                              */
 /* ---------------------------------------------------------------------- */

@@ -140,3 +140,25 @@ def test_mixed_deterministic(mf):
     assert r1.iterations == r2.iterations and r1.refinements == r2.refinements
     assert np.array_equal(x1, x2)
     M.close()
+
+
+def test_bounded_waits_expire_and_context_stays_usable(mf):
+    """The persistent kernels' waits are bounded: a grid-barrier epoch that
+    nobody completes and an mbarrier nobody arrives at both expire after the
+    budget with MF_ERR_TIMEOUT in the status word, the kernel returns, and
+    the next solve runs normally."""
+    import ctypes as C
+
+    L = mf.lib()
+    L.mf_selftest_bounded_waits.argtypes = [C.c_double, C.c_void_p]
+    res = np.zeros(7, np.int32)
+    assert L.mf_selftest_bounded_waits(0.2, res.ctypes.data) == 0
+    assert res[0] == 4  # MF_ERR_TIMEOUT
+    for cta in range(2):
+        assert list(res[1 + 3 * cta: 4 + 3 * cta]) == [1, 0, 1], res
+    A = mf.synth_laplace2d(32, 32)
+    b = A.matvec(np.ones(A.n_rows))
+    M = mf.Matrix(A)
+    x, rep = M.solve_host(b, tol=1e-10)
+    assert rep.status == 0 and np.max(np.abs(x - 1.0)) < 1e-8
+    M.close()

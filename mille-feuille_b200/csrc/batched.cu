@@ -415,10 +415,11 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                 }
                 if (!__syncthreads_and(w)) {
                     fail = true;
-                    // the later stages may still be landing
+                    // this stage and the later ones may still be landing
+                    mbar_drain(&S.bar[k], (use[k] - 1u) & 1u, a.queue + 1, a.budget_ns);
                     for (int j = 1; j < BNS && c + j < cl1; j++) {
                         const int kj = (c + j - cl0) % BNS;
-                        mbar_wait_bounded(&S.bar[kj], use[kj] & 1u, a.queue + 1, a.budget_ns);
+                        mbar_drain(&S.bar[kj], use[kj] & 1u, a.queue + 1, a.budget_ns);
                         use[kj]++;
                     }
                     break;

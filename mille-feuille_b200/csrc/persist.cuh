@@ -318,9 +318,14 @@ __device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb,
         // CTA-wide vote on the bounded wait so that every thread leaves together
         if (!__syncthreads_and(mbar_wait_bounded(&S.bar[k], gc.use[k] & 1u, a.status, a.budget_ns))) {
             ok = false;
-            // the other stage may still have a copy in flight: wait for it
-            // (bounded) before leaving so no copy lands in freed memory
-            if (c + 1 < ce) mbar_wait_bounded(&S.bar[k ^ 1], gc.use[k ^ 1] & 1u, a.status, a.budget_ns);
+            // this stage and the other may still have copies in flight: wait
+            // for them before leaving so no copy lands in freed memory
+            mbar_drain(&S.bar[k], gc.use[k] & 1u, a.status, a.budget_ns);
+            gc.use[k]++;
+            if (c + 1 < ce) {
+                mbar_drain(&S.bar[k ^ 1], gc.use[k ^ 1] & 1u, a.status, a.budget_ns);
+                gc.use[k ^ 1]++;
+            }
             break;
         }
         gc.use[k]++;
@@ -580,10 +585,11 @@ __device__ bool spmv_slots(const CgArgs &a, SlotSmem &S, GridCtx &gc, int cb, in
             }
         }
         if (!__syncthreads_and(w)) {
-            // chunks c+1 .. c+NSTG-1 may still be landing
+            // chunks c .. c+NSTG-1 may still be landing
+            mbar_drain(&S.bar[k], (gc.use[k] - 1u) & 1u, a.status, a.budget_ns);
             for (int jj = 1; jj < NSTG && c + jj < ce; jj++) {
                 const int kj = (c + jj - cb) % NSTG;
-                mbar_wait_bounded(&S.bar[kj], gc.use[kj] & 1u, a.status, a.budget_ns);
+                mbar_drain(&S.bar[kj], gc.use[kj] & 1u, a.status, a.budget_ns);
                 gc.use[kj]++;
             }
             __syncthreads();

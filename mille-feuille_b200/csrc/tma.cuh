@@ -82,4 +82,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity
     }
 }
 
+// Failure paths: waits for copies known to be in flight before a CTA
+// leaves.  Bounded, but never shorter than one second, so that a tiny wait
+// budget given to a solve cannot let a CTA leave while bulk copies are still
+// landing in its shared memory.
+__device__ __forceinline__ void mbar_drain(uint64_t *bar, unsigned parity, int *status, unsigned long long budget_ns)
+{
+    mbar_wait_bounded(bar, parity, status, budget_ns > 1000000000ull ? budget_ns : 1000000000ull);
+}
+
 }  // namespace mf

@@ -162,3 +162,58 @@ def test_bounded_waits_expire_and_context_stays_usable(mf):
     x, rep = M.solve_host(b, tol=1e-10)
     assert rep.status == 0 and np.max(np.abs(x - 1.0)) < 1e-8
     M.close()
+
+
+def test_tiny_wait_budget_is_safe(mf):
+    """A 1 ns wait budget: every grid-barrier and stage wait either completes
+    at its first polls or expires; the solve ends with MF_OK or
+    MF_ERR_TIMEOUT (copies in flight are drained before a CTA leaves), and
+    the next solve on the same matrix runs normally.  (The deterministic
+    expiry of both wait kinds is mf_selftest_bounded_waits' test.)"""
+    import ctypes as C
+
+    A = mf.synth_laplace2d(128, 128)
+    b = A.matvec(np.ones(A.n_rows))
+    M = mf.Matrix(A)
+    x = np.zeros(A.n_rows)
+    rep = mf.SolveReport()
+    o = mf.solve_opts(tol=1e-10, maxiter=5000, wait_budget_s=1e-9)
+    st = mf.lib().mf_cg_solve_host(M.h, b.ctypes.data, x.ctypes.data, C.byref(o), C.byref(rep))
+    assert st in (0, 4) and rep.status == st  # MF_OK or MF_ERR_TIMEOUT
+    x, rep = M.solve_host(b, tol=1e-10, maxiter=5000)
+    assert rep.status == 0 and np.max(np.abs(x - 1.0)) < 1e-7
+    M.close()
+
+
+def test_nan_value_reports_breakdown(mf):
+    import ctypes as C
+
+    A = mf.synth_laplace2d(32, 32)
+    A.val[5] = np.nan
+    M = mf.Matrix(A)
+    b = np.ones(A.n_rows)
+    x = np.zeros(A.n_rows)
+    rep = mf.SolveReport()
+    o = mf.solve_opts(tol=1e-10, maxiter=1000)
+    st = mf.lib().mf_cg_solve_host(M.h, b.ctypes.data, x.ctypes.data, C.byref(o), C.byref(rep))
+    assert st == 5 and rep.status == 5  # MF_ERR_BREAKDOWN
+    M.close()
+
+
+def test_zero_curvature_reports_breakdown(mf):
+    """A = blocks [[0, 1], [1, 0]], b = e_0: q = A b = e_1, p.q = 0."""
+    import ctypes as C
+
+    n = 32
+    rp = np.arange(0, n + 1, dtype=np.int32)
+    ci = np.array([i ^ 1 for i in range(n)], np.int32)
+    A = mf.HostCsr(n, n, rp, ci, np.ones(n))
+    M = mf.Matrix(A)
+    b = np.zeros(n)
+    b[0] = 1.0
+    x = np.zeros(n)
+    rep = mf.SolveReport()
+    o = mf.solve_opts(tol=1e-10, maxiter=100)
+    st = mf.lib().mf_cg_solve_host(M.h, b.ctypes.data, x.ctypes.data, C.byref(o), C.byref(rep))
+    assert st == 5 and rep.status == 5
+    M.close()

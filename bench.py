@@ -14,6 +14,8 @@ Workloads (--workload):
                   100-611, one graph-captured batched launch per step; the
                   plain FP64 tiled solves of the same systems one after
                   another are timed beside it (fp64 key).
+  lap2d           CG on the 2D 5-point Laplacian 128^2 (seed 0) to 1e-10: small
+                  enough to live in L2; reports the latency-bound regime.
   convdiff        BiCGSTAB on the 96^3 convection-diffusion system to 1e-9.
   aniso           160^3 anisotropic diffusion (seed 3) with a learned policy
                   file (--policy-file), the rule policy and plain FP64.
@@ -264,6 +266,9 @@ def workload_single(args, mf, world, local):
     if args.workload == "poisson3d":
         A = mf.synth_poisson3d_scaled(GRID, SEED)
         seed, tol, name = SEED, TOL, f"poisson3d_scaled_{GRID}^3 CG to 1e-10"
+    elif args.workload == "lap2d":
+        A = mf.synth_laplace2d(128, 128)
+        seed, tol, name = 0, TOL, "laplace2d_128^2 CG to 1e-10 (L2-resident, latency-bound)"
     elif args.workload == "convdiff":
         A = mf.synth_convdiff3d(96)
         seed, tol, name = 2, 1e-9, "convdiff3d_96^3 BiCGSTAB to 1e-9"
@@ -378,7 +383,9 @@ def workload_single(args, mf, world, local):
     kname = ("k_bicgstab" if method == "bicgstab" else "k_cg") + ("_fp64" if args.policy == "fp64" else "_mixed")
     result["roofline_in"] = (per_launch, mean_ms, kname, statistics.mean(iters))
     result["dtype"] = "f64" if args.policy == "fp64" else "mixed(f32/f16/i8 tiles, f32 accumulate, f64 refinement)"
-    result["cpu"] = (A, b) if args.workload == "poisson3d" else None
+    # FP64 CG iterations to 1e-10 from the CPU oracle (scale of the CPU sample)
+    oracle_iters = {"poisson3d": FP64_ITERS_ORACLE, "lap2d": 380}.get(args.workload)
+    result["cpu"] = (A, b, oracle_iters) if oracle_iters else None
     M.close()
     return result, info
 
@@ -527,15 +534,15 @@ def run_mf(args):
         "e2e": res["e2e"], "gpu_launches": int(res["launches"]), "clocks": res["clocks"],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and res["cpu"] is not None:
-        A, b = res["cpu"]
+        A, b, oracle_iters = res["cpu"]
         cpu = CpuReference(A, b)
         if cpu.ref is not None:
-            k = cpu.auto_iters(15.0)
+            k = min(cpu.auto_iters(15.0), oracle_iters)
             t = cpu.seconds_per_iteration(k)
-            line["cpu_baseline"] = {"value": 1.0 / (t * FP64_ITERS_ORACLE), "unit": UNIT, "cores": cpu.threads,
+            line["cpu_baseline"] = {"value": 1.0 / (t * oracle_iters), "unit": UNIT, "cores": cpu.threads,
                                     "kind": "reference",
                                     "sample": f"{k} CG iterations (reference blockspmv_cpu, serial, + OpenMP vector "
-                                              f"loops on {cpu.threads} threads), scaled by {FP64_ITERS_ORACLE} "
+                                              f"loops on {cpu.threads} threads), scaled by {oracle_iters} "
                                               f"FP64 iterations to 1e-10; reference Tile_create {cpu.setup_s:.1f} s "
                                               f"not timed"}
     if rank == 0:
@@ -551,7 +558,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mf", "reference"], default="mf")
-    ap.add_argument("--workload", default="poisson3d", choices=["poisson3d", "batched", "convdiff", "aniso"])
+    ap.add_argument("--workload", default="poisson3d", choices=["poisson3d", "lap2d", "batched", "convdiff", "aniso"])
     ap.add_argument("--policy", default="static", choices=["fp64", "static", "rule", "learned"])
     ap.add_argument("--policy-file", default=None, help="learned policy (mf_policy_save format)")
     ap.add_argument("--no-fp64-baseline", action="store_true")

@@ -31,7 +31,7 @@ constexpr int RECS = 64;                    // chunk records cached in shared me
 // Byte layout of one shared-memory stage (every region 16-byte aligned,
 // sized for the largest 16-byte-rounded range it receives).
 constexpr int OFF_TPTR = 0;                                   // tile_ptr[s0..s1]
-constexpr int OFF_TCOL = 112;                                 // tile_columnidx[t0..t1)
+constexpr int OFF_TCOL = ((CH_STRIPS + 1) * 4 + 32 + 15) / 16 * 16;  // tile_columnidx[t0..t1)
 constexpr int OFF_TNNZ = OFF_TCOL + CH_TILES * 4 + 32;        // tile_nnz[t0..t1]
 constexpr int OFF_POFF = OFF_TNNZ + CH_TILES * 4 + 48;        // packed offsets[t0..t1]
 constexpr int OFF_WCLS = OFF_POFF + CH_TILES * 4 + 48;        // classes[t0..t1)
@@ -64,8 +64,8 @@ struct __align__(16) SolverSmem {
 // payload).  Every region is 16-byte aligned and sized for the largest
 // 16-byte-rounded range it receives.
 constexpr int SOFF_SSLOT = 0;
-constexpr int SOFF_TPTR = 112;
-constexpr int SOFF_TCOL = 224;
+constexpr int SOFF_TPTR = ((SC_STRIPS + 1) * 4 + 32 + 15) / 16 * 16;
+constexpr int SOFF_TCOL = 2 * SOFF_TPTR;
 constexpr int SOFF_META = SOFF_TCOL + SC_TILES * 4 + 32;
 constexpr int SOFF_DATA = SOFF_META + SC_SLOTS * MF_TILE * 2 + 32;
 constexpr int SOFF_PAY = SOFF_DATA + SC_SLOTS * 4 + 32;  // mixed payload after the slot headers

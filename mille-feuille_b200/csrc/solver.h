@@ -30,7 +30,7 @@ struct ChunkRec {
 // slots, and the parts' sums are added in order.  A strip too large for a
 // stage on its own is a one-strip chunk with `direct` set (16 half-warps,
 // read from global memory).
-constexpr int SC_STRIPS = 16, SC_SLOTS = 128, SC_TILES = 256;
+constexpr int SC_STRIPS = CH_STRIPS, SC_SLOTS = 8 * SC_STRIPS, SC_TILES = 16 * SC_STRIPS;
 struct SlotChunk {
     int s0, s1;            // strips [s0, s1)
     int k0, k1;            // slots [k0, k1)

@@ -398,7 +398,7 @@ def workload_batched(args, mf, world, local):
     from concurrent.futures import ThreadPoolExecutor
 
     L = mf.lib()
-    N = 512
+    N = args.systems
     with ThreadPoolExecutor(16) as ex:
         systems = list(ex.map(lambda k: mf.synth_random_spd(100 + k), range(N)))
         xs = list(ex.map(lambda k: mf.synth_xstar(100 + k, systems[k].n_rows), range(N)))
@@ -446,7 +446,7 @@ def workload_batched(args, mf, world, local):
     alg = 0
     for A, it in zip(systems, its):
         alg += int(it) * (A.nnz * (sb + 1) + 24 * tiles_of(A) + 16 * A.n_rows + vb * A.n_rows)
-    info = {"workload": "batched random SPD x512 (n ~ log-uniform[1k,64k], seeds 100-611) CG to 1e-10",
+    info = {"workload": f"batched random SPD x{N} (n ~ log-uniform[1k,64k], seeds 100-{99 + N}) CG to 1e-10",
             "systems": N, "rows_total": int(sum(A.n_rows for A in systems)),
             "nnz_total": int(sum(A.nnz for A in systems)), "policy": args.policy,
             "iterations_mean": float(its.mean()), "iterations_max": int(its.max()),
@@ -564,6 +564,7 @@ def main():
     ap.add_argument("--policy", default="static", choices=["fp64", "static", "rule", "learned"])
     ap.add_argument("--policy-file", default=None, help="learned policy (mf_policy_save format)")
     ap.add_argument("--no-fp64-baseline", action="store_true")
+    ap.add_argument("--systems", type=int, default=512, help="batched workload: number of systems (seeds 100..)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="device solves only (no e2e, clocks or CPU baseline): the command profiled with ncu")

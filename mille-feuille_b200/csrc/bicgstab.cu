@@ -37,7 +37,7 @@ __device__ __forceinline__ void grid_sum2(const CgArgs &a, double l0, double l1,
         a.partials[(slot + 1) * G + blockIdx.x] = c1;
     }
     gc.epoch++;
-    gc.ok = gc.ok && grid_barrier_fast(a.bar, gc.epoch, a.status, a.budget_ns);
+    gc.ok = gc.ok && MF_GRID_BARRIER(a.bar, gc.epoch, a.status, a.budget_ns);
     o0 = block_sum_partials<NT>(a.partials + slot * G, G, S.warp);
     o1 = block_sum_partials<NT>(a.partials + (slot + 1) * G, G, S.warp);
 }

@@ -194,6 +194,44 @@ __device__ __forceinline__ bool grid_barrier_fast(unsigned long long *ctr, unsig
     return s_ok != 0;
 }
 
+__device__ __forceinline__ void red_add_release_u64(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Grid-wide barrier on one counter: every CTA adds 1 with a release
+// reduction (no round trip to wait for) and spins with acquire loads until
+// the counter reaches epoch * gridDim.x.  Same bounded-spin and status rules
+// as grid_barrier_fast; ctr[0] must be zero at launch.
+__device__ __forceinline__ bool grid_barrier_flat(unsigned long long *ctr, unsigned long long epoch, int *status,
+                                                  unsigned long long budget_ns)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned long long target = epoch * (unsigned long long)gridDim.x;
+        red_add_release_u64(ctr, 1ull);
+        if (ld_acquire_u64(ctr) < target) {
+            const unsigned long long t0 = globaltimer_ns();
+            unsigned spins = 0;
+            while (ld_acquire_u64(ctr) < target) {
+                if (((++spins) & 31u) == 0u) {
+                    if (ld_volatile_i32(status) != DEV_OK) { ok = 0; break; }
+                    if (globaltimer_ns() - t0 > budget_ns) {
+                        atomicCAS(status, DEV_OK, DEV_TIMEOUT);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 // Deterministic CTA reduction of one double per thread: warp butterfly, then
 // the warp results summed in warp order.  All threads get the result.
 template <int NT>

@@ -24,6 +24,14 @@ constexpr int MINB = MF_CG_MINB;  // CTAs per SM the registers allow
 #ifndef MF_SLOT_U
 #define MF_SLOT_U 4
 #endif
+#ifndef MF_FLAT_BARRIER
+#define MF_FLAT_BARRIER 1
+#endif
+#if MF_FLAT_BARRIER
+#define MF_GRID_BARRIER grid_barrier_flat
+#else
+#define MF_GRID_BARRIER grid_barrier_fast
+#endif
 constexpr int SMINB = MF_SLOT_MINB;  // CTAs per SM of the row-slot kernels
 constexpr int SLOT_U = MF_SLOT_U;    // slots loaded before any is used
 constexpr int RECS = 64;                    // chunk records cached in shared memory
@@ -118,14 +126,14 @@ __device__ __forceinline__ double grid_sum(const CgArgs &a, double local, int sl
     double cta = block_sum<NT>(local, S.warp);
     if (threadIdx.x == 0) a.partials[slot * G + blockIdx.x] = cta;
     gc.epoch++;
-    gc.ok = gc.ok && grid_barrier_fast(a.bar, gc.epoch, a.status, a.budget_ns);
+    gc.ok = gc.ok && MF_GRID_BARRIER(a.bar, gc.epoch, a.status, a.budget_ns);
     return block_sum_partials<NT>(a.partials + slot * G, G, S.warp);
 }
 
 __device__ __forceinline__ void grid_sync(const CgArgs &a, GridCtx &gc)
 {
     gc.epoch++;
-    gc.ok = gc.ok && grid_barrier_fast(a.bar, gc.epoch, a.status, a.budget_ns);
+    gc.ok = gc.ok && MF_GRID_BARRIER(a.bar, gc.epoch, a.status, a.budget_ns);
 }
 
 // Offset of tile t's u8 row pointers in Blockcsr_Ptr (csrptr_offset without

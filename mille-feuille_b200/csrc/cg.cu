@@ -245,6 +245,119 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_cg(CgArgs a)
     }
 }
 
+// FP64 CG with one grid-wide reduction per iteration (the vector updates
+// ride on the SpMV pass).  Pass k gathers p_k = r_{k-1} - alpha q_{k-1} +
+// beta p_{k-1} on the fly from the previous pass's vectors (double-buffered
+// r, q, p), computes q_k = A p_k, and for its own rows writes p_k, q_k,
+// r_k = r_{k-1} - alpha q_{k-1} and x_k = x_{k-1} + alpha p_{k-1}; one
+// reduction then gives p.q, r.q, q.q and r.r, from which alpha_k =
+// (r.r)/(p.q) and the next ||r||^2 = r.r - 2 alpha r.q + alpha^2 q.q (so
+// beta_k) follow without a second reduction.  In exact arithmetic this is the
+// textbook method; the expanded ||r||^2 only feeds beta, the convergence test
+// uses the explicit r.r.  Pass 0 starts from r = b, q = p = 0, alpha = beta
+// = 0, so every pass runs the same code.  No checkpoints (the tracing and
+// mixed-precision solves use k_cg).
+template <int LAY>
+__global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_cg1(CgArgs a)
+{
+    using SM = typename std::conditional<LAY == 0, SolverSmem, SlotSmem>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SM &S = *reinterpret_cast<SM *>(smem_raw);
+    const MfTiles &A = a.A;
+    const int g = blockIdx.x;
+    const int sb0 = a.part[g], se0 = a.part[g + 1];
+    const int cb = LAY == 0 ? a.cta_chunk[g] : a.scta_chunk[g], ce = LAY == 0 ? a.cta_chunk[g + 1] : a.scta_chunk[g + 1];
+    const int row0 = sb0 * MF_TILE, row1 = min(se0 * MF_TILE, A.rows);
+    double *rb[2] = {(double *)a.r, (double *)a.rhat};
+    double *qb[2] = {(double *)a.q, (double *)a.v0};
+    double *pb[2] = {(double *)a.p0, (double *)a.p1};
+    double *x = a.xhi;
+    GridCtx gc;
+    gc.epoch = 0;
+    gc.ok = true;
+    gc.use[0] = gc.use[1] = gc.use[2] = gc.use[3] = 0;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < (LAY == 0 ? 2 : NSTG); i++) mbar_init(&S.bar[i], 1);
+        mbar_fence_init();
+    }
+    if constexpr (LAY == 0) {
+        for (int c = cb + threadIdx.x; c < ce && c - cb < RECS; c += NT) S.recs[c - cb] = a.chunks[c];
+    } else {
+        for (int c = cb + threadIdx.x; c < ce && c - cb < SRECS; c += NT) S.recs[c - cb] = a.schunks[c];
+    }
+    double lb = 0.0;
+    for (int i = row0 + threadIdx.x; i < row1; i += NT) {
+        const double bv = a.b[i];
+        rb[0][i] = bv;
+        qb[0][i] = 0.0;
+        pb[0][i] = 0.0;
+        x[i] = 0.0;
+        lb = __dadd_rn(lb, __dmul_rn(bv, bv));
+    }
+    __syncthreads();
+    const double bb = grid_sum(a, lb, 0, gc, S);
+    const double nb = sqrt(bb) > 0.0 ? sqrt(bb) : 1.0;
+    if (a.hist && g == 0 && threadIdx.x == 0) a.hist[0] = sqrt(bb) / nb;
+    double alpha = 0.0, beta = 0.0, rr = bb;
+    int it = -1;  // updates done; pass 0 makes r_0
+    int exit_reason = EXIT_MAXITER;
+    while (gc.ok) {
+        const int o = (it + 1) & 1;  // buffers of the previous pass
+        const double *ro = rb[o], *qo = qb[o], *po = pb[o];
+        double *rn = rb[o ^ 1], *qn = qb[o ^ 1], *pn = pb[o ^ 1];
+        const double al = alpha, be = beta;
+        auto psrc = [=](int c) -> double { return fma(be, po[c], fma(-al, qo[c], ro[c])); };
+        double l[4] = {0.0, 0.0, 0.0, 0.0};  // p.q, r.q, q.q, r.r
+        auto aout = [&](int s, int rw, double y, double xown, bool has_own) {
+            const int i = s * MF_TILE + rw;
+            const double pv = has_own ? xown : psrc(i);
+            const double rv = fma(-al, qo[i], ro[i]);
+            x[i] = fma(al, po[i], x[i]);
+            pn[i] = pv;
+            qn[i] = y;
+            rn[i] = rv;
+            l[0] = __dadd_rn(l[0], __dmul_rn(pv, y));
+            l[1] = __dadd_rn(l[1], __dmul_rn(rv, y));
+            l[2] = __dadd_rn(l[2], __dmul_rn(y, y));
+            l[3] = __dadd_rn(l[3], __dmul_rn(rv, rv));
+        };
+        if (!spmv_any<0, LAY>(a, S, gc, cb, ce, sb0, se0, psrc, aout, nullptr)) gc.ok = false;
+        double d[4];
+        grid_sum4(a, l, 4, gc, S, d);
+        if (!gc.ok) break;
+        it++;
+        rr = d[3];
+        if (a.hist && g == 0 && threadIdx.x == 0) a.hist[it] = sqrt(rr) / nb;
+        if ((!a.fixed && sqrt(rr) <= a.tol * nb) || rr == 0.0) {
+            exit_reason = EXIT_CONVERGED;
+            break;
+        }
+        if (it >= a.maxiter) {
+            exit_reason = EXIT_MAXITER;
+            break;
+        }
+        if (!(d[0] != 0.0) || !isfinite(d[0])) {
+            if (g == 0 && threadIdx.x == 0) atomicCAS(a.status, DEV_OK, DEV_BREAKDOWN);
+            exit_reason = EXIT_BREAKDOWN;
+            break;
+        }
+        alpha = rr / d[0];
+        const double rr_next = rr - 2.0 * alpha * d[1] + alpha * alpha * d[2];
+        beta = rr_next / rr;
+    }
+    if (g == 0 && threadIdx.x == 0) {
+        double *st = a.state;
+        st[S_RHO] = rr;
+        st[S_BETA] = beta;
+        st[S_NB] = nb;
+        st[S_RMAX] = sqrt(rr);
+        st[S_ITERS] = (double)(it < 0 ? 0 : it);
+        st[S_REFS] = 0.0;
+        st[S_EXIT] = (double)exit_reason;
+        st[S_RELRES] = sqrt(rr) / nb;
+    }
+}
+
 // ||b - A x||^2 and ||b||^2 from y = A x, deterministic: per-CTA partials,
 // then one CTA sums them in a fixed tree.
 __global__ void k_resid_partials(int n, const double *__restrict__ b, const double *__restrict__ ax,
@@ -389,6 +502,27 @@ mf_status launch_cg(bool mixed, CgArgs &a, int G, cudaStream_t s)
     note_launch();
     const void *fn;
     size_t dyn;
+    if (!mixed && a.one_reduction) {
+        // the grid was sized for k_cg; k_cg1 runs when as many of its CTAs
+        // are resident (same launch bounds, its own occupancy checked once)
+        static int resident[2] = {-1, -1};
+        const int li = a.sslot ? 1 : 0;
+        dyn = a.sslot ? smem_bytes<1>() : smem_bytes<0>();
+        fn = a.sslot ? (const void *)k_cg1<1> : (const void *)k_cg1<0>;
+        if (resident[li] < 0) {
+            int dev = 0, sms = 0, per = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            MF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+            MF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, NT, dyn));
+            resident[li] = sms * per;
+        }
+        if (G <= resident[li]) {
+            MF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(NT), args, dyn, s));
+            return MF_OK;
+        }
+        a.one_reduction = 0;  // fall through to the two-reduction kernel
+    }
     if (a.sslot) {
         dyn = smem_bytes<1>();
         if (mixed) max_ctas_for<true, 1>(), fn = (const void *)k_cg<true, 1>;

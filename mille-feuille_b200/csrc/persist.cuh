@@ -130,6 +130,60 @@ __device__ __forceinline__ double grid_sum(const CgArgs &a, double local, int sl
     return block_sum_partials<NT>(a.partials + slot * G, G, S.warp);
 }
 
+// Four sums at once (one barrier, one batch of partial loads): slots
+// slot..slot+3 of the partials; every CTA gets the same four values.
+template <class SM>
+__device__ __forceinline__ void grid_sum4(const CgArgs &a, const double (&l)[4], int slot, GridCtx &gc, SM &S,
+                                          double (&o)[4])
+{
+    const int G = gridDim.x;
+    __shared__ double s_w4[NT / 32][4];
+    double v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        v[k] = l[k];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], off);
+    }
+    const int w = threadIdx.x >> 5;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < 4; k++) s_w4[w][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            double c = 0.0;
+            for (int i = 0; i < NT / 32; i++) c += s_w4[i][k];
+            a.partials[(slot + k) * G + blockIdx.x] = c;
+        }
+    }
+    gc.epoch++;
+    gc.ok = gc.ok && MF_GRID_BARRIER(a.bar, gc.epoch, a.status, a.budget_ns);
+    // every thread loads its share of all four partial arrays, then one tree
+#pragma unroll
+    for (int k = 0; k < 4; k++) v[k] = 0.0;
+    for (int i = threadIdx.x; i < G; i += NT)
+#pragma unroll
+        for (int k = 0; k < 4; k++) v[k] += __ldcg(a.partials + (slot + k) * G + i);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], off);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < 4; k++) s_w4[w][k] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        double c = 0.0;
+        for (int i = 0; i < NT / 32; i++) c += s_w4[i][k];
+        o[k] = c;
+    }
+}
+
 __device__ __forceinline__ void grid_sync(const CgArgs &a, GridCtx &gc)
 {
     gc.epoch++;

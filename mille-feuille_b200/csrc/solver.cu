@@ -2,6 +2,7 @@
 // checkpoints, reports).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -92,6 +93,17 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
     // checkpoints (policy updates between launches) for CG's dynamic policies
     a.exit_on_refine = (!bicg && mixed && o.policy != MF_POLICY_STATIC) ? 1 : 0;
     a.checkpoint_every = (hook && !bicg) ? hook->every : 0;
+    // FP64 CG without checkpoints on small, short-row systems (latency-bound:
+    // the grid-wide waits dominate): one reduction per iteration.  Larger or
+    // long-row systems keep the two-reduction kernel, whose SpMV gathers two
+    // vectors instead of three.  MF_CG_VARIANT=1 / 2 forces either.
+    {
+        const char *v = getenv("MF_CG_VARIANT");
+        const bool small = m->v.rows <= (1 << 19) && (long long)m->v.nnz <= 16LL * m->v.rows;
+        const int force = v ? atoi(v) : 0;
+        const bool want = force == 1 || (force != 2 && small);
+        a.one_reduction = (!bicg && !mixed && a.checkpoint_every == 0 && want) ? 1 : 0;
+    }
     a.budget_ns = (unsigned long long)(o.wait_budget_s * 1e9);
     a.start = 1;
     a.timing = o.phase_times ? w.timing : nullptr;

@@ -86,6 +86,7 @@ struct CgArgs {
     const unsigned char *spay;     // mixed: slot payload
     const int *scta_chunk;         // [G+1] slot-chunk range of each CTA
     const SlotChunk *schunks;
+    int one_reduction;             // FP64: the single-reduction CG kernel (k_cg1)
 };
 
 struct SolverWork {

@@ -178,8 +178,13 @@ typedef struct mf_solve_report {
      * spent in [0] the SpMV phase, [1] its reduction wait, [2] the vector
      * update phase, [3] its reduction wait, [4] reliable updates, [5] the
      * largest per-CTA SpMV-phase time; inside the SpMV phase: [6] waiting
-     * for staged chunks, [7] building x segments, [8] computing rows */
+     * for staged chunks, then for tile chunks [7] building x segments and
+     * [8] computing rows, for row slots [7] computing rows and [8] the
+     * closing barrier and refill */
     double phase_us[9];
+    int layout;            /* execution layout of the solve: 0 tile chunks,
+                              1 row slots, 2 staged row slots (the chunk's
+                              vector entries copied to shared memory) */
 } mf_solve_report;
 
 /* Fills opts with the defaults (maxiter 20000, tol 1e-10, FP64 policy). */

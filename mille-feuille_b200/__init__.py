@@ -55,7 +55,7 @@ class BatchReport(C.Structure):
 class SolveReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("refinements", C.c_int), ("relres", C.c_double),
                 ("relres_true", C.c_double), ("kernel_ms", C.c_double), ("bytes_moved", C.c_longlong),
-                ("grid_ctas", C.c_int), ("phase_us", C.c_double * 9)]
+                ("grid_ctas", C.c_int), ("phase_us", C.c_double * 9), ("layout", C.c_int)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}

@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_bicgstab(CgArgs
     GridCtx gc;
     gc.epoch = 0;
     gc.ok = true;
-    gc.use[0] = gc.use[1] = gc.use[2] = gc.use[3] = 0;
+    gc.par = 0u;
     double *st = a.state;
     if (threadIdx.x == 0) {
         for (int i = 0; i < (LAY == 0 ? 2 : NSTG); i++) mbar_init(&S.bar[i], 1);

@@ -37,11 +37,26 @@ namespace mf {
 namespace {
 using namespace persist;
 
+#ifndef MF_STAGED_MINB_MIX
+#define MF_STAGED_MINB_MIX 4
+#endif
+#ifndef MF_STAGED_MINB_FP64
+#define MF_STAGED_MINB_FP64 2
+#endif
+// CTAs per SM of the kernels on staged chunks (shared memory allows them)
+constexpr int staged_minb(bool mix) { return mix ? MF_STAGED_MINB_MIX : MF_STAGED_MINB_FP64; }
+
 template <bool MIX, int LAY>
-__global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_cg(CgArgs a)
+struct CgSmem {
+    using type = typename std::conditional<LAY == 0, SolverSmem,
+                                           typename std::conditional<LAY == 1, SlotSmem, StagedSmem<MIX>>::type>::type;
+};
+
+template <bool MIX, int LAY>
+__global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : staged_minb(MIX)) k_cg(CgArgs a)
 {
     using VT = typename VecT<MIX>::T;
-    using SM = typename std::conditional<LAY == 0, SolverSmem, SlotSmem>::type;
+    using SM = typename CgSmem<MIX, LAY>::type;
     constexpr int PK = MIX ? 1 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SM &S = *reinterpret_cast<SM *>(smem_raw);
@@ -54,7 +69,7 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_cg(CgArgs a)
     GridCtx gc;
     gc.epoch = 0;
     gc.ok = true;
-    gc.use[0] = gc.use[1] = gc.use[2] = gc.use[3] = 0;
+    gc.par = 0u;
     double *st = a.state;
     if (threadIdx.x == 0) {
         for (int i = 0; i < (LAY == 0 ? 2 : NSTG); i++) mbar_init(&S.bar[i], 1);
@@ -63,7 +78,8 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_cg(CgArgs a)
     if constexpr (LAY == 0) {
         for (int c = cb + threadIdx.x; c < ce && c - cb < RECS; c += NT) S.recs[c - cb] = a.chunks[c];
     } else {
-        for (int c = cb + threadIdx.x; c < ce && c - cb < SRECS; c += NT) S.recs[c - cb] = a.schunks[c];
+        constexpr int NREC = LAY == 1 ? SRECS : TRECS;
+        for (int c = cb + threadIdx.x; c < ce && c - cb < NREC; c += NT) S.recs[c - cb] = a.schunks[c];
     }
     __syncthreads();
 
@@ -129,7 +145,9 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_cg(CgArgs a)
         MF_MARK(-1);
         // ---- q = A p_new, p_new = r + beta p_old formed on the fly ----
         double loc = 0.0;
-        auto aout = [&](int s, int rw, double y, double xown, bool has_own) {
+        // y and xown: double, or float from the staged mixed SpMV (the same
+        // values either way)
+        auto aout = [&](int s, int rw, auto y, auto xown, bool has_own) {
             const int i = s * MF_TILE + rw;
             const VT pn = has_own ? (VT)xown : psrc(i);
             const VT qi = (VT)y;
@@ -137,7 +155,12 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_cg(CgArgs a)
             q[i] = qi;
             loc = __dadd_rn(loc, __dmul_rn((double)pn, (double)qi));
         };
-        if (!spmv_any<PK, LAY>(a, S, gc, cb, ce, sb0, se0, psrc, aout, timed ? tph : nullptr)) gc.ok = false;
+        if constexpr (LAY == 2) {
+            if (!spmv_staged<PK, true, VT, 2>(a, S, gc, cb, ce, rr, pold, bt, aout, timed ? tph : nullptr))
+                gc.ok = false;
+        } else {
+            if (!spmv_any<PK, LAY>(a, S, gc, cb, ce, sb0, se0, psrc, aout, timed ? tph : nullptr)) gc.ok = false;
+        }
         MF_MARK(0);
         const double pq = grid_sum(a, loc, 2, gc, S);
         MF_MARK(1);
@@ -191,7 +214,9 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_cg(CgArgs a)
         if (MIX && (sqrt(rho_new) <= a.delta * rmax || (!a.fixed && sqrt(rho_new) <= a.tol * nb))) {
             // ---- reliable update: x_hi += x_lo; r = b - A x_hi in FP64 ----
             for (int i = row0 + threadIdx.x; i < row1; i += NT) {
-                a.xhi[i] = a.xhi[i] + (double)xlo[i];
+                const double xn = a.xhi[i] + (double)xlo[i];
+                a.xhi[i] = xn;
+                if (LAY == 2) a.xs[i] = xn;  // padded copy the staged SpMV reads
                 xlo[i] = (VT)0;
             }
             grid_sync(a, gc);
@@ -199,13 +224,19 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_cg(CgArgs a)
             loc = 0.0;
             const double *xh = a.xhi;
             auto xsrc = [=](int c) -> double { return xh[c]; };
-            auto rout = [&](int s, int rw, double y, double, bool) {
+            auto rout = [&](int s, int rw, double y, auto, bool) {
                 const int i = s * MF_TILE + rw;
                 const VT rv = (VT)(a.b[i] - y);
                 r[i] = rv;
                 loc = __dadd_rn(loc, __dmul_rn((double)rv, (double)rv));
             };
-            if (!spmv_any<0, LAY>(a, S, gc, cb, ce, sb0, se0, xsrc, rout, nullptr)) gc.ok = false;
+            if constexpr (LAY == 2) {
+                if (!spmv_staged<0, false, double, 1>(a, S, gc, cb, ce, (const double *)a.xs, (const double *)nullptr,
+                                                      0.0, rout, nullptr))
+                    gc.ok = false;
+            } else {
+                if (!spmv_any<0, LAY>(a, S, gc, cb, ce, sb0, se0, xsrc, rout, nullptr)) gc.ok = false;
+            }
             rho_new = grid_sum(a, loc, 1, gc, S);
             if (!gc.ok) break;
             rmax = sqrt(rho_new);
@@ -275,7 +306,7 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_cg1(CgArgs a)
     GridCtx gc;
     gc.epoch = 0;
     gc.ok = true;
-    gc.use[0] = gc.use[1] = gc.use[2] = gc.use[3] = 0;
+    gc.par = 0u;
     if (threadIdx.x == 0) {
         for (int i = 0; i < (LAY == 0 ? 2 : NSTG); i++) mbar_init(&S.bar[i], 1);
         mbar_fence_init();
@@ -394,10 +425,10 @@ __global__ void k_resid_final(int nblk, const double *__restrict__ part, double 
     }
 }
 
-template <int LAY>
+template <int LAY, bool MIX = false>
 constexpr size_t smem_bytes()
 {
-    return LAY == 0 ? sizeof(SolverSmem) : sizeof(SlotSmem);
+    return sizeof(typename CgSmem<MIX, LAY>::type);
 }
 
 template <bool MIX, int LAY>
@@ -408,7 +439,7 @@ int max_ctas_for()
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const size_t dyn = smem_bytes<LAY>();
+        const size_t dyn = smem_bytes<LAY, MIX>();
         cudaFuncSetAttribute(k_cg<MIX, LAY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg<MIX, LAY>, NT, dyn);
         cached = sms * (per > 0 ? per : 1);
@@ -463,10 +494,12 @@ mf_status solver_resources(mf_matrix m, int G, SolverWork &w)
     return MF_OK;
 }
 
-int solver_grid(mf_matrix m, bool mixed, bool slots)
+int solver_grid(mf_matrix m, bool mixed, int layout)
 {
-    int maxc = slots ? (mixed ? max_ctas_for<true, 1>() : max_ctas_for<false, 1>())
-                     : (mixed ? max_ctas_for<true, 0>() : max_ctas_for<false, 0>());
+    const bool slots = layout != 0;
+    int maxc = layout == 2   ? (mixed ? max_ctas_for<true, 2>() : max_ctas_for<false, 2>())
+               : layout == 1 ? (mixed ? max_ctas_for<true, 1>() : max_ctas_for<false, 1>())
+                             : (mixed ? max_ctas_for<true, 0>() : max_ctas_for<false, 0>());
     if (const char *e = getenv("MF_SOLVER_CTAS")) {
         const int v = atoi(e);
         if (v > 0 && v < maxc) maxc = v;
@@ -523,7 +556,10 @@ mf_status launch_cg(bool mixed, CgArgs &a, int G, cudaStream_t s)
         }
         a.one_reduction = 0;  // fall through to the two-reduction kernel
     }
-    if (a.sslot) {
+    if (a.spos) {
+        if (mixed) dyn = smem_bytes<2, true>(), max_ctas_for<true, 2>(), fn = (const void *)k_cg<true, 2>;
+        else dyn = smem_bytes<2, false>(), max_ctas_for<false, 2>(), fn = (const void *)k_cg<false, 2>;
+    } else if (a.sslot) {
         dyn = smem_bytes<1>();
         if (mixed) max_ctas_for<true, 1>(), fn = (const void *)k_cg<true, 1>;
         else max_ctas_for<false, 1>(), fn = (const void *)k_cg<false, 1>;

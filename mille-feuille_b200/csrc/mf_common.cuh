@@ -64,6 +64,15 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
     return v;
 }
 
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 __device__ __forceinline__ int ld_volatile_i32(const int *p)
 {
     return *(const volatile int *)p;
@@ -212,11 +221,16 @@ __device__ __forceinline__ bool grid_barrier_flat(unsigned long long *ctr, unsig
         int ok = 1;
         const unsigned long long target = epoch * (unsigned long long)gridDim.x;
         red_add_release_u64(ctr, 1ull);
-        if (ld_acquire_u64(ctr) < target) {
+        if (ld_relaxed_u64(ctr) < target) {
+            // relaxed polls (no L1 invalidation each), a short sleep after
+            // the first few so that a waiting CTA leaves the issue slots to
+            // the CTAs still computing on its SM
             const unsigned long long t0 = globaltimer_ns();
             unsigned spins = 0;
-            while (ld_acquire_u64(ctr) < target) {
-                if (((++spins) & 31u) == 0u) {
+            while (ld_relaxed_u64(ctr) < target) {
+                ++spins;
+                if (spins > 8u) __nanosleep(64);
+                if ((spins & 15u) == 0u) {
                     if (ld_volatile_i32(status) != DEV_OK) { ok = 0; break; }
                     if (globaltimer_ns() - t0 > budget_ns) {
                         atomicCAS(status, DEV_OK, DEV_TIMEOUT);
@@ -226,6 +240,7 @@ __device__ __forceinline__ bool grid_barrier_flat(unsigned long long *ctr, unsig
                 }
             }
         }
+        fence_acq_rel_gpu();  // with the relaxed load that saw the target: acquire
         s_ok = ok;
     }
     __syncthreads();

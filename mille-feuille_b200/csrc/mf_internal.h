@@ -83,6 +83,10 @@ struct mf_matrix_s {
     int *d_scta_chunk = nullptr;   // slot chunk table of the current partition
     void *d_schunks = nullptr;
     int schunk_ctas = 0, nschunks = 0;
+    int schunk_mode = 0;           // chunks built for: 1 plain, 2 staged
+    int schunk_staged = 0;         // 1: staged chunks, every one qualified
+    int schunk_unstaged = 0;       // staged build: chunks that did not qualify
+    uint16_t *d_spos = nullptr;    // staged positions of the slot entries
     // per-strip partials of mf_residual_norm
     double *d_resid = nullptr;
     size_t resid_bytes = 0;

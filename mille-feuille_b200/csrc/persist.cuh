@@ -6,6 +6,7 @@
 #include <cuda_fp16.h>
 
 #include <cstdlib>
+#include <type_traits>
 
 #include "solver.h"
 #include "tma.cuh"
@@ -116,7 +117,7 @@ struct VecT<true> {
 struct GridCtx {
     unsigned long long epoch;
     bool ok;
-    unsigned use[4];  // completed uses of each stage (mbarrier phase parity)
+    unsigned par;  // bit k: parity of the completed uses of stage k (its mbarrier phase)
 };
 
 template <class SM>
@@ -378,19 +379,19 @@ __device__ bool spmv_chunks(const CgArgs &a, SolverSmem &S, GridCtx &gc, int cb,
     for (int c = cb; c < ce; c++) {
         const int k = (c - cb) & 1;
         // CTA-wide vote on the bounded wait so that every thread leaves together
-        if (!__syncthreads_and(mbar_wait_bounded(&S.bar[k], gc.use[k] & 1u, a.status, a.budget_ns))) {
+        if (!__syncthreads_and(mbar_wait_bounded(&S.bar[k], (gc.par >> (k)) & 1u, a.status, a.budget_ns))) {
             ok = false;
             // this stage and the other may still have copies in flight: wait
             // for them before leaving so no copy lands in freed memory
-            mbar_drain(&S.bar[k], gc.use[k] & 1u, a.status, a.budget_ns);
-            gc.use[k]++;
+            mbar_drain(&S.bar[k], (gc.par >> (k)) & 1u, a.status, a.budget_ns);
+            gc.par ^= 1u << (k);
             if (c + 1 < ce) {
-                mbar_drain(&S.bar[k ^ 1], gc.use[k ^ 1] & 1u, a.status, a.budget_ns);
-                gc.use[k ^ 1]++;
+                mbar_drain(&S.bar[k ^ 1], (gc.par >> (k ^ 1)) & 1u, a.status, a.budget_ns);
+                gc.par ^= 1u << (k ^ 1);
             }
             break;
         }
-        gc.use[k]++;
+        gc.par ^= 1u << (k);
         MF_SUB(5);
         const ChunkRec &rec = S.hdr[k].rec;
         if (rec.direct) {
@@ -558,8 +559,19 @@ __device__ void issue_slot_chunk(const CgArgs &a, SlotSmem &S, int c, int k)
 // together -- after waiting (bounded) for the copies still in flight, so
 // that none lands in freed shared memory.  Returns false when a wait expired.
 template <int PK, class Src, class Out>
-__device__ bool spmv_slots(const CgArgs &a, SlotSmem &S, GridCtx &gc, int cb, int ce, Src src, Out &out)
+__device__ bool spmv_slots(const CgArgs &a, SlotSmem &S, GridCtx &gc, int cb, int ce, Src src, Out &out,
+                           unsigned long long *tph)
 {
+    // optional thread-0 timers: [5] waiting for staged chunks, [6] computing
+    // rows, [7] the closing barrier and the refill
+    const bool timed = tph != nullptr && threadIdx.x == 0;
+    unsigned long long tm = timed ? globaltimer_ns() : 0ull;
+#define MF_SSUB(k)                                       \
+    if (timed) {                                         \
+        const unsigned long long nw_ = globaltimer_ns(); \
+        tph[(k)] += nw_ - tm;                            \
+        tm = nw_;                                        \
+    }
     const MfTiles &A = a.A;
     const int tid = threadIdx.x, hw = tid >> 4, hl = tid & 15;
     if (tid == 0)
@@ -567,8 +579,9 @@ __device__ bool spmv_slots(const CgArgs &a, SlotSmem &S, GridCtx &gc, int cb, in
     __syncthreads();
     for (int c = cb; c < ce; c++) {
         const int k = (c - cb) % NSTG;
-        const bool w = mbar_wait_bounded(&S.bar[k], gc.use[k] & 1u, a.status, a.budget_ns);
-        gc.use[k]++;
+        const bool w = mbar_wait_bounded(&S.bar[k], (gc.par >> (k)) & 1u, a.status, a.budget_ns);
+        gc.par ^= 1u << (k);
+        MF_SSUB(5);
         const SlotHdr &h = S.hdr[k];
         const SlotChunk &rec = h.rec;
         // the header is valid whether or not the data arrived (written before
@@ -646,19 +659,309 @@ __device__ bool spmv_slots(const CgArgs &a, SlotSmem &S, GridCtx &gc, int cb, in
                 out(s, hl, yy, xo, ow);
             }
         }
+        MF_SSUB(6);
         if (!__syncthreads_and(w)) {
             // chunks c .. c+NSTG-1 may still be landing
-            mbar_drain(&S.bar[k], (gc.use[k] - 1u) & 1u, a.status, a.budget_ns);
+            mbar_drain(&S.bar[k], ((gc.par >> k) & 1u) ^ 1u, a.status, a.budget_ns);
             for (int jj = 1; jj < NSTG && c + jj < ce; jj++) {
                 const int kj = (c + jj - cb) % NSTG;
-                mbar_drain(&S.bar[kj], gc.use[kj] & 1u, a.status, a.budget_ns);
-                gc.use[kj]++;
+                mbar_drain(&S.bar[kj], (gc.par >> (kj)) & 1u, a.status, a.budget_ns);
+                gc.par ^= 1u << (kj);
             }
             __syncthreads();
             return false;
         }
         if (tid == 0 && c + NSTG < ce) issue_slot_chunk<PK>(a, S, c + NSTG, k);
+        MF_SSUB(7);
     }
+#undef MF_SSUB
+    return true;
+}
+
+// ---- staged slot chunks ----
+//
+// Stage layout: strip slot offsets, slot positions, FP64 values or the mixed
+// slot headers and payload, then the staged vectors (the chunk's column runs
+// of one FP64 vector or of two vectors of the solver's type, one after the
+// other, SC_XCAP elements apart).  Every region is 16-byte aligned and sized
+// for the largest 16-byte-rounded range it receives.
+template <bool MIX>
+struct StagedCfg {
+    static constexpr int OFF_SSLOT = 0;
+    static constexpr int OFF_META = SOFF_TPTR;
+    static constexpr int OFF_DATA = OFF_META + SC_SLOTS * MF_TILE * 2 + 32;
+    static constexpr int OFF_PAY = OFF_DATA + SC_SLOTS * 4 + 32;
+    static constexpr int OFF_VEC = MIX ? OFF_PAY + SC_SLOTS * 64 + 32 : OFF_DATA + SC_SLOTS * MF_TILE * 8 + 32;
+    static constexpr int VEC_BYTES = SC_XCAP * 8 * (MIX ? 1 : 2);
+    static constexpr int STAGE = OFF_VEC + VEC_BYTES;
+    static_assert(OFF_META % 16 == 0 && OFF_DATA % 16 == 0 && OFF_PAY % 16 == 0 && OFF_VEC % 16 == 0 &&
+                      STAGE % 16 == 0 && SC_XCAP % 16 == 0,
+                  "staged regions must be 16-byte aligned");
+};
+constexpr int TRECS = 32;  // staged chunk records cached in shared memory
+
+template <bool MIX>
+struct __align__(16) StagedSmem {
+    unsigned char stage[NSTG][StagedCfg<MIX>::STAGE];
+    SlotHdr hdr[NSTG];
+    SlotChunk recs[TRECS];
+    double py[NT], px[NT];
+    unsigned char pown[NT];
+    uint64_t bar[NSTG];
+    double warp[NT / 32];
+    double res;
+};
+
+// Thread 0: stage chunk c into stage k: slot offsets, positions, the values
+// when STV (FP64 values for PK 0, mixed headers and payload for PK 1), and
+// the chunk's column runs of v0 (and v1 when NV is 2).  The caller has
+// fenced the vectors (see spmv_staged).
+template <int PK, bool STV, typename VT, int NV, bool MIX>
+__device__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S, int c, int k, const VT *v0, const VT *v1)
+{
+    using C = StagedCfg<MIX>;
+    const int cb = a.scta_chunk[blockIdx.x];
+    SlotHdr &h = S.hdr[k];
+    if (c - cb < TRECS) h.rec = S.recs[c - cb];
+    else h.rec = a.schunks[c];
+    const SlotChunk &r = h.rec;  // read in place (shared memory), not copied to local memory
+    unsigned char *st = S.stage[k];
+    const long long m0 = 2ll * MF_TILE * r.k0, m1 = 2ll * MF_TILE * r.k1;
+    unsigned total = range_bytes(4ll * r.s0, 4ll * (r.s1 + 1)) + range_bytes(m0, m1);
+    if (STV) {
+        if (PK == 0) total += range_bytes(8ll * MF_TILE * r.k0, 8ll * MF_TILE * r.k1);
+        else total += range_bytes(4ll * r.k0, 4ll * (r.k1 + 1)) + range_bytes(r.y0, r.y1);
+    }
+    for (int j = 0; j < r.nrun; j++) total += (unsigned)(NV * r.rl[j] * (int)sizeof(VT));
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&S.bar[k], total);
+    add_range(st + C::OFF_SSLOT, (const unsigned char *)a.sslot, 4ll * r.s0, 4ll * (r.s1 + 1), &S.bar[k],
+              h.sh_sslot);
+    add_range(st + C::OFF_META, (const unsigned char *)a.spos, m0, m1, &S.bar[k], h.sh_meta);
+    if (STV) {
+        if (PK == 0) {
+            add_range(st + C::OFF_DATA, (const unsigned char *)a.sval, 8ll * MF_TILE * r.k0, 8ll * MF_TILE * r.k1,
+                      &S.bar[k], h.sh_data);
+        } else {
+            add_range(st + C::OFF_DATA, (const unsigned char *)a.shdr, 4ll * r.k0, 4ll * (r.k1 + 1), &S.bar[k],
+                      h.sh_data);
+            add_range(st + C::OFF_PAY, a.spay, r.y0, r.y1, &S.bar[k], h.sh_pay);
+        }
+    }
+    VT *sv = (VT *)(st + C::OFF_VEC);
+    for (int j = 0; j < r.nrun; j++) {
+        const unsigned bytes = (unsigned)(r.rl[j] * (int)sizeof(VT));
+        bulk_g2s(sv + r.rs[j], v0 + r.rg[j], bytes, &S.bar[k]);
+        if (NV == 2) bulk_g2s(sv + SC_XCAP + r.rs[j], v1 + r.rg[j], bytes, &S.bar[k]);
+    }
+}
+
+// One row from a staged chunk: the slot words are positions in the staged
+// vectors, whose entry is v0 (NV 1) or bt * v1 + v0 (NV 2, one rounding);
+// otherwise as slot_row (the position's tile, pos >> 4, changes exactly
+// where the tile column does, so the FP64 per-tile partial sums are those of
+// blockspmv_cpu).  vd may point to shared or global memory.
+#ifndef MF_STAGED_UNROLL
+#define MF_STAGED_UNROLL 2
+#endif
+constexpr int STAGED_UNROLL = MF_STAGED_UNROLL;
+
+__device__ __forceinline__ float fma_vt(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_vt(double a, double b, double c) { return fma(a, b, c); }
+
+// One FP64 row from a staged chunk: the slot words are positions in the
+// staged vectors, whose entry is v0 (NV 1) or bt * v1 + v0 (NV 2, one
+// rounding); per-tile partial sums as slot_row (the position's tile, pos >>
+// 4, changes exactly where the tile column does, so the sums round as
+// blockspmv_cpu's).  vd may point to shared or global memory.
+template <int NV>
+__device__ __forceinline__ double staged_row_fp64(const unsigned short *mt, const double *vd, int K, const double *sv0,
+                                                  const double *sv1, double bt)
+{
+    double yd = 0.0, part = 0.0;
+    int prevj = -1;
+#pragma unroll STAGED_UNROLL
+    for (int k = 0; k < K; k++) {
+        const unsigned m = mt[k * MF_TILE];
+        const double v = vd[k * MF_TILE];
+        if (m == 0xFFFFu) continue;
+        const double xv = NV == 2 ? fma(bt, sv1[m], sv0[m]) : sv0[m];
+        const int j = (int)(m >> 4);
+        if (j != prevj) {
+            yd = __dadd_rn(yd, part);
+            part = 0.0;
+            prevj = j;
+        }
+        part = __dadd_rn(part, __dmul_rn(xv, v));
+    }
+    return __dadd_rn(yd, part);
+}
+
+// One mixed row from a staged chunk: FP32 fused multiply-add accumulation in
+// row order of v = bt * v1 + v0 times the slot value decoded to FP32, empty
+// entries and bypassed slots skipped (the same operations as slot_row).
+// FMT 0 / 1 / 2: every slot of the chunk is fp32 / fp16 / int8, so slot k's
+// 16 values sit at pay_u + k * (64 >> FMT); FMT -1: each slot's header gives
+// its format and payload offset.  No branches: a skipped entry reads a
+// valid position and leaves the sum unchanged.
+template <int FMT>
+__device__ __forceinline__ float staged_row_mixed(const unsigned short *mt, const unsigned *hd, const unsigned char *pay,
+                                                  const unsigned char *pay_u, int K, int hl, const float *sv0,
+                                                  const float *sv1, float bt)
+{
+    float yf = 0.f;
+#pragma unroll STAGED_UNROLL
+    for (int k = 0; k < K; k++) {
+        const unsigned m = mt[k * MF_TILE];
+        float f;
+        bool use = m != 0xFFFFu;
+        if constexpr (FMT == 0) {
+            f = ((const float *)(pay_u + k * 64))[hl];
+        } else if constexpr (FMT == 1) {
+            f = __half2float(((const __half *)(pay_u + k * 32))[hl]);
+        } else if constexpr (FMT == 2) {
+            f = (float)((const signed char *)(pay_u + k * 16))[hl];
+        } else {
+            const unsigned h = hd[k];
+            const unsigned char *d = pay + (h >> 2) * 16u;
+            const unsigned fm = h & 3u;
+            if (fm == 0u) f = ((const float *)d)[hl];
+            else if (fm == 1u) f = __half2float(((const __half *)d)[hl]);
+            else f = (float)((const signed char *)d)[hl];
+            use = use && fm != 3u;  // every tile of this slot is bypassed
+        }
+        const unsigned mm = use ? m : 0u;
+        const float xv = fmaf(bt, sv1[mm], sv0[mm]);
+        yf = use ? fmaf(f, xv, yf) : yf;
+    }
+    return yf;
+}
+
+// y = A v over this CTA's staged chunks [cb, ce), v = v0 (NV 1) or
+// bt * v1 + v0 (NV 2); out(s, r, y, xown, has_own) receives every row, xown
+// being the row's own entry of v when its column is staged.  The pipeline,
+// bounded waits, vote and drain are those of spmv_slots; no row reads a
+// vector from global memory.  STV false leaves the values in global memory
+// (a.sval: the FP64 refinement SpMV of the mixed kernel, whose stages are
+// sized for the mixed payload).  Optional thread-0 timers as spmv_slots.
+template <int PK, bool STV, typename VT, int NV, bool MIX, class Out>
+__device__ bool spmv_staged(const CgArgs &a, StagedSmem<MIX> &S, GridCtx &gc, int cb, int ce, const VT *v0,
+                            const VT *v1, VT bt, Out &out, unsigned long long *tph)
+{
+    using C = StagedCfg<MIX>;
+    static_assert(NV * SC_XCAP * (int)sizeof(VT) <= C::VEC_BYTES, "staged vectors must fit the stage");
+    static_assert(STV || PK == 0, "mixed payload is always staged");
+    static_assert(!STV || PK == 1 || !MIX, "FP64 values are staged only in FP64 stages");
+    const bool timed = tph != nullptr && threadIdx.x == 0;
+    unsigned long long tm = timed ? globaltimer_ns() : 0ull;
+#define MF_TSUB(k)                                       \
+    if (timed) {                                         \
+        const unsigned long long nw_ = globaltimer_ns(); \
+        tph[(k)] += nw_ - tm;                            \
+        tm = nw_;                                        \
+    }
+    const MfTiles &A = a.A;
+    const int tid = threadIdx.x, hw = tid >> 4, hl = tid & 15;
+    if (tid == 0) {
+        // the vectors were written earlier in this kernel by ordinary stores
+        // of other CTAs, made visible here by the grid barrier; the proxy
+        // fence orders them before the bulk copies, which read through the
+        // async proxy.  They do not change during the pass.
+        asm volatile("fence.proxy.async.global;\n" ::: "memory");
+        for (int j = 0; j < NSTG && cb + j < ce; j++) issue_staged<PK, STV, VT, NV>(a, S, cb + j, j, v0, v1);
+    }
+    __syncthreads();
+    for (int c = cb; c < ce; c++) {
+        const int k = (c - cb) % NSTG;
+        const bool w = mbar_wait_bounded(&S.bar[k], (gc.par >> (k)) & 1u, a.status, a.budget_ns);
+        gc.par ^= 1u << (k);
+        MF_TSUB(5);
+        const SlotHdr &h = S.hdr[k];
+        const SlotChunk &rec = h.rec;
+        // the header is valid whether or not the data arrived (written before
+        // the copies were issued), so L and the barriers below are uniform
+        const int L = rec.lanes;
+        const int j = L == 1 ? hw : hw / L, part = L == 1 ? 0 : hw % L;
+        const int s = rec.s0 + j;
+        const bool row_ok = w && s < rec.s1 && hl < ((s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE);
+        // FP32 sums stay FP32 until the caller converts them (mixed payload)
+        using YT = typename std::conditional<PK == 0, double, float>::type;
+        YT y = 0;
+        VT xown = 0;
+        bool own = false;
+        if (row_ok) {
+            const unsigned char *st = S.stage[k];
+            const int *ssl = (const int *)(st + C::OFF_SSLOT + h.sh_sslot);
+            const int K = ssl[j + 1] - ssl[j];
+            const int kb = L == 1 ? 0 : K * part / L, ke = L == 1 ? K : K * (part + 1) / L;
+            const int row = s * MF_TILE + hl;
+            int ownpos = -1;
+            for (int q = 0; q < rec.nrun; q++)
+                if (row >= rec.rg[q] && row < rec.rg[q] + rec.rl[q]) ownpos = rec.rs[q] + row - rec.rg[q];
+            const int kA = ssl[j] - rec.k0 + kb;
+            const unsigned short *mt = (const unsigned short *)(st + C::OFF_META + h.sh_meta) + kA * MF_TILE + hl;
+            const VT *sv0 = (const VT *)(st + C::OFF_VEC), *sv1 = sv0 + SC_XCAP;
+            if constexpr (PK == 0) {
+                const double *vd = STV ? (const double *)(st + C::OFF_DATA + h.sh_data) + kA * MF_TILE + hl
+                                       : a.sval + (size_t)(ssl[j] + kb) * MF_TILE + hl;
+                y = staged_row_fp64<NV>(mt, vd, ke - kb, (const double *)sv0, (const double *)sv1, (double)bt);
+            } else {
+                const unsigned *hd = (const unsigned *)(st + C::OFF_DATA + h.sh_data) + kA;
+                const unsigned char *pay = st + C::OFF_PAY + h.sh_pay - rec.y0;
+                const unsigned char *pay0 = st + C::OFF_PAY + h.sh_pay;  // first slot of the chunk
+                const float *f0 = (const float *)sv0, *f1 = (const float *)sv1;
+                const float fb = (float)bt;
+                if (rec.fmt == 0) y = staged_row_mixed<0>(mt, hd, pay, pay0 + kA * 64, ke - kb, hl, f0, f1, fb);
+                else if (rec.fmt == 1) y = staged_row_mixed<1>(mt, hd, pay, pay0 + kA * 32, ke - kb, hl, f0, f1, fb);
+                else if (rec.fmt == 2) y = staged_row_mixed<2>(mt, hd, pay, pay0 + kA * 16, ke - kb, hl, f0, f1, fb);
+                else y = staged_row_mixed<-1>(mt, hd, pay, pay0, ke - kb, hl, f0, f1, fb);
+            }
+            // the row's own entry of v (its column is staged when the chunk
+            // holds its diagonal tile)
+            if (ownpos >= 0) {
+                if constexpr (NV == 2) xown = fma_vt(bt, sv1[ownpos], sv0[ownpos]);
+                else xown = sv0[ownpos];
+                own = true;
+            }
+        }
+        if (L == 1) {
+            if (row_ok) out(s, hl, y, xown, own);
+        } else {
+            // the parts' sums are added in order
+            S.py[tid] = (double)y;
+            S.px[tid] = (double)xown;
+            S.pown[tid] = own ? 1 : 0;
+            __syncthreads();
+            if (row_ok && part == 0) {
+                double yy = 0.0, xo = 0.0;
+                bool ow = false;
+                for (int q = 0; q < L; q++) {
+                    const int t = ((j * L + q) << 4) | hl;
+                    yy = __dadd_rn(yy, S.py[t]);
+                    if (!ow && S.pown[t]) {
+                        ow = true;
+                        xo = S.px[t];
+                    }
+                }
+                out(s, hl, yy, xo, ow);
+            }
+        }
+        MF_TSUB(6);
+        if (!__syncthreads_and(w)) {
+            // chunks c .. c+NSTG-1 may still be landing
+            mbar_drain(&S.bar[k], ((gc.par >> k) & 1u) ^ 1u, a.status, a.budget_ns);
+            for (int jj = 1; jj < NSTG && c + jj < ce; jj++) {
+                const int kj = (c + jj - cb) % NSTG;
+                mbar_drain(&S.bar[kj], (gc.par >> (kj)) & 1u, a.status, a.budget_ns);
+                gc.par ^= 1u << (kj);
+            }
+            __syncthreads();
+            return false;
+        }
+        if (tid == 0 && c + NSTG < ce) issue_staged<PK, STV, VT, NV>(a, S, c + NSTG, k, v0, v1);
+        MF_TSUB(7);
+    }
+#undef MF_TSUB
     return true;
 }
 
@@ -671,7 +974,7 @@ __device__ __forceinline__ bool spmv_any(const CgArgs &a, SM &S, GridCtx &gc, in
     if constexpr (LAY == 0) {
         return spmv_chunks<PK>(a, S, gc, cb, ce, src, out, tph);
     } else {
-        return spmv_slots<PK>(a, S, gc, cb, ce, src, out);
+        return spmv_slots<PK>(a, S, gc, cb, ce, src, out, tph);
     }
 }
 

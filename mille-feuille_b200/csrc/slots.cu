@@ -174,15 +174,60 @@ __global__ void k_slot_pack(MfTiles A, const int *__restrict__ sslot, const unsi
     }
 }
 
+// Sorted union of a staged chunk's tile columns while the walk grows it.
+struct StageUnion {
+    int n, runs;
+    int u[SC_TILES];
+    int tmp[SC_TILES];
+};
+
+// Merges the (sorted) tile columns tcol[a, b) of one strip into U and counts
+// its runs of consecutive tile columns; false, with U unchanged, when the
+// union would exceed SC_TILES tile columns or SC_XCAP columns (both only
+// grow with the chunk; the run count does not: a strip of a 3D stencil has
+// five runs that merge into three once the chunk spans a grid line).
+__device__ bool union_add(StageUnion &U, const int *__restrict__ tcol, int a, int b)
+{
+    int i = 0, j = a, n = 0, runs = 0, prev = -2;
+    while (i < U.n || j < b) {
+        int v;
+        if (j >= b || (i < U.n && U.u[i] <= tcol[j])) {
+            v = U.u[i++];
+            if (j < b && tcol[j] == v) j++;
+        } else {
+            v = tcol[j++];
+        }
+        if (n > 0 && U.tmp[n - 1] == v) continue;
+        if (n >= SC_TILES) return false;
+        if (v != prev + 1) runs++;
+        U.tmp[n++] = v;
+        prev = v;
+    }
+    if (n * MF_TILE > SC_XCAP) return false;
+    for (int k = 0; k < n; k++) U.u[k] = U.tmp[k];
+    U.n = n;
+    U.runs = runs;
+    return true;
+}
+
 // Greedy chunking of one CTA's strips (the same walk counts and fills): a
 // chunk grows while its strips fit the stage and 16 / lanes(max K) half-warp
-// groups.
-__device__ __forceinline__ int slot_walk(int s, int se, const int *sslot, const int *tile_ptr, bool &direct,
-                                         int &lanes)
+// groups and, for staged chunks (U given), while its tile columns fit the
+// staged vectors; it then ends after the longest prefix whose columns form
+// SC_RUNS runs at most, and U is left holding that prefix's union.  A strip
+// that cannot be staged on its own becomes a one-strip chunk with staged =
+// false.
+__device__ int slot_walk(int s, int se, const int *sslot, const int *tile_ptr, const int *tcol, StageUnion *U,
+                         bool &direct, int &lanes, bool &staged)
 {
     const int s0 = s;
-    int kmax = 0;
+    int kmax = 0, best = -1, best_kmax = 0;
     direct = false;
+    staged = U != nullptr;
+    if (U) {
+        U->n = 0;
+        U->runs = 0;
+    }
     while (s < se) {
         const int K = sslot[s + 1] - sslot[s];
         const int km = K > kmax ? K : kmax;
@@ -190,21 +235,45 @@ __device__ __forceinline__ int slot_walk(int s, int se, const int *sslot, const 
         if (s - s0 + 1 > SC_STRIPS / slot_lanes(km) || nk > SC_SLOTS || nt > SC_TILES) {
             if (s == s0) {
                 direct = true;
+                staged = false;
                 kmax = km;
                 s++;
             }
             break;
         }
+        if (U) {
+            if (!union_add(*U, tcol, tile_ptr[s], tile_ptr[s + 1])) break;
+            if (U->runs <= SC_RUNS) {
+                best = s + 1;
+                best_kmax = km;
+            }
+        }
         kmax = km;
         s++;
+    }
+    if (U && !direct) {
+        if (best > s0) {
+            s = best;
+            kmax = best_kmax;
+            // the union of the prefix kept
+            U->n = 0;
+            U->runs = 0;
+            for (int t = s0; t < s; t++) union_add(*U, tcol, tile_ptr[t], tile_ptr[t + 1]);
+        } else {
+            staged = false;
+            s = s0 + 1;
+            kmax = sslot[s0 + 1] - sslot[s0];
+        }
     }
     lanes = direct ? 16 : slot_lanes(kmax);
     return s;
 }
 
 __global__ void k_slot_chunk_count(int G, const int *__restrict__ part, const int *__restrict__ sslot,
-                                   const int *__restrict__ tile_ptr, int *__restrict__ cnt)
+                                   const int *__restrict__ tile_ptr, const int *__restrict__ tcol, int staged,
+                                   int *__restrict__ cnt)
 {
+    StageUnion U;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g <= G; g += gridDim.x * blockDim.x) {
         if (g == G) {
             cnt[g] = 0;
@@ -212,10 +281,10 @@ __global__ void k_slot_chunk_count(int G, const int *__restrict__ part, const in
         }
         int c = 0, s = part[g];
         const int se = part[g + 1];
-        bool d;
+        bool d, st;
         int l;
         while (s < se) {
-            s = slot_walk(s, se, sslot, tile_ptr, d, l);
+            s = slot_walk(s, se, sslot, tile_ptr, tcol, staged ? &U : nullptr, d, l, st);
             c++;
         }
         cnt[g] = c;
@@ -223,16 +292,17 @@ __global__ void k_slot_chunk_count(int G, const int *__restrict__ part, const in
 }
 
 __global__ void k_slot_chunk_fill(int G, const int *__restrict__ part, const int *__restrict__ sslot,
-                                  const int *__restrict__ tile_ptr, const int *__restrict__ off,
-                                  SlotChunk *__restrict__ rec)
+                                  const int *__restrict__ tile_ptr, const int *__restrict__ tcol, int staged,
+                                  const int *__restrict__ off, SlotChunk *__restrict__ rec, int *__restrict__ unstaged)
 {
+    StageUnion U;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
         int c = off[g], s = part[g];
         const int se = part[g + 1];
         while (s < se) {
-            bool d;
+            bool d, st;
             int l;
-            const int s1 = slot_walk(s, se, sslot, tile_ptr, d, l);
+            const int s1 = slot_walk(s, se, sslot, tile_ptr, tcol, staged ? &U : nullptr, d, l, st);
             SlotChunk r;
             r.s0 = s;
             r.s1 = s1;
@@ -243,47 +313,125 @@ __global__ void k_slot_chunk_fill(int G, const int *__restrict__ part, const int
             r.direct = d ? 1 : 0;
             r.lanes = l;
             r.y0 = r.y1 = 0;
+            r.fmt = -1;
+            r.nrun = -1;
+            r.xlen = 0;
+            for (int j = 0; j < SC_RUNS; j++) r.rg[j] = r.rl[j] = r.rs[j] = 0;
+            if (st) {
+                // runs of consecutive tile columns, staged one after another
+                int nr = 0, pos = 0;
+                for (int k = 0; k < U.n; k++) {
+                    if (k == 0 || U.u[k] != U.u[k - 1] + 1) {
+                        r.rg[nr] = U.u[k] * MF_TILE;
+                        r.rs[nr] = (unsigned short)pos;
+                        r.rl[nr] = 0;
+                        nr++;
+                    }
+                    r.rl[nr - 1] = (unsigned short)(r.rl[nr - 1] + MF_TILE);
+                    pos += MF_TILE;
+                }
+                r.nrun = nr;
+                r.xlen = pos;
+            } else if (staged) {
+                atomicAdd(unstaged, 1);
+            }
             rec[c++] = r;
             s = s1;
         }
     }
 }
 
-// Mixed payload byte range of every chunk (after each packing).
+// Staged chunks: each slot entry's position in its chunk's staged vectors
+// (run start + offset of its column in the run); one half-warp per strip.
+__global__ void k_slot_pos(MfTiles A, int nch, const SlotChunk *__restrict__ rec, const int *__restrict__ sslot,
+                           const uint16_t *__restrict__ smeta, uint16_t *__restrict__ spos)
+{
+    const int hl = threadIdx.x & 15;
+    const int nhw = (gridDim.x * blockDim.x) >> 4;
+    // half-warp h takes chunk h / 16 and its strips h % 16, h % 16 + 16, ...
+    for (long long h = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 4; h < (long long)nch * 16; h += nhw) {
+        const SlotChunk &r = rec[h >> 4];
+        for (int s = r.s0 + (int)(h & 15); s < r.s1; s += 16) {
+            const int t0 = A.tile_ptr[s], k0 = sslot[s], K = sslot[s + 1] - k0;
+            for (int k = 0; k < K; k++) {
+                const size_t e = (size_t)(k0 + k) * MF_TILE + hl;
+                const uint16_t m = smeta[e];
+                uint16_t p = 0xFFFFu;
+                if (m != 0xFFFFu && r.nrun >= 0) {
+                    const int c0 = A.tile_columnidx[t0 + (m >> 4)] * MF_TILE;
+                    for (int j = 0; j < r.nrun; j++)
+                        if (c0 >= r.rg[j] && c0 < r.rg[j] + r.rl[j]) p = (uint16_t)(r.rs[j] + (c0 - r.rg[j]) + (m & 15));
+                }
+                spos[e] = p;
+            }
+        }
+    }
+}
+
+// Mixed payload byte range of every chunk (after each packing) and whether
+// all its slots share one stored format.
 __global__ void k_slot_chunk_pay(int nch, const unsigned *__restrict__ shdr, SlotChunk *__restrict__ rec)
 {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nch; c += gridDim.x * blockDim.x) {
-        rec[c].y0 = (long long)(shdr[rec[c].k0] >> 2) * 16;
-        rec[c].y1 = (long long)(shdr[rec[c].k1] >> 2) * 16;
+        const int k0 = rec[c].k0, k1 = rec[c].k1;
+        rec[c].y0 = (long long)(shdr[k0] >> 2) * 16;
+        rec[c].y1 = (long long)(shdr[k1] >> 2) * 16;
+        int f = k1 > k0 ? (int)(shdr[k0] & 3u) : -1;
+        for (int k = k0 + 1; k < k1 && f >= 0; k++)
+            if ((int)(shdr[k] & 3u) != f) f = -1;
+        rec[c].fmt = f == 3 ? -1 : f;
     }
 }
 
 }  // namespace
 
-mf_status build_slot_chunks(mf_matrix m, int G, cudaStream_t s)
+mf_status build_slot_chunks(mf_matrix m, int G, bool staged, cudaStream_t s)
 {
-    if (m->schunk_ctas == G && m->d_schunks) return MF_OK;
+    const int mode = staged ? 2 : 1;
+    if (m->schunk_ctas == G && m->d_schunks && m->schunk_mode == mode) return MF_OK;
     if (m->d_scta_chunk) cudaFree(m->d_scta_chunk);
     if (m->d_schunks) cudaFree(m->d_schunks);
     m->d_scta_chunk = nullptr;
     m->d_schunks = nullptr;
     m->schunk_ctas = 0;
+    m->schunk_mode = 0;
+    m->schunk_staged = 0;
     MF_CUDA(cudaMalloc(&m->d_scta_chunk, sizeof(int) * (G + 1)));
     int *cnt = nullptr;
-    MF_CUDA(pool_malloc_async(&cnt, sizeof(int) * (G + 1), s));
-    k_slot_chunk_count<<<grid_for3(G + 1, 128), 128, 0, s>>>(G, m->d_part, m->d_sslot, m->d_tile_ptr, cnt);
+    MF_CUDA(pool_malloc_async(&cnt, sizeof(int) * (G + 2), s));
+    int *unstaged = cnt + G + 1;
+    MF_CUDA(cudaMemsetAsync(unstaged, 0, sizeof(int), s));
+    const int *tcol = m->v.tile_columnidx;
+    k_slot_chunk_count<<<grid_for3(G + 1, 128), 128, 0, s>>>(G, m->d_part, m->d_sslot, m->d_tile_ptr, tcol,
+                                                             staged ? 1 : 0, cnt);
     note_launch();
     MF_CUDA(cudaGetLastError());
     int total = 0;
     MF_TRY(exclusive_scan_i32(cnt, m->d_scta_chunk, G + 1, s, &total));
-    cudaFreeAsync(cnt, s);
     MF_CUDA(cudaMalloc(&m->d_schunks, sizeof(SlotChunk) * (size_t)(total > 0 ? total : 1)));
-    k_slot_chunk_fill<<<grid_for3(G, 128), 128, 0, s>>>(G, m->d_part, m->d_sslot, m->d_tile_ptr, m->d_scta_chunk,
-                                                        (SlotChunk *)m->d_schunks);
+    k_slot_chunk_fill<<<grid_for3(G, 128), 128, 0, s>>>(G, m->d_part, m->d_sslot, m->d_tile_ptr, tcol,
+                                                        staged ? 1 : 0, m->d_scta_chunk, (SlotChunk *)m->d_schunks,
+                                                        unstaged);
     note_launch();
     MF_CUDA(cudaGetLastError());
+    int h_unstaged = 0;
+    MF_CUDA(cudaMemcpyAsync(&h_unstaged, unstaged, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MF_CUDA(cudaStreamSynchronize(s));
+    cudaFreeAsync(cnt, s);
     m->nschunks = total;
     m->schunk_ctas = G;
+    m->schunk_mode = mode;
+    m->schunk_unstaged = h_unstaged;
+    if (staged && !h_unstaged) {
+        if (!m->d_spos) MF_CUDA(cudaMalloc(&m->d_spos, sizeof(uint16_t) * (size_t)m->nslots * MF_TILE + 32));
+        if (total > 0) {
+            k_slot_pos<<<grid_for3((long long)total * 16 * MF_TILE, 256), 256, 0, s>>>(
+                m->v, total, (const SlotChunk *)m->d_schunks, m->d_sslot, m->d_smeta, m->d_spos);
+            note_launch();
+            MF_CUDA(cudaGetLastError());
+        }
+        m->schunk_staged = 1;
+    }
     if (m->d_shdr && m->slot_policy >= 0) {  // payload ranges of an existing packing
         k_slot_chunk_pay<<<grid_for3(total, 256), 256, 0, s>>>(total, m->d_shdr, (SlotChunk *)m->d_schunks);
         note_launch();

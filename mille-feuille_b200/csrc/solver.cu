@@ -1,6 +1,7 @@
 // solver.cu -- host orchestration of the persistent CG solves (policies,
 // checkpoints, reports).
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -15,18 +16,54 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
                                   const TraceHook *hook = nullptr)
 {
     const bool mixed = o.policy != MF_POLICY_FP64;
-    // execution layout: row slots unless disabled or not describable
+    // FP64 CG without checkpoints on small, short-row systems (latency-bound:
+    // the grid-wide waits dominate): one reduction per iteration.  Larger or
+    // long-row systems keep the two-reduction kernel, whose SpMV gathers two
+    // vectors instead of three.  MF_CG_VARIANT=1 / 2 forces either.
+    bool one_reduction;
+    {
+        const char *v = getenv("MF_CG_VARIANT");
+        const bool small = m->v.rows <= (1 << 19) && (long long)m->v.nnz <= 16LL * m->v.rows;
+        const int force = v ? atoi(v) : 0;
+        const bool want = force == 1 || (force != 2 && small);
+        one_reduction = !bicg && !mixed && !hook && want;
+    }
+    // execution layout: staged row slots for the mixed-precision
+    // two-reduction CG kernel, plain row slots otherwise or when a chunk
+    // cannot be staged, tile chunks when the slots cannot describe the
+    // matrix.  (The FP64 kernel stages two FP64 vectors, which leaves room
+    // for two CTAs per SM only; its plain row slots run faster.)
+    // MF_SOLVER_LAYOUT=tiles / slots restricts the choice, =staged also
+    // stages the FP64 kernel.
     const char *lay = getenv("MF_SOLVER_LAYOUT");
     const bool want_slots = !(lay && !strcmp(lay, "tiles"));
     if (want_slots) MF_TRY(build_slots(m, s));
     const bool slots = want_slots && m->slots_state == 1;
-    const int G = bicg ? bicgstab_grid(m, mixed, slots) : solver_grid(m, mixed, slots);
-    if (m->part_ctas != G || (!slots && !m->d_chunks)) {
-        MF_TRY(strip_partition(m, G, s));
-        if (!slots) MF_TRY(build_chunks(m, s));
-        m->packed_policy = -1;  // chunk payload offsets must be refreshed
+    const bool force_staged = lay && !strcmp(lay, "staged");
+    bool staged = slots && !bicg && !one_reduction && (mixed || force_staged) &&
+                  !(lay && !strcmp(lay, "slots")) && (long long)m->v.tilen <= (long long)m->v.tilem;
+    auto layout_grid = [&](bool st) {
+        return bicg ? bicgstab_grid(m, mixed, slots) : solver_grid(m, mixed, st ? 2 : slots ? 1 : 0);
+    };
+    int G = layout_grid(staged);
+    auto prepare = [&]() -> mf_status {
+        if (m->part_ctas != G || (!slots && !m->d_chunks)) {
+            MF_TRY(strip_partition(m, G, s));
+            if (!slots) MF_TRY(build_chunks(m, s));
+            m->packed_policy = -1;  // chunk payload offsets must be refreshed
+        }
+        if (slots) MF_TRY(build_slot_chunks(m, G, staged, s));
+        return MF_OK;
+    };
+    MF_TRY(prepare());
+    if (getenv("MF_LAYOUT_DEBUG"))
+        fprintf(stderr, "mf: layout %s, grid %d, %d chunks, %d not stageable\n",
+                staged ? "staged" : slots ? "slots" : "tiles", G, m->nschunks, m->schunk_unstaged);
+    if (staged && !m->schunk_staged) {  // some chunk's columns do not fit: plain slots
+        staged = false;
+        G = layout_grid(false);
+        MF_TRY(prepare());
     }
-    if (slots) MF_TRY(build_slot_chunks(m, G, s));
     SolverWork w;
     MF_TRY(solver_resources(m, G, w));
     const int T = m->v.tilenum;
@@ -66,6 +103,10 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
         a.spay = m->d_spay;
         a.scta_chunk = m->d_scta_chunk;
         a.schunks = (const SlotChunk *)m->d_schunks;
+        if (staged) {
+            a.spos = m->d_spos;
+            a.xs = (double *)w.t;  // padded to whole strips (tile columns of a square tile grid)
+        }
     }
     a.pay = m->d_pay;
     a.poff = m->d_poff;
@@ -93,17 +134,7 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
     // checkpoints (policy updates between launches) for CG's dynamic policies
     a.exit_on_refine = (!bicg && mixed && o.policy != MF_POLICY_STATIC) ? 1 : 0;
     a.checkpoint_every = (hook && !bicg) ? hook->every : 0;
-    // FP64 CG without checkpoints on small, short-row systems (latency-bound:
-    // the grid-wide waits dominate): one reduction per iteration.  Larger or
-    // long-row systems keep the two-reduction kernel, whose SpMV gathers two
-    // vectors instead of three.  MF_CG_VARIANT=1 / 2 forces either.
-    {
-        const char *v = getenv("MF_CG_VARIANT");
-        const bool small = m->v.rows <= (1 << 19) && (long long)m->v.nnz <= 16LL * m->v.rows;
-        const int force = v ? atoi(v) : 0;
-        const bool want = force == 1 || (force != 2 && small);
-        a.one_reduction = (!bicg && !mixed && a.checkpoint_every == 0 && want) ? 1 : 0;
-    }
+    a.one_reduction = (one_reduction && a.checkpoint_every == 0) ? 1 : 0;
     a.budget_ns = (unsigned long long)(o.wait_budget_s * 1e9);
     a.start = 1;
     a.timing = o.phase_times ? w.timing : nullptr;
@@ -154,6 +185,7 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
     rep.iterations = (int)st[S_ITERS];
     rep.refinements = (int)st[S_REFS];
     rep.grid_ctas = G;
+    rep.layout = staged ? 2 : slots ? 1 : 0;
     rep.kernel_ms = ms;
     rep.relres = st[S_RELRES];
     const long long n = m->v.rows, nnz = m->v.nnz;

@@ -30,14 +30,29 @@ struct ChunkRec {
 // slots, and the parts' sums are added in order.  A strip too large for a
 // stage on its own is a one-strip chunk with `direct` set (16 half-warps,
 // read from global memory).
+//
+// Staged chunks (the CG kernels' default when every chunk qualifies): the
+// chunk's tile columns form at most SC_RUNS runs of consecutive tile
+// columns holding SC_XCAP columns at most; the runs of the vectors the SpMV
+// reads are copied into shared memory next to the slots, and the slot words
+// are positions in that staged copy (spos), so no row reads a vector from
+// global memory.
 constexpr int SC_STRIPS = CH_STRIPS, SC_SLOTS = 8 * SC_STRIPS, SC_TILES = 16 * SC_STRIPS;
+constexpr int SC_RUNS = 6, SC_XCAP = 1280;
 struct SlotChunk {
     int s0, s1;            // strips [s0, s1)
     int k0, k1;            // slots [k0, k1)
     int t0, t1;            // tiles [t0, t1)
     int direct, lanes;
     long long y0, y1;      // mixed payload bytes [y0, y1)
+    int fmt;               // mixed payload: 0 / 1 / 2 every slot fp32 / fp16 / int8, -1 otherwise
+    int nrun;              // staged: column runs (-1: the chunk cannot be staged)
+    int xlen;              // staged: columns staged (multiple of 16)
+    int rg[SC_RUNS];                 // staged: first column of each run (multiple of 16)
+    unsigned short rl[SC_RUNS];      // staged: columns of each run (multiple of 16)
+    unsigned short rs[SC_RUNS];      // staged: position of each run in the staged vectors
 };
+static_assert(SC_XCAP < 65536, "staged run lengths and positions are 16-bit");
 
 // Half-warps per strip for a strip of K slots: about 8 slots each.
 __host__ __device__ __forceinline__ int slot_lanes(int K)
@@ -87,6 +102,9 @@ struct CgArgs {
     const int *scta_chunk;         // [G+1] slot-chunk range of each CTA
     const SlotChunk *schunks;
     int one_reduction;             // FP64: the single-reduction CG kernel (k_cg1)
+    // staged slot chunks (null otherwise)
+    const uint16_t *spos;          // [slots*16] position in the chunk's staged vectors (0xFFFF empty)
+    double *xs;                    // padded FP64 copy of x that the refinement SpMV stages
 };
 
 struct SolverWork {
@@ -113,14 +131,16 @@ mf_status cg_solve_traced(mf_matrix m, const double *b, double *x, const mf_solv
 // chunks.cu: chunk table for the current partition; payload offsets refresh
 mf_status build_chunks(mf_matrix m, cudaStream_t s);
 mf_status refresh_chunk_payload(mf_matrix m, cudaStream_t s);
-int solver_grid(mf_matrix m, bool mixed, bool slots);
+int solver_grid(mf_matrix m, bool mixed, int layout);  // layout: 0 tiles, 1 slots, 2 staged slots
 mf_status launch_cg(bool mixed, CgArgs &a, int G, cudaStream_t s);
 mf_status launch_bicgstab(bool mixed, CgArgs &a, int G, cudaStream_t s);
 int bicgstab_grid(mf_matrix m, bool mixed, bool slots);
 // slots.cu: the row-slot layout (built once; state -1 = not describable)
 mf_status build_slots(mf_matrix m, cudaStream_t s);
 mf_status pack_slots(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s);
-mf_status build_slot_chunks(mf_matrix m, int G, cudaStream_t s);
+// staged = true builds staged chunks and the positions; m->schunk_staged
+// tells whether every chunk qualified (otherwise the chunks are plain)
+mf_status build_slot_chunks(mf_matrix m, int G, bool staged, cudaStream_t s);
 mf_status true_residual(mf_matrix m, const double *b, const double *x, SolverWork &w, double *relres, cudaStream_t s);
 // payload.cu
 mf_status pack_payload(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s);

@@ -169,7 +169,7 @@ mf_status mf_matrix_destroy(mf_matrix m)
                     m->d_tile_rowidx, m->d_block_signal, m->d_blockrowid_new, m->d_blockcsr_ptr_new, m->d_rbb_rowidx,
                     m->d_rbb_colstart, m->d_rbb_colstop, m->d_part, m->d_cta_chunk, m->d_chunks, m->work, m->host_io,
                     m->d_wcls, m->d_poff, m->d_pay, m->d_resid, m->d_pol, m->d_sslot, m->d_smeta, m->d_sval,
-                    m->d_shdr, m->d_spay, m->d_scta_chunk, m->d_schunks, m->d_spos};
+                    m->d_shdr, m->d_spay, m->d_scta_chunk, m->d_schunks, m->d_spos, m->d_sdesc};
     for (void *p : bufs)
         if (p) cudaFree(p);
     delete m;

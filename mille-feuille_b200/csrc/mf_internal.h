@@ -87,6 +87,7 @@ struct mf_matrix_s {
     int schunk_staged = 0;         // 1: staged chunks, every one qualified
     int schunk_unstaged = 0;       // staged build: chunks that did not qualify
     uint16_t *d_spos = nullptr;    // staged positions of the slot entries
+    int2 *d_sdesc = nullptr;       // staged strip descriptors
     // per-strip partials of mf_residual_norm
     double *d_resid = nullptr;
     size_t resid_bytes = 0;

@@ -5,6 +5,7 @@
 #pragma once
 #include <cuda_fp16.h>
 
+#include <climits>
 #include <cstdlib>
 #include <type_traits>
 
@@ -680,15 +681,15 @@ __device__ bool spmv_slots(const CgArgs &a, SlotSmem &S, GridCtx &gc, int cb, in
 
 // ---- staged slot chunks ----
 //
-// Stage layout: strip slot offsets, slot positions, FP64 values or the mixed
+// Stage layout: strip descriptors, slot positions, FP64 values or the mixed
 // slot headers and payload, then the staged vectors (the chunk's column runs
 // of one FP64 vector or of two vectors of the solver's type, one after the
 // other, SC_XCAP elements apart).  Every region is 16-byte aligned and sized
 // for the largest 16-byte-rounded range it receives.
 template <bool MIX>
 struct StagedCfg {
-    static constexpr int OFF_SSLOT = 0;
-    static constexpr int OFF_META = SOFF_TPTR;
+    static constexpr int OFF_SDESC = 0;  // strip descriptors (8 bytes each)
+    static constexpr int OFF_META = (SC_STRIPS * 8 + 32 + 15) / 16 * 16;
     static constexpr int OFF_DATA = OFF_META + SC_SLOTS * MF_TILE * 2 + 32;
     static constexpr int OFF_PAY = OFF_DATA + SC_SLOTS * 4 + 32;
     static constexpr int OFF_VEC = MIX ? OFF_PAY + SC_SLOTS * 64 + 32 : OFF_DATA + SC_SLOTS * MF_TILE * 8 + 32;
@@ -727,7 +728,7 @@ __device__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S, int c, int k, 
     const SlotChunk &r = h.rec;  // read in place (shared memory), not copied to local memory
     unsigned char *st = S.stage[k];
     const long long m0 = 2ll * MF_TILE * r.k0, m1 = 2ll * MF_TILE * r.k1;
-    unsigned total = range_bytes(4ll * r.s0, 4ll * (r.s1 + 1)) + range_bytes(m0, m1);
+    unsigned total = range_bytes(8ll * r.s0, 8ll * r.s1) + range_bytes(m0, m1);
     if (STV) {
         if (PK == 0) total += range_bytes(8ll * MF_TILE * r.k0, 8ll * MF_TILE * r.k1);
         else total += range_bytes(4ll * r.k0, 4ll * (r.k1 + 1)) + range_bytes(r.y0, r.y1);
@@ -735,8 +736,7 @@ __device__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S, int c, int k, 
     for (int j = 0; j < r.nrun; j++) total += (unsigned)(NV * r.rl[j] * (int)sizeof(VT));
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(&S.bar[k], total);
-    add_range(st + C::OFF_SSLOT, (const unsigned char *)a.sslot, 4ll * r.s0, 4ll * (r.s1 + 1), &S.bar[k],
-              h.sh_sslot);
+    add_range(st + C::OFF_SDESC, (const unsigned char *)a.sdesc, 8ll * r.s0, 8ll * r.s1, &S.bar[k], h.sh_sslot);
     add_range(st + C::OFF_META, (const unsigned char *)a.spos, m0, m1, &S.bar[k], h.sh_meta);
     if (STV) {
         if (PK == 0) {
@@ -762,7 +762,7 @@ __device__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S, int c, int k, 
 // where the tile column does, so the FP64 per-tile partial sums are those of
 // blockspmv_cpu).  vd may point to shared or global memory.
 #ifndef MF_STAGED_UNROLL
-#define MF_STAGED_UNROLL 2
+#define MF_STAGED_UNROLL 4
 #endif
 constexpr int STAGED_UNROLL = MF_STAGED_UNROLL;
 
@@ -839,11 +839,21 @@ __device__ __forceinline__ float staged_row_mixed(const unsigned short *mt, cons
 
 // y = A v over this CTA's staged chunks [cb, ce), v = v0 (NV 1) or
 // bt * v1 + v0 (NV 2); out(s, r, y, xown, has_own) receives every row, xown
-// being the row's own entry of v when its column is staged.  The pipeline,
-// bounded waits, vote and drain are those of spmv_slots; no row reads a
+// being the row's own entry of v when its column is staged.  No row reads a
 // vector from global memory.  STV false leaves the values in global memory
 // (a.sval: the FP64 refinement SpMV of the mixed kernel, whose stages are
-// sized for the mixed payload).  Optional thread-0 timers as spmv_slots.
+// sized for the mixed payload).
+//
+// Only thread 0 waits on the stage barriers: after computing chunk c it
+// waits (bounded) for chunk c+1, and the CTA barrier that closes chunk c
+// hands the result to every thread, which then reads chunk c+1's stage (the
+// copies' writes, observed by thread 0 through the mbarrier, are ordered
+// before the other threads' reads by that barrier).  One CTA barrier per
+// chunk, and no warp sleeps in an mbarrier wait.  The barrier votes: when a
+// wait expired, the copies still in flight are drained (bounded, at least
+// one second) before the CTA leaves, so none lands in freed shared memory.
+// Optional thread-0 timers: [5] waiting for the next chunk, [6] computing
+// rows, [7] the closing barrier and the refill.
 template <int PK, bool STV, typename VT, int NV, bool MIX, class Out>
 __device__ bool spmv_staged(const CgArgs &a, StagedSmem<MIX> &S, GridCtx &gc, int cb, int ce, const VT *v0,
                             const VT *v1, VT bt, Out &out, unsigned long long *tph)
@@ -870,20 +880,33 @@ __device__ bool spmv_staged(const CgArgs &a, StagedSmem<MIX> &S, GridCtx &gc, in
         asm volatile("fence.proxy.async.global;\n" ::: "memory");
         for (int j = 0; j < NSTG && cb + j < ce; j++) issue_staged<PK, STV, VT, NV>(a, S, cb + j, j, v0, v1);
     }
-    __syncthreads();
+    // copies of chunks [c0, c0 + n) may be in flight: wait for them
+    // (bounded) before leaving, each with the parity its stage expects
+    auto drain = [&](int c0, int n) {
+        for (int jj = 0; jj < n && c0 + jj < ce; jj++) {
+            const int kj = (c0 + jj - cb) % NSTG;
+            if (tid == 0) mbar_drain(&S.bar[kj], (gc.par >> kj) & 1u, a.status, a.budget_ns);
+            gc.par ^= 1u << kj;
+        }
+        __syncthreads();
+    };
+    {
+        bool w0 = true;
+        if (tid == 0 && cb < ce) w0 = mbar_wait_bounded(&S.bar[0], gc.par & 1u, a.status, a.budget_ns);
+        if (!__syncthreads_and(w0)) {
+            drain(cb, NSTG);  // the chunks issued so far
+            return false;
+        }
+        if (cb < ce) gc.par ^= 1u;
+    }
     for (int c = cb; c < ce; c++) {
         const int k = (c - cb) % NSTG;
-        const bool w = mbar_wait_bounded(&S.bar[k], (gc.par >> (k)) & 1u, a.status, a.budget_ns);
-        gc.par ^= 1u << (k);
-        MF_TSUB(5);
         const SlotHdr &h = S.hdr[k];
         const SlotChunk &rec = h.rec;
-        // the header is valid whether or not the data arrived (written before
-        // the copies were issued), so L and the barriers below are uniform
         const int L = rec.lanes;
         const int j = L == 1 ? hw : hw / L, part = L == 1 ? 0 : hw % L;
         const int s = rec.s0 + j;
-        const bool row_ok = w && s < rec.s1 && hl < ((s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE);
+        const bool row_ok = s < rec.s1 && hl < ((s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE);
         // FP32 sums stay FP32 until the caller converts them (mixed payload)
         using YT = typename std::conditional<PK == 0, double, float>::type;
         YT y = 0;
@@ -891,19 +914,19 @@ __device__ bool spmv_staged(const CgArgs &a, StagedSmem<MIX> &S, GridCtx &gc, in
         bool own = false;
         if (row_ok) {
             const unsigned char *st = S.stage[k];
-            const int *ssl = (const int *)(st + C::OFF_SSLOT + h.sh_sslot);
-            const int K = ssl[j + 1] - ssl[j];
+            // one load: the strip's first slot in the chunk, its slot count
+            // and the offset from a row to its own staged position
+            const int2 dsc = ((const int2 *)(st + C::OFF_SDESC + h.sh_sslot))[j];
+            const int K = dsc.x >> 16;
             const int kb = L == 1 ? 0 : K * part / L, ke = L == 1 ? K : K * (part + 1) / L;
             const int row = s * MF_TILE + hl;
-            int ownpos = -1;
-            for (int q = 0; q < rec.nrun; q++)
-                if (row >= rec.rg[q] && row < rec.rg[q] + rec.rl[q]) ownpos = rec.rs[q] + row - rec.rg[q];
-            const int kA = ssl[j] - rec.k0 + kb;
+            const int ownpos = dsc.y == INT_MIN ? -1 : row + dsc.y;
+            const int kA = (dsc.x & 0xFFFF) + kb;
             const unsigned short *mt = (const unsigned short *)(st + C::OFF_META + h.sh_meta) + kA * MF_TILE + hl;
             const VT *sv0 = (const VT *)(st + C::OFF_VEC), *sv1 = sv0 + SC_XCAP;
             if constexpr (PK == 0) {
                 const double *vd = STV ? (const double *)(st + C::OFF_DATA + h.sh_data) + kA * MF_TILE + hl
-                                       : a.sval + (size_t)(ssl[j] + kb) * MF_TILE + hl;
+                                       : a.sval + (size_t)(rec.k0 + kA) * MF_TILE + hl;
                 y = staged_row_fp64<NV>(mt, vd, ke - kb, (const double *)sv0, (const double *)sv1, (double)bt);
             } else {
                 const unsigned *hd = (const unsigned *)(st + C::OFF_DATA + h.sh_data) + kA;
@@ -947,17 +970,16 @@ __device__ bool spmv_staged(const CgArgs &a, StagedSmem<MIX> &S, GridCtx &gc, in
             }
         }
         MF_TSUB(6);
-        if (!__syncthreads_and(w)) {
-            // chunks c .. c+NSTG-1 may still be landing
-            mbar_drain(&S.bar[k], ((gc.par >> k) & 1u) ^ 1u, a.status, a.budget_ns);
-            for (int jj = 1; jj < NSTG && c + jj < ce; jj++) {
-                const int kj = (c + jj - cb) % NSTG;
-                mbar_drain(&S.bar[kj], (gc.par >> (kj)) & 1u, a.status, a.budget_ns);
-                gc.par ^= 1u << (kj);
-            }
-            __syncthreads();
+        const int kn = (c + 1 - cb) % NSTG;
+        bool wn = true;
+        if (tid == 0 && c + 1 < ce) wn = mbar_wait_bounded(&S.bar[kn], (gc.par >> kn) & 1u, a.status, a.budget_ns);
+        MF_TSUB(5);
+        if (!__syncthreads_and(wn)) {
+            drain(c + 1, NSTG - 1);  // chunks c+1 .. c+NSTG-1 (c+NSTG is not issued yet)
             return false;
         }
+        if (c + 1 < ce) gc.par ^= 1u << kn;
+        // every thread is done with stage k
         if (tid == 0 && c + NSTG < ce) issue_staged<PK, STV, VT, NV>(a, S, c + NSTG, k, v0, v1);
         MF_TSUB(7);
     }

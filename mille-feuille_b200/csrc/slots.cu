@@ -26,6 +26,8 @@
 // a matrix with one keeps the chunked tile path.
 #include <cuda_fp16.h>
 
+#include <climits>
+
 #include "solver.h"
 
 namespace mf {
@@ -342,9 +344,12 @@ __global__ void k_slot_chunk_fill(int G, const int *__restrict__ part, const int
 }
 
 // Staged chunks: each slot entry's position in its chunk's staged vectors
-// (run start + offset of its column in the run); one half-warp per strip.
+// (run start + offset of its column in the run), and each strip's
+// descriptor (first slot within the chunk | slots << 16; the offset from a
+// row to its own staged position, INT_MIN when the strip's diagonal tile
+// column is not staged); one half-warp per strip.
 __global__ void k_slot_pos(MfTiles A, int nch, const SlotChunk *__restrict__ rec, const int *__restrict__ sslot,
-                           const uint16_t *__restrict__ smeta, uint16_t *__restrict__ spos)
+                           const uint16_t *__restrict__ smeta, uint16_t *__restrict__ spos, int2 *__restrict__ sdesc)
 {
     const int hl = threadIdx.x & 15;
     const int nhw = (gridDim.x * blockDim.x) >> 4;
@@ -353,6 +358,12 @@ __global__ void k_slot_pos(MfTiles A, int nch, const SlotChunk *__restrict__ rec
         const SlotChunk &r = rec[h >> 4];
         for (int s = r.s0 + (int)(h & 15); s < r.s1; s += 16) {
             const int t0 = A.tile_ptr[s], k0 = sslot[s], K = sslot[s + 1] - k0;
+            if (hl == 0) {
+                int od = INT_MIN;
+                for (int j = 0; j < r.nrun; j++)
+                    if (s * MF_TILE >= r.rg[j] && s * MF_TILE < r.rg[j] + r.rl[j]) od = r.rs[j] - r.rg[j];
+                sdesc[s] = make_int2((k0 - r.k0) | (K << 16), od);
+            }
             for (int k = 0; k < K; k++) {
                 const size_t e = (size_t)(k0 + k) * MF_TILE + hl;
                 const uint16_t m = smeta[e];
@@ -424,9 +435,10 @@ mf_status build_slot_chunks(mf_matrix m, int G, bool staged, cudaStream_t s)
     m->schunk_unstaged = h_unstaged;
     if (staged && !h_unstaged) {
         if (!m->d_spos) MF_CUDA(cudaMalloc(&m->d_spos, sizeof(uint16_t) * (size_t)m->nslots * MF_TILE + 32));
+        if (!m->d_sdesc) MF_CUDA(cudaMalloc(&m->d_sdesc, sizeof(int2) * ((size_t)m->v.tilem + 2)));
         if (total > 0) {
             k_slot_pos<<<grid_for3((long long)total * 16 * MF_TILE, 256), 256, 0, s>>>(
-                m->v, total, (const SlotChunk *)m->d_schunks, m->d_sslot, m->d_smeta, m->d_spos);
+                m->v, total, (const SlotChunk *)m->d_schunks, m->d_sslot, m->d_smeta, m->d_spos, m->d_sdesc);
             note_launch();
             MF_CUDA(cudaGetLastError());
         }

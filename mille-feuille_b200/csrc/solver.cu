@@ -105,6 +105,7 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
         a.schunks = (const SlotChunk *)m->d_schunks;
         if (staged) {
             a.spos = m->d_spos;
+            a.sdesc = m->d_sdesc;
             a.xs = (double *)w.t;  // padded to whole strips (tile columns of a square tile grid)
         }
     }

@@ -104,6 +104,8 @@ struct CgArgs {
     int one_reduction;             // FP64: the single-reduction CG kernel (k_cg1)
     // staged slot chunks (null otherwise)
     const uint16_t *spos;          // [slots*16] position in the chunk's staged vectors (0xFFFF empty)
+    const int2 *sdesc;             // [tilem] per strip: first slot within its chunk | slots << 16, and
+                                   // the offset from a row to its own staged position (INT_MIN: none)
     double *xs;                    // padded FP64 copy of x that the refinement SpMV stages
 };
 

@@ -15,7 +15,10 @@
 // p and v are double-buffered so no pass has to finish writing them before
 // the next SpMV starts.  Mixed precision follows the CG solver: packed
 // per-tile classes, FP32 vectors and accumulation, FP64 dot products and
-// FP64 reliable updates of the residual.
+// FP64 reliable updates of the residual.  On staged chunks (LAY 2, mixed)
+// each SpMV copies two vectors into shared memory: the update pass, which
+// knows omega, stores w = p - omega v (one rounding, as the on-the-fly form)
+// over p, so the next p = r + beta w needs r and w only.
 #include <algorithm>
 #include <type_traits>
 
@@ -42,11 +45,22 @@ __device__ __forceinline__ void grid_sum2(const CgArgs &a, double l0, double l1,
     o1 = block_sum_partials<NT>(a.partials + (slot + 1) * G, G, S.warp);
 }
 
+#ifndef MF_STAGED_MINB_BICG
+#define MF_STAGED_MINB_BICG 4
+#endif
+
 template <bool MIX, int LAY>
-__global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_bicgstab(CgArgs a)
+struct BicgSmem {
+    using type = typename std::conditional<
+        LAY == 0, SolverSmem, typename std::conditional<LAY == 1, SlotSmem, StagedSmem<MIX>>::type>::type;
+};
+
+template <bool MIX, int LAY>
+__global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : MF_STAGED_MINB_BICG) k_bicgstab(CgArgs a)
 {
     using VT = typename VecT<MIX>::T;
-    using SM = typename std::conditional<LAY == 0, SolverSmem, SlotSmem>::type;
+    using SM = typename BicgSmem<MIX, LAY>::type;
+    static_assert(LAY != 2 || MIX, "staged BiCGSTAB is the mixed kernel");
     constexpr int PK = MIX ? 1 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SM &S = *reinterpret_cast<SM *>(smem_raw);
@@ -68,7 +82,8 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_bicgstab(CgArgs
     if constexpr (LAY == 0) {
         for (int c = cb + threadIdx.x; c < ce && c - cb < RECS; c += NT) S.recs[c - cb] = a.chunks[c];
     } else {
-        for (int c = cb + threadIdx.x; c < ce && c - cb < SRECS; c += NT) S.recs[c - cb] = a.schunks[c];
+        constexpr int NREC = LAY == 1 ? SRECS : TRECS;
+        for (int c = cb + threadIdx.x; c < ce && c - cb < NREC; c += NT) S.recs[c - cb] = a.schunks[c];
     }
     __syncthreads();
 
@@ -129,12 +144,14 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_bicgstab(CgArgs
         const VT bt = (VT)beta, om = (VT)omega;
         const VT *rr = r;
         // ---- v = A p, p = r + beta (p_old - omega v_old) ----
+        // (staged: p_old already holds w = p_old - omega v_old)
         auto psrc = [=](int c) -> VT {
-            if constexpr (MIX) return fmaf(bt, fmaf(-om, vold[c], pold[c]), rr[c]);
+            if constexpr (LAY == 2) return fmaf(bt, pold[c], rr[c]);
+            else if constexpr (MIX) return fmaf(bt, fmaf(-om, vold[c], pold[c]), rr[c]);
             else return fma(bt, fma(-om, vold[c], pold[c]), rr[c]);
         };
         double loc = 0.0;
-        auto aout = [&](int s, int rw, double y, double xown, bool has_own) {
+        auto aout = [&](int s, int rw, auto y, auto xown, bool has_own) {
             const int i = s * MF_TILE + rw;
             const VT pn = has_own ? (VT)xown : psrc(i);
             const VT vi = (VT)y;
@@ -142,7 +159,11 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_bicgstab(CgArgs
             vnew[i] = vi;
             loc = __dadd_rn(loc, __dmul_rn((double)rh[i], (double)vi));
         };
-        if (!spmv_any<PK, LAY>(a, S, gc, cb, ce, sb0, se0, psrc, aout, nullptr)) gc.ok = false;
+        if constexpr (LAY == 2) {
+            if (!spmv_staged<PK, true, VT, 2>(a, S, gc, cb, ce, rr, pold, bt, aout, nullptr)) gc.ok = false;
+        } else {
+            if (!spmv_any<PK, LAY>(a, S, gc, cb, ce, sb0, se0, psrc, aout, nullptr)) gc.ok = false;
+        }
         double rv, dummy;
         grid_sum2(a, loc, 0.0, 2, gc, S, rv, dummy);
         if (!gc.ok) break;
@@ -160,7 +181,7 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_bicgstab(CgArgs
             else return fma(-al, vn[c], rr[c]);
         };
         double lts = 0.0, ltt = 0.0;
-        auto tout = [&](int s, int rw, double y, double xown, bool has_own) {
+        auto tout = [&](int s, int rw, auto y, auto xown, bool has_own) {
             const int i = s * MF_TILE + rw;
             const VT si = has_own ? (VT)xown : ssrc(i);
             const VT ti = (VT)y;
@@ -168,7 +189,11 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_bicgstab(CgArgs
             lts = __dadd_rn(lts, __dmul_rn((double)ti, (double)si));
             ltt = __dadd_rn(ltt, __dmul_rn((double)ti, (double)ti));
         };
-        if (!spmv_any<PK, LAY>(a, S, gc, cb, ce, sb0, se0, ssrc, tout, nullptr)) gc.ok = false;
+        if constexpr (LAY == 2) {
+            if (!spmv_staged<PK, true, VT, 2>(a, S, gc, cb, ce, rr, vn, (VT)-al, tout, nullptr)) gc.ok = false;
+        } else {
+            if (!spmv_any<PK, LAY>(a, S, gc, cb, ce, sb0, se0, ssrc, tout, nullptr)) gc.ok = false;
+        }
         double ts, tt;
         grid_sum2(a, lts, ltt, 4, gc, S, ts, tt);
         if (!gc.ok) break;
@@ -181,6 +206,8 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_bicgstab(CgArgs
             const VT ri = MIX ? (VT)fmaf((float)-omn, (float)t[i], (float)si) : (VT)fma(-(double)omn, (double)t[i], (double)si);
             if (MIX) {
                 xlo[i] = fmaf((float)omn, (float)si, fmaf((float)al, (float)pnew[i], (float)xlo[i]));
+                // staged: w = p - omega v, read by the next first SpMV
+                if (LAY == 2) pnew[i] = (VT)fmaf(-(float)omn, (float)vnew[i], (float)pnew[i]);
             } else {
                 a.xhi[i] = fma(omega, (double)si, fma(alpha, (double)pnew[i], a.xhi[i]));
             }
@@ -196,7 +223,9 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_bicgstab(CgArgs
         if (MIX && (rnorm <= a.delta * rmax || (!a.fixed && rnorm <= a.tol * nb))) {
             // ---- reliable update: x_hi += x_lo; r = b - A x_hi in FP64 ----
             for (int i = row0 + threadIdx.x; i < row1; i += NT) {
-                a.xhi[i] = a.xhi[i] + (double)xlo[i];
+                const double xn = a.xhi[i] + (double)xlo[i];
+                a.xhi[i] = xn;
+                if (LAY == 2) a.xs[i] = xn;  // padded copy the staged SpMV reads
                 xlo[i] = (VT)0;
             }
             grid_sync(a, gc);
@@ -204,14 +233,20 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_bicgstab(CgArgs
             double l1 = 0.0, l2 = 0.0;
             const double *xh = a.xhi;
             auto xsrc = [=](int c) -> double { return xh[c]; };
-            auto rout = [&](int s, int rw, double y, double, bool) {
+            auto rout = [&](int s, int rw, double y, auto, bool) {
                 const int i = s * MF_TILE + rw;
                 const VT rv2 = (VT)(a.b[i] - y);
                 r[i] = rv2;
                 l1 = __dadd_rn(l1, __dmul_rn((double)rh[i], (double)rv2));
                 l2 = __dadd_rn(l2, __dmul_rn((double)rv2, (double)rv2));
             };
-            if (!spmv_any<0, LAY>(a, S, gc, cb, ce, sb0, se0, xsrc, rout, nullptr)) gc.ok = false;
+            if constexpr (LAY == 2) {
+                if (!spmv_staged<0, false, double, 1>(a, S, gc, cb, ce, (const double *)a.xs, (const double *)nullptr,
+                                                      0.0, rout, nullptr))
+                    gc.ok = false;
+            } else {
+                if (!spmv_any<0, LAY>(a, S, gc, cb, ce, sb0, se0, xsrc, rout, nullptr)) gc.ok = false;
+            }
             grid_sum2(a, l1, l2, 0, gc, S, rho_new, rrn);
             if (!gc.ok) break;
             rnorm = sqrt(rrn);
@@ -261,7 +296,7 @@ int max_ctas_bicg()
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const size_t dyn = LAY == 0 ? sizeof(SolverSmem) : sizeof(SlotSmem);
+        const size_t dyn = sizeof(typename BicgSmem<MIX, LAY>::type);
         cudaFuncSetAttribute(k_bicgstab<MIX, LAY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bicgstab<MIX, LAY>, NT, dyn);
         cached = sms * (per > 0 ? per : 1);
@@ -271,10 +306,12 @@ int max_ctas_bicg()
 
 }  // namespace
 
-int bicgstab_grid(mf_matrix m, bool mixed, bool slots)
+int bicgstab_grid(mf_matrix m, bool mixed, int layout)
 {
-    int maxc = slots ? (mixed ? max_ctas_bicg<true, 1>() : max_ctas_bicg<false, 1>())
-                     : (mixed ? max_ctas_bicg<true, 0>() : max_ctas_bicg<false, 0>());
+    const bool slots = layout != 0;
+    int maxc = layout == 2   ? max_ctas_bicg<true, 2>()  // mixed only
+               : layout == 1 ? (mixed ? max_ctas_bicg<true, 1>() : max_ctas_bicg<false, 1>())
+                             : (mixed ? max_ctas_bicg<true, 0>() : max_ctas_bicg<false, 0>());
     if (const char *e = getenv("MF_SOLVER_CTAS")) {
         const int v = atoi(e);
         if (v > 0 && v < maxc) maxc = v;
@@ -292,7 +329,10 @@ mf_status launch_bicgstab(bool mixed, CgArgs &a, int G, cudaStream_t s)
     note_launch();
     const void *fn;
     size_t dyn;
-    if (a.sslot) {
+    if (a.spos && mixed) {
+        dyn = sizeof(StagedSmem<true>);
+        max_ctas_bicg<true, 2>(), fn = (const void *)k_bicgstab<true, 2>;
+    } else if (a.sslot) {
         dyn = sizeof(SlotSmem);
         if (mixed) max_ctas_bicg<true, 1>(), fn = (const void *)k_bicgstab<true, 1>;
         else max_ctas_bicg<false, 1>(), fn = (const void *)k_bicgstab<false, 1>;

@@ -29,21 +29,22 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
         one_reduction = !bicg && !mixed && !hook && want;
     }
     // execution layout: staged row slots for the mixed-precision
-    // two-reduction CG kernel, plain row slots otherwise or when a chunk
-    // cannot be staged, tile chunks when the slots cannot describe the
-    // matrix.  (The FP64 kernel stages two FP64 vectors, which leaves room
-    // for two CTAs per SM only; its plain row slots run faster.)
-    // MF_SOLVER_LAYOUT=tiles / slots restricts the choice, =staged also
-    // stages the FP64 kernel.
+    // two-reduction CG kernel and the mixed BiCGSTAB kernel, plain row slots
+    // otherwise or when a chunk cannot be staged, tile chunks when the slots
+    // cannot describe the matrix.  (The FP64 CG kernel stages two FP64
+    // vectors, which leaves room for two CTAs per SM only; its plain row
+    // slots run faster.)  MF_SOLVER_LAYOUT=tiles / slots restricts the
+    // choice, =staged also stages the FP64 CG kernel.
     const char *lay = getenv("MF_SOLVER_LAYOUT");
     const bool want_slots = !(lay && !strcmp(lay, "tiles"));
     if (want_slots) MF_TRY(build_slots(m, s));
     const bool slots = want_slots && m->slots_state == 1;
     const bool force_staged = lay && !strcmp(lay, "staged");
-    bool staged = slots && !bicg && !one_reduction && (mixed || force_staged) &&
+    bool staged = slots && !one_reduction && (bicg ? mixed : (mixed || force_staged)) &&
                   !(lay && !strcmp(lay, "slots")) && (long long)m->v.tilen <= (long long)m->v.tilem;
     auto layout_grid = [&](bool st) {
-        return bicg ? bicgstab_grid(m, mixed, slots) : solver_grid(m, mixed, st ? 2 : slots ? 1 : 0);
+        const int l = st ? 2 : slots ? 1 : 0;
+        return bicg ? bicgstab_grid(m, mixed, l) : solver_grid(m, mixed, l);
     };
     int G = layout_grid(staged);
     auto prepare = [&]() -> mf_status {
@@ -106,7 +107,9 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
         if (staged) {
             a.spos = m->d_spos;
             a.sdesc = m->d_sdesc;
-            a.xs = (double *)w.t;  // padded to whole strips (tile columns of a square tile grid)
+            // padded to whole strips (tile columns of a square tile grid); a
+            // buffer the kernel does not otherwise use (BiCGSTAB uses t)
+            a.xs = (double *)(bicg ? w.q : w.t);
         }
     }
     a.pay = m->d_pay;

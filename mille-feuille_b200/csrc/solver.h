@@ -136,7 +136,7 @@ mf_status refresh_chunk_payload(mf_matrix m, cudaStream_t s);
 int solver_grid(mf_matrix m, bool mixed, int layout);  // layout: 0 tiles, 1 slots, 2 staged slots
 mf_status launch_cg(bool mixed, CgArgs &a, int G, cudaStream_t s);
 mf_status launch_bicgstab(bool mixed, CgArgs &a, int G, cudaStream_t s);
-int bicgstab_grid(mf_matrix m, bool mixed, bool slots);
+int bicgstab_grid(mf_matrix m, bool mixed, int layout);  // layout as solver_grid (2: mixed only)
 // slots.cu: the row-slot layout (built once; state -1 = not describable)
 mf_status build_slots(mf_matrix m, cudaStream_t s);
 mf_status pack_slots(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s);

@@ -139,3 +139,20 @@ def test_staged_fixed_iterations_and_tiny_budget(mf, monkeypatch):
     x, rep = M.solve_host(b, tol=1e-10, maxiter=5000, policy="static")
     assert rep.status == 0 and rep.layout == 2 and rep.relres_true <= 1.05e-10
     M.close()
+
+
+@pytest.mark.parametrize("g", [24, 33])
+def test_staged_bicgstab_bit_identical_to_slots(mf, monkeypatch, g):
+    """Mixed BiCGSTAB on staged chunks (w = p - omega v stored by the update
+    pass, so each SpMV stages two vectors) equals the plain slots bit for
+    bit on the nonsymmetric convection-diffusion system."""
+    A = mf.synth_convdiff3d(g)
+    b = A.matvec(mf.synth_xstar(2, A.n_rows))
+    M = mf.Matrix(A)
+    x2, r2 = _solve(mf, M, b, monkeypatch, None, method="bicgstab", tol=1e-9, maxiter=5000, policy="static")
+    x1, r1 = _solve(mf, M, b, monkeypatch, "slots", method="bicgstab", tol=1e-9, maxiter=5000, policy="static")
+    assert r2.layout == 2 and r1.layout == 1
+    assert r1.status == r2.status == 0 and r1.iterations == r2.iterations
+    assert np.array_equal(x1.view(np.uint64), x2.view(np.uint64))
+    assert ol.oracle_true_relres(ol.Csr(A.n_rows, A.n_cols, A.rowptr, A.colidx, A.val), b, x2) <= 1.05e-9
+    M.close()

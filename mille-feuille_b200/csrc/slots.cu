@@ -176,6 +176,8 @@ __global__ void k_slot_pack(MfTiles A, const int *__restrict__ sslot, const unsi
     }
 }
 
+constexpr int WALK_NT = 16;  // walking threads per block of the chunk walk kernels
+
 // Sorted union of a staged chunk's tile columns while the walk grows it.
 struct StageUnion {
     int n, runs;
@@ -275,7 +277,10 @@ __global__ void k_slot_chunk_count(int G, const int *__restrict__ part, const in
                                    const int *__restrict__ tile_ptr, const int *__restrict__ tcol, int staged,
                                    int *__restrict__ cnt)
 {
-    StageUnion U;
+    // the walking thread's tile-column union, in shared memory (WALK_NT
+    // threads per block): in local memory its merges went to L2
+    __shared__ StageUnion su[WALK_NT];
+    StageUnion &U = su[threadIdx.x];
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g <= G; g += gridDim.x * blockDim.x) {
         if (g == G) {
             cnt[g] = 0;
@@ -297,7 +302,10 @@ __global__ void k_slot_chunk_fill(int G, const int *__restrict__ part, const int
                                   const int *__restrict__ tile_ptr, const int *__restrict__ tcol, int staged,
                                   const int *__restrict__ off, SlotChunk *__restrict__ rec, int *__restrict__ unstaged)
 {
-    StageUnion U;
+    // the walking thread's tile-column union, in shared memory (WALK_NT
+    // threads per block): in local memory its merges went to L2
+    __shared__ StageUnion su[WALK_NT];
+    StageUnion &U = su[threadIdx.x];
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
         int c = off[g], s = part[g];
         const int se = part[g + 1];
@@ -413,14 +421,14 @@ mf_status build_slot_chunks(mf_matrix m, int G, bool staged, cudaStream_t s)
     int *unstaged = cnt + G + 1;
     MF_CUDA(cudaMemsetAsync(unstaged, 0, sizeof(int), s));
     const int *tcol = m->v.tile_columnidx;
-    k_slot_chunk_count<<<grid_for3(G + 1, 128), 128, 0, s>>>(G, m->d_part, m->d_sslot, m->d_tile_ptr, tcol,
+    k_slot_chunk_count<<<grid_for3(G + 1, WALK_NT), WALK_NT, 0, s>>>(G, m->d_part, m->d_sslot, m->d_tile_ptr, tcol,
                                                              staged ? 1 : 0, cnt);
     note_launch();
     MF_CUDA(cudaGetLastError());
     int total = 0;
     MF_TRY(exclusive_scan_i32(cnt, m->d_scta_chunk, G + 1, s, &total));
     MF_CUDA(cudaMalloc(&m->d_schunks, sizeof(SlotChunk) * (size_t)(total > 0 ? total : 1)));
-    k_slot_chunk_fill<<<grid_for3(G, 128), 128, 0, s>>>(G, m->d_part, m->d_sslot, m->d_tile_ptr, tcol,
+    k_slot_chunk_fill<<<grid_for3(G, WALK_NT), WALK_NT, 0, s>>>(G, m->d_part, m->d_sslot, m->d_tile_ptr, tcol,
                                                         staged ? 1 : 0, m->d_scta_chunk, (SlotChunk *)m->d_schunks,
                                                         unstaged);
     note_launch();

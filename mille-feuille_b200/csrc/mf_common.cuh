@@ -287,13 +287,14 @@ __device__ __forceinline__ double warp_sum_partials(const double *part, int coun
 }
 
 // Deterministic sum of `count` per-CTA partials by a whole CTA (same order
-// in every CTA): thread t sums entries t, t + NT, ... (loads issued
-// together), then the fixed block tree.  All threads get the result.
+// in every CTA): thread t sums entries t, t + NT, ... (loads issued four at
+// a time: up to 4 NT partials in one L2 round trip), then the fixed block
+// tree.  All threads get the result.
 template <int NT>
 __device__ __forceinline__ double block_sum_partials(const double *part, int count, double *s_warp)
 {
     double s = 0.0;
-    constexpr int B = 2;
+    constexpr int B = 4;
     for (int i0 = threadIdx.x; i0 < count; i0 += NT * B) {
         double v[B];
 #pragma unroll

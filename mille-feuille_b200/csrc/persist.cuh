@@ -699,7 +699,10 @@ struct StagedCfg {
                       STAGE % 16 == 0 && SC_XCAP % 16 == 0,
                   "staged regions must be 16-byte aligned");
 };
-constexpr int TRECS = 32;  // staged chunk records cached in shared memory
+#ifndef MF_STAGED_RECS
+#define MF_STAGED_RECS 32
+#endif
+constexpr int TRECS = MF_STAGED_RECS;  // staged chunk records cached in shared memory
 
 template <bool MIX>
 struct __align__(16) StagedSmem {
@@ -762,7 +765,7 @@ __device__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S, int c, int k, 
 // where the tile column does, so the FP64 per-tile partial sums are those of
 // blockspmv_cpu).  vd may point to shared or global memory.
 #ifndef MF_STAGED_UNROLL
-#define MF_STAGED_UNROLL 4
+#define MF_STAGED_UNROLL 8
 #endif
 constexpr int STAGED_UNROLL = MF_STAGED_UNROLL;
 

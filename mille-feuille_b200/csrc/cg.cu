@@ -43,6 +43,9 @@ using namespace persist;
 #ifndef MF_STAGED_MINB_FP64
 #define MF_STAGED_MINB_FP64 2
 #endif
+#ifndef MF_VEC_U
+#define MF_VEC_U 4  // rows per thread in flight in the vector update pass
+#endif
 // CTAs per SM of the kernels on staged chunks (shared memory allows them)
 constexpr int staged_minb(bool mix) { return mix ? MF_STAGED_MINB_MIX : MF_STAGED_MINB_FP64; }
 
@@ -174,7 +177,7 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : stage
         // ---- x += alpha p, r -= alpha q over this CTA's rows ----
         loc = 0.0;
         {
-            constexpr int U = 4;
+            constexpr int U = MF_VEC_U;
             for (int i0 = row0 + threadIdx.x; i0 < row1; i0 += NT * U) {
                 VT xv[U], pv[U], qv[U], rv[U];
 #pragma unroll

@@ -64,6 +64,10 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
     return v;
 }
 
+#ifndef MF_BARRIER_SLEEP_NS
+#define MF_BARRIER_SLEEP_NS 64  // sleep between grid-barrier polls after the first few
+#endif
+
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p)
 {
     unsigned long long v;
@@ -229,7 +233,7 @@ __device__ __forceinline__ bool grid_barrier_flat(unsigned long long *ctr, unsig
             unsigned spins = 0;
             while (ld_relaxed_u64(ctr) < target) {
                 ++spins;
-                if (spins > 8u) __nanosleep(64);
+                if (MF_BARRIER_SLEEP_NS > 0 && spins > 8u) __nanosleep(MF_BARRIER_SLEEP_NS);
                 if ((spins & 15u) == 0u) {
                     if (ld_volatile_i32(status) != DEV_OK) { ok = 0; break; }
                     if (globaltimer_ns() - t0 > budget_ns) {

@@ -17,7 +17,10 @@
  *                           / blockspmv_cpu          src/blockspmv_cpu.h:2
  *   mf_cg_solve             persistent CG kernels    src/Mille-feuille-cg.h:168,352,1109
  *                           mixed persistent CG      src/main-cg-mixed.cu:99,998
- *   mf_read_matrix_market   read_Dmatrix_32          src/biio2.0/src/biio.h:153
+ *   mf_read_matrix_market   read_Dmatrix_32 (.mtx)   src/biio2.0/src/biio.h:153
+ *   mf_read_matrix          read_Dmatrix_32          src/biio2.0/src/biio.h:153
+ *   mf_read_cbd / _write_cbd binary_read_csr /       src/biio2.0/src/biio.h:22, 72
+ *                           binary_write_csr
  * The reference's own solve entry points (cg_solve_*, bicgstab*) keep their
  * signatures in Mille-feuille-cg.h / Mille-feuille-bicg.h beside this file.
  */
@@ -309,6 +312,24 @@ mf_status mf_selftest_bounded_waits(double budget_s, int *results);
  * file placed right after its original (mmio_highlevel.h:151-321). */
 mf_status mf_read_matrix_market(const char *path, int *m, int *n, int *nnz, int **rowptr,
                                 int **colidx, double **val, int *is_symmetric);
+
+/* Binary CSR files (".cbd"), the reference's cache of a parsed matrix
+ * (binary_read_csr / binary_write_csr, src/biio2.0/src/biio.h:22-94):
+ * int32 rows, int32 cols, int64 nnz, int64 row_ptr[rows+1],
+ * int32 col_idx[nnz], double val[nnz], machine byte order.  The reader
+ * allocates with malloc (free with mf_free_host) and reports a file whose
+ * length, row pointers or column indices do not match its header as
+ * MF_ERR_IO; more than 2^31-1 entries is MF_ERR_UNSUPPORTED. */
+mf_status mf_read_cbd(const char *path, int *m, int *n, int *nnz, int **rowptr, int **colidx, double **val);
+mf_status mf_write_cbd(const char *path, int m, int n, int nnz, const int *rowptr, const int *colidx,
+                       const double *val);
+
+/* The CLIs' reader (read_Dmatrix_32, src/biio2.0/src/biio.h:153): ".cbd"
+ * files through mf_read_cbd (*is_symmetric set to 0: the file holds the
+ * matrix as stored), ".mtx" files through mf_read_matrix_market; any other
+ * name is MF_ERR_IO. */
+mf_status mf_read_matrix(const char *path, int *m, int *n, int *nnz, int **rowptr, int **colidx, double **val,
+                         int *is_symmetric);
 void mf_free_host(void *p);
 
 /*

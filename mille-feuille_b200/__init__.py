@@ -103,6 +103,9 @@ def lib() -> C.CDLL:
         L.mf_bicgstab_solve.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport), vp, vp]
         L.mf_bicgstab_solve_host.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]
         L.mf_read_matrix_market.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
+        L.mf_read_matrix.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
+        L.mf_read_cbd.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp)]
+        L.mf_write_cbd.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, vp]
         L.mf_free_host.argtypes = [vp]
         L.mf_free_host.restype = None
         L.mf_rng_u01.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64]
@@ -223,6 +226,34 @@ def read_matrix_market(path):
     check(L.mf_read_matrix_market(str(path).encode(), C.byref(m), C.byref(n), C.byref(nnz), C.byref(rp),
                                   C.byref(ci), C.byref(v), C.byref(sym)))
     return _take_csr(m.value, nnz.value, rp, ci, v, n_cols=n.value)
+
+
+def read_matrix(path):
+    """.mtx or .cbd by extension (mf_read_matrix); returns (HostCsr, is_symmetric)."""
+    L = lib()
+    m, n, nnz, sym = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    rp, ci = C.POINTER(C.c_int)(), C.POINTER(C.c_int)()
+    v = C.POINTER(C.c_double)()
+    check(L.mf_read_matrix(str(path).encode(), C.byref(m), C.byref(n), C.byref(nnz), C.byref(rp), C.byref(ci),
+                           C.byref(v), C.byref(sym)))
+    return _take_csr(m.value, nnz.value, rp, ci, v, n_cols=n.value), sym.value
+
+
+def read_cbd(path):
+    """A binary CSR (.cbd) file (mf_read_cbd)."""
+    L = lib()
+    m, n, nnz = C.c_int(), C.c_int(), C.c_int()
+    rp, ci = C.POINTER(C.c_int)(), C.POINTER(C.c_int)()
+    v = C.POINTER(C.c_double)()
+    check(L.mf_read_cbd(str(path).encode(), C.byref(m), C.byref(n), C.byref(nnz), C.byref(rp), C.byref(ci),
+                        C.byref(v)))
+    return _take_csr(m.value, nnz.value, rp, ci, v, n_cols=n.value)
+
+
+def write_cbd(path, A):
+    """Writes A as a binary CSR (.cbd) file (mf_write_cbd)."""
+    check(lib().mf_write_cbd(str(path).encode(), A.n_rows, A.n_cols, A.nnz, A.rowptr.ctypes.data,
+                             A.colidx.ctypes.data, A.val.ctypes.data))
 
 
 def solve_opts(**kw):

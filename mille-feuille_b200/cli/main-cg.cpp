@@ -1,9 +1,10 @@
 // main-cg / main-cg-mixed: the reference's CG drivers (src/main-cg.cu:1630-1673,
-// src/main-cg-mixed.cu:3006-3042).  Reads a Matrix Market file, truncates the
+// src/main-cg-mixed.cu:3006-3042).  Reads a Matrix Market or binary CSR file, truncates the
 // rows to a multiple of 16, sets b = A * ones and calls the CG entry point
 // the reference picks by nnz (main-cg) or cg_solve_inc (main-cg-mixed).
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "Mille-feuille-cg.h"
@@ -12,14 +13,18 @@
 int main(int argc, char **argv)
 {
     if (argc < 2) {
-        fprintf(stderr, "usage: %s matrix.mtx\n", argv[0]);
+        fprintf(stderr, "usage: %s matrix.mtx|matrix.cbd\n", argv[0]);
         return 1;
     }
     char *filename = argv[1];
     int m = 0, n = 0, nnzR = 0, sym = 0;
     int *RowPtr = nullptr, *ColIdx = nullptr;
     double *Val = nullptr;
-    if (mf_read_matrix_market(filename, &m, &n, &nnzR, &RowPtr, &ColIdx, &Val, &sym) != MF_OK) {
+    // .mtx or .cbd by extension, as the reference's read_Dmatrix_32, which
+    // announces a binary file on stdout
+    const size_t flen = strlen(filename);
+    if (flen >= 3 && !strcmp(filename + flen - 3, "cbd")) printf("read binary file %s\n", filename);
+    if (mf_read_matrix(filename, &m, &n, &nnzR, &RowPtr, &ColIdx, &Val, &sym) != MF_OK) {
         fprintf(stderr, "%s\n", mf_last_error());
         return 1;
     }

@@ -9,6 +9,7 @@
 // keep file order (columns are not sorted).  Unlike the reference, a
 // malformed file is reported as MF_ERR_IO instead of being read past its end.
 #include <cerrno>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -193,4 +194,124 @@ extern "C" mf_status mf_read_matrix_market(const char *path, int *m_out, int *n_
     *val = va;
     if (is_symmetric) *is_symmetric = sym ? 1 : 0;
     return MF_OK;
+}
+
+// ---- binary CSR (.cbd) ------------------------------------------------
+//
+// The reference's binary cache of a parsed matrix (binary_read_csr /
+// binary_write_csr, src/biio2.0/src/biio.h:22-94): int32 rows, int32 cols,
+// int64 nnz, then int64 row_ptr[rows + 1], int32 col_idx[nnz] and double
+// val[nnz], in the machine's byte order.  The layout is kept because files
+// written by the reference must read here and the other way round.  Unlike
+// the reference, the reader checks the file length against the header and
+// the row pointers and column indices against the sizes, and reports a
+// malformed file as MF_ERR_IO.
+
+extern "C" mf_status mf_read_cbd(const char *path, int *m_out, int *n_out, int *nnz_out, int **rowptr, int **colidx,
+                                 double **val)
+{
+    if (!path || !m_out || !n_out || !nnz_out || !rowptr || !colidx || !val) return MF_ERR_INVALID_ARG;
+    FILE *f = fopen(path, "rb");
+    if (!f) {
+        mf::set_last_error("cannot open %s: %s", path, strerror(errno));
+        return MF_ERR_IO;
+    }
+    fseek(f, 0, SEEK_END);
+    const long long fsz = (long long)ftell(f);
+    fseek(f, 0, SEEK_SET);
+    int32_t rows = 0, cols = 0;
+    int64_t nnz = 0;
+    if (fread(&rows, 4, 1, f) != 1 || fread(&cols, 4, 1, f) != 1 || fread(&nnz, 8, 1, f) != 1) {
+        fclose(f);
+        mf::set_last_error("%s: truncated header", path);
+        return MF_ERR_IO;
+    }
+    if (rows < 0 || cols < 0 || nnz < 0 || nnz > 0x7fffffffLL ||
+        fsz != 16 + 8LL * ((long long)rows + 1) + 12LL * (long long)nnz) {
+        fclose(f);
+        if (nnz > 0x7fffffffLL) {
+            mf::set_last_error("%s: more than 2^31-1 entries", path);
+            return MF_ERR_UNSUPPORTED;
+        }
+        mf::set_last_error("%s: header (%d x %d, %lld entries) does not match the file length %lld", path, rows, cols,
+                           (long long)nnz, fsz);
+        return MF_ERR_IO;
+    }
+    std::vector<int64_t> rp64((size_t)rows + 1);
+    int *rp = (int *)malloc(sizeof(int) * ((size_t)rows + 1));
+    int *cc = (int *)malloc(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1));
+    double *va = (double *)malloc(sizeof(double) * (size_t)(nnz > 0 ? nnz : 1));
+    auto fail = [&](mf_status st, const char *what) {
+        fclose(f);
+        free(rp);
+        free(cc);
+        free(va);
+        if (what) mf::set_last_error("%s: %s", path, what);
+        return st;
+    };
+    if (!rp || !cc || !va) return fail(MF_ERR_NO_MEMORY, nullptr);
+    if (fread(rp64.data(), 8, (size_t)rows + 1, f) != (size_t)rows + 1 ||
+        fread(cc, 4, (size_t)nnz, f) != (size_t)nnz || fread(va, 8, (size_t)nnz, f) != (size_t)nnz)
+        return fail(MF_ERR_IO, "truncated arrays");
+    if (rp64[0] != 0 || rp64[rows] != nnz) return fail(MF_ERR_IO, "row pointers do not span the entries");
+    for (int r = 0; r < rows; r++) {
+        if (rp64[r + 1] < rp64[r]) return fail(MF_ERR_IO, "row pointers decrease");
+        rp[r] = (int)rp64[r];
+    }
+    rp[rows] = (int)nnz;
+    for (int64_t k = 0; k < nnz; k++)
+        if (cc[k] < 0 || cc[k] >= cols) return fail(MF_ERR_IO, "column index out of range");
+    fclose(f);
+    *m_out = rows;
+    *n_out = cols;
+    *nnz_out = (int)nnz;
+    *rowptr = rp;
+    *colidx = cc;
+    *val = va;
+    return MF_OK;
+}
+
+extern "C" mf_status mf_write_cbd(const char *path, int m, int n, int nnz, const int *rowptr, const int *colidx,
+                                  const double *val)
+{
+    if (!path || m < 0 || n < 0 || nnz < 0 || !rowptr || (nnz > 0 && (!colidx || !val))) return MF_ERR_INVALID_ARG;
+    FILE *f = fopen(path, "wb");
+    if (!f) {
+        mf::set_last_error("cannot create %s: %s", path, strerror(errno));
+        return MF_ERR_IO;
+    }
+    const int32_t rows = m, cols = n;
+    const int64_t nz = nnz;
+    std::vector<int64_t> rp64((size_t)m + 1);
+    for (int r = 0; r <= m; r++) rp64[r] = rowptr[r];
+    bool ok = fwrite(&rows, 4, 1, f) == 1 && fwrite(&cols, 4, 1, f) == 1 && fwrite(&nz, 8, 1, f) == 1 &&
+              fwrite(rp64.data(), 8, (size_t)m + 1, f) == (size_t)m + 1 &&
+              (nnz == 0 || (fwrite(colidx, 4, (size_t)nnz, f) == (size_t)nnz &&
+                            fwrite(val, 8, (size_t)nnz, f) == (size_t)nnz));
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) {
+        mf::set_last_error("%s: write failed", path);
+        return MF_ERR_IO;
+    }
+    return MF_OK;
+}
+
+// The reference CLIs' reader (read_Dmatrix_32, src/biio2.0/src/biio.h:153-194):
+// the file name's extension picks the format, ".cbd" binary CSR or ".mtx"
+// Matrix Market.  A binary file holds the matrix as stored, so
+// *is_symmetric is 0 for it.
+extern "C" mf_status mf_read_matrix(const char *path, int *m, int *n, int *nnz, int **rowptr, int **colidx,
+                                    double **val, int *is_symmetric)
+{
+    if (!path) return MF_ERR_INVALID_ARG;
+    const size_t len = strlen(path);
+    if (len >= 3 && !strcmp(path + len - 3, "cbd")) {
+        const mf_status st = mf_read_cbd(path, m, n, nnz, rowptr, colidx, val);
+        if (st == MF_OK && is_symmetric) *is_symmetric = 0;
+        return st;
+    }
+    if (len >= 3 && !strcmp(path + len - 3, "mtx"))
+        return mf_read_matrix_market(path, m, n, nnz, rowptr, colidx, val, is_symmetric);
+    mf::set_last_error("%s: unsupported file type (expected .mtx or .cbd)", path);
+    return MF_ERR_IO;
 }

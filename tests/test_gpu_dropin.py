@@ -252,3 +252,20 @@ def test_cli_end_to_end(mf, tmp_path, cli, csv, tag):
     rows = _csv_rows(tmp_path / "data" / csv)
     assert len(rows) == 2 and rows[0][0] == str(f) and int(rows[0][3]) == A.nnz
     assert float(rows[1][4]) <= 2e-10
+
+
+@pytest.mark.parametrize("cli,csv,tag", [("main-cg", "cg_performance.csv", "time_cg="),
+                                         ("main-bicg-mixed", "bicg_performance.csv", "time_bicg=")])
+def test_cli_end_to_end_binary_csr(mf, tmp_path, cli, csv, tag):
+    """The same Laplacian as a binary CSR (.cbd) file, which the reference's
+    CLIs also take: announced on stdout, then the solve as from the .mtx."""
+    (tmp_path / "data").mkdir()
+    A = mf.synth_laplace2d(30, 30)
+    f = tmp_path / "lap30.cbd"
+    mf.write_cbd(f, A)
+    p = _run(cli, [str(f)], tmp_path)
+    assert p.returncode == 0, p.stderr
+    first, rest = p.stdout.split("\n", 1)
+    assert first == f"read binary file {f}" and rest.startswith(tag), p.stdout
+    rows = _csv_rows(tmp_path / "data" / csv)
+    assert len(rows) == 1 and rows[0][0] == str(f) and int(rows[0][3]) == A.nnz

@@ -8,12 +8,17 @@
 // entry (i,j), the entry (i,j) in row i and (j,i) in row j; entries of a row
 // keep file order (columns are not sorted).  Unlike the reference, a
 // malformed file is reported as MF_ERR_IO instead of being read past its end.
+// Large files are parsed by several threads (same numbers: std::from_chars
+// rounds as strtod does).
+#include <algorithm>
 #include <cerrno>
+#include <charconv>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "mf.h"
@@ -57,6 +62,139 @@ std::string lower(std::string s)
 {
     for (auto &c : s) c = (char)tolower((unsigned char)c);
     return s;
+}
+
+inline bool is_space(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\n'; }
+
+// One whitespace-delimited number for the parallel parser: std::from_chars
+// (correctly rounded, so the same double as strtod), with strtoll / strtod
+// for what from_chars does not take (a leading '+', hexadecimal floats).
+inline bool tok_ll(const char *&p, const char *e, long long &v)
+{
+    while (p < e && is_space(*p)) p++;
+    if (p >= e) return false;
+    const char *q = (*p == '+') ? p + 1 : p;
+    const auto r = std::from_chars(q, e, v);
+    if (r.ec == std::errc() && (r.ptr == e || is_space(*r.ptr))) {
+        p = r.ptr;
+        return true;
+    }
+    char *end;
+    v = strtoll(p, &end, 10);
+    if (end == p) return false;
+    p = end;
+    return true;
+}
+
+inline bool tok_d(const char *&p, const char *e, double &v)
+{
+    while (p < e && is_space(*p)) p++;
+    if (p >= e) return false;
+    const char *q = (*p == '+') ? p + 1 : p;
+    const auto r = std::from_chars(q, e, v);
+    if (r.ec == std::errc() && (r.ptr == e || is_space(*r.ptr))) {
+        p = r.ptr;
+        return true;
+    }
+    char *end;
+    v = strtod(p, &end);
+    if (end == p) return false;
+    p = end;
+    return true;
+}
+
+// Entries of a coordinate file parsed by several threads: the entry lines
+// are cut at line starts into one piece per thread, each piece's numbers
+// are counted (so that every piece knows its first entry), then parsed into
+// place.  Returns false -- and the caller parses serially, which also
+// gives the exact error -- unless every piece holds whole entries and every
+// entry parses with its indices in range.
+bool parse_entries_parallel(const char *p, const char *e, long long NZ, long long M, long long N, bool pattern,
+                            bool complex_, bool integer, int nthreads, std::vector<int> &ri, std::vector<int> &ci,
+                            std::vector<double> &vv)
+{
+    const int per = 2 + (pattern ? 0 : (complex_ ? 2 : 1));  // numbers per entry
+    const int T = nthreads;
+    std::vector<const char *> b((size_t)T + 1);
+    b[0] = p;
+    b[T] = e;
+    for (int t = 1; t < T; t++) {
+        const char *q = p + (size_t)(e - p) * (size_t)t / (size_t)T;
+        if (q < b[t - 1]) q = b[t - 1];
+        const char *nl = (const char *)memchr(q, '\n', (size_t)(e - q));
+        b[t] = nl ? nl + 1 : e;
+    }
+    std::vector<long long> cnt((size_t)T, 0);
+    auto count = [&](int t) {
+        long long c = 0;
+        const char *q = b[t], *qe = b[t + 1];
+        while (q < qe) {
+            while (q < qe && is_space(*q)) q++;
+            if (q >= qe) break;
+            c++;
+            while (q < qe && !is_space(*q)) q++;
+        }
+        cnt[t] = c;
+    };
+    {
+        std::vector<std::thread> th;
+        for (int t = 1; t < T; t++) th.emplace_back(count, t);
+        count(0);
+        for (auto &x : th) x.join();
+    }
+    std::vector<long long> first((size_t)T + 1, 0);
+    for (int t = 0; t < T; t++) {
+        if (cnt[t] % per != 0) return false;  // an entry spans two pieces: not one entry per line
+        first[t + 1] = first[t] + cnt[t] / per;
+    }
+    if (first[T] < NZ) return false;  // truncated: the serial parser reports where
+    std::vector<char> bad((size_t)T, 0);
+    auto parse = [&](int t) {
+        const char *q = b[t];
+        const char *qe = b[t + 1];
+        const long long k1 = std::min(first[t + 1], NZ);
+        for (long long k = first[t]; k < k1; k++) {
+            long long i, j;
+            double v = 1.0, im;
+            if (!tok_ll(q, qe, i) || !tok_ll(q, qe, j)) {
+                bad[t] = 1;
+                return;
+            }
+            if (!pattern) {
+                if (integer) {
+                    long long iv;
+                    if (!tok_ll(q, qe, iv)) {
+                        bad[t] = 1;
+                        return;
+                    }
+                    v = (double)(int)iv;
+                } else if (!tok_d(q, qe, v)) {
+                    bad[t] = 1;
+                    return;
+                }
+                if (complex_ && !tok_d(q, qe, im)) {
+                    bad[t] = 1;
+                    return;
+                }
+            }
+            if (i < 1 || i > M || j < 1 || j > N) {
+                bad[t] = 1;
+                return;
+            }
+            ri[k] = (int)(i - 1);
+            ci[k] = (int)(j - 1);
+            vv[k] = v;
+        }
+    };
+    {
+        std::vector<std::thread> th;
+        for (int t = 1; t < T; t++) th.emplace_back(parse, t);
+        parse(0);
+        for (auto &x : th) x.join();
+    }
+    for (int t = 0; t < T; t++)
+        if (bad[t]) return false;
+    return true;
 }
 
 }  // namespace
@@ -112,8 +250,15 @@ extern "C" mf_status mf_read_matrix_market(const char *path, int *m_out, int *n_
     }
     std::vector<int> ri((size_t)NZ), ci((size_t)NZ);
     std::vector<double> vv((size_t)NZ);
-    std::vector<long long> cnt((size_t)M + 1, 0);
-    for (long long k = 0; k < NZ; k++) {
+    // entries in parallel on files of 200,000 entries or more, serially
+    // otherwise or when the file is not one entry per line;
+    // MF_MTX_THREADS=<t> sets the threads for every file (1: serial)
+    int nth = (int)std::thread::hardware_concurrency();
+    if (NZ < 200000) nth = 1;
+    if (const char *env = getenv("MF_MTX_THREADS")) nth = atoi(env);
+    nth = std::max(1, std::min(nth, 64));
+    bool parsed = nth > 1 && parse_entries_parallel(rd.p, e, NZ, M, N, pattern, complex_, integer, nth, ri, ci, vv);
+    for (long long k = 0; !parsed && k < NZ; k++) {
         long long i, j;
         double v = 1.0, im;
         if (!rd.next_long(i) || !rd.next_long(j)) {
@@ -144,6 +289,9 @@ extern "C" mf_status mf_read_matrix_market(const char *path, int *m_out, int *n_
         ri[k] = (int)(i - 1);
         ci[k] = (int)(j - 1);
         vv[k] = v;
+    }
+    std::vector<long long> cnt((size_t)M + 1, 0);
+    for (long long k = 0; k < NZ; k++) {
         cnt[ri[k]]++;
         if (sym && ri[k] != ci[k]) {
             if (ci[k] >= M) {

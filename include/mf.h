@@ -166,6 +166,13 @@ typedef struct mf_solve_opts {
     double wait_budget_s; /* bound on every grid-wide wait inside a kernel */
     int record_history;   /* keep ||r_k||/||b|| per iteration (see report) */
     int phase_times;      /* fill mf_solve_report.phase_us (device timers) */
+    int precond;          /* CG only: 0 none (the reference's method), 1 Jacobi
+                             (z = D^-1 r with D the diagonal of A; a zero
+                             diagonal entry leaves its row unscaled).  No
+                             reference counterpart: the preconditioned
+                             method cuts iterations on rows of very different
+                             scales.  BiCGSTAB and the batched solver reject
+                             it with MF_ERR_UNSUPPORTED. */
 } mf_solve_opts;
 
 typedef struct mf_solve_report {

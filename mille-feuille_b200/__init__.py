@@ -39,7 +39,8 @@ class MatrixInfo(C.Structure):
 
 class SolveOpts(C.Structure):
     _fields_ = [("maxiter", C.c_int), ("tol", C.c_double), ("policy", C.c_int), ("refine_delta", C.c_double),
-                ("wait_budget_s", C.c_double), ("record_history", C.c_int), ("phase_times", C.c_int)]
+                ("wait_budget_s", C.c_double), ("record_history", C.c_int), ("phase_times", C.c_int),
+                ("precond", C.c_int)]
 
 
 class BatchReport(C.Structure):

@@ -304,6 +304,7 @@ void mf_solve_opts_default(mf_solve_opts *o)
     o->wait_budget_s = 5.0;
     o->record_history = 0;
     o->phase_times = 0;
+    o->precond = 0;
 }
 
 static mf_status solve_common(bool bicg, mf_matrix m, const double *b, double *x, const mf_solve_opts *opts,
@@ -317,9 +318,14 @@ static mf_status solve_common(bool bicg, mf_matrix m, const double *b, double *x
     mf_solve_opts o;
     mf_solve_opts_default(&o);
     if (opts) o = *opts;
-    if (o.maxiter < 0 || o.wait_budget_s <= 0 || o.policy < 0 || o.policy > MF_POLICY_LEARNED) {
-        set_last_error("solve: maxiter < 0, wait budget <= 0 or unknown policy");
+    if (o.maxiter < 0 || o.wait_budget_s <= 0 || o.policy < 0 || o.policy > MF_POLICY_LEARNED || o.precond < 0 ||
+        o.precond > 1) {
+        set_last_error("solve: maxiter < 0, wait budget <= 0, unknown policy or unknown preconditioner");
         return MF_ERR_INVALID_ARG;
+    }
+    if (bicg && o.precond) {
+        set_last_error("solve: the Jacobi preconditioner is available for CG only");
+        return MF_ERR_UNSUPPORTED;
     }
     if (m->v.rows != m->v.cols) {
         set_last_error("solve: matrix is %d x %d, a square system is required", m->v.rows, m->v.cols);

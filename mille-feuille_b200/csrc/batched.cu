@@ -812,6 +812,10 @@ mf_status mf_batch_cg_solve(mf_batch bt, const double *b, double *x, const mf_so
         set_last_error("batched CG needs tol > 0 and maxiter > 0");
         return MF_ERR_INVALID_ARG;
     }
+    if (o.precond) {
+        set_last_error("batched CG: no preconditioner");
+        return MF_ERR_UNSUPPORTED;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     int lanes = bt->tuned_lanes ? bt->tuned_lanes : 8;
     int cluster = bt->tuned_cluster ? bt->tuned_cluster : 4;

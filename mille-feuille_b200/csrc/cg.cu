@@ -55,7 +55,9 @@ struct CgSmem {
                                            typename std::conditional<LAY == 1, SlotSmem, StagedSmem<MIX>>::type>::type;
 };
 
-template <bool MIX, int LAY>
+// PC: Jacobi-preconditioned CG (z = D^-1 r; p = z + beta p; beta from r.z;
+// convergence on ||r||), the same kernel otherwise.
+template <bool MIX, int LAY, bool PC = false>
 __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : staged_minb(MIX)) k_cg(CgArgs a)
 {
     using VT = typename VecT<MIX>::T;
@@ -69,6 +71,8 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : stage
     const int cb = LAY == 0 ? a.cta_chunk[g] : a.scta_chunk[g], ce = LAY == 0 ? a.cta_chunk[g + 1] : a.scta_chunk[g + 1];
     const int row0 = sb0 * MF_TILE, row1 = min(se0 * MF_TILE, A.rows);
     VT *r = (VT *)a.r, *q = (VT *)a.q, *xlo = (VT *)a.xlo;
+    VT *z = (VT *)a.z;
+    const double *dinv = a.dinv;
     GridCtx gc;
     gc.epoch = 0;
     gc.ok = true;
@@ -87,9 +91,10 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : stage
     __syncthreads();
 
     double rho, beta, nb, rmax;
+    double rz = 0.0;  // PC: r.z
     int it, refs;
     if (a.start) {
-        double lb = 0.0, lr = 0.0;
+        double lb = 0.0, lr = 0.0, lz = 0.0;
         for (int i = row0 + threadIdx.x; i < row1; i += NT) {
             const double bv = a.b[i];
             const VT rv = (VT)bv;
@@ -97,11 +102,17 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : stage
             r[i] = rv;
             ((VT *)a.p0)[i] = (VT)0;
             if (MIX) xlo[i] = (VT)0;
+            if constexpr (PC) {
+                const VT zv = (VT)(dinv[i] * (double)rv);
+                z[i] = zv;
+                lz = __dadd_rn(lz, __dmul_rn((double)rv, (double)zv));
+            }
             lb = __dadd_rn(lb, __dmul_rn(bv, bv));
             lr = __dadd_rn(lr, __dmul_rn((double)rv, (double)rv));
         }
         const double bb = grid_sum(a, lb, 0, gc, S);
         rho = MIX ? grid_sum(a, lr, 1, gc, S) : bb;
+        if constexpr (PC) rz = grid_sum(a, lz, 5, gc, S);
         nb = sqrt(bb) > 0.0 ? sqrt(bb) : 1.0;
         beta = 0.0;
         rmax = sqrt(rho);
@@ -115,6 +126,7 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : stage
         rmax = st[S_RMAX];
         it = (int)st[S_ITERS];
         refs = (int)st[S_REFS];
+        rz = st[S_RZ];
     }
     int exit_reason = EXIT_MAXITER;
     double relres_true = sqrt(rho) / nb;
@@ -140,7 +152,7 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : stage
         const VT *pold = (const VT *)((it & 1) ? a.p1 : a.p0);
         VT *pnew = (VT *)((it & 1) ? a.p0 : a.p1);
         const VT bt = (VT)beta;
-        const VT *rr = r;
+        const VT *rr = PC ? z : r;  // p = rr + beta p_old (z when preconditioned)
         auto psrc = [=](int c) -> VT {
             if constexpr (MIX) return fmaf(bt, pold[c], rr[c]);
             else return fma(bt, pold[c], rr[c]);
@@ -173,9 +185,10 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : stage
             exit_reason = EXIT_BREAKDOWN;
             break;
         }
-        const double alpha = rho / pq;
+        const double alpha = (PC ? rz : rho) / pq;
         // ---- x += alpha p, r -= alpha q over this CTA's rows ----
         loc = 0.0;
+        double locz = 0.0;  // PC: r.z
         {
             constexpr int U = MF_VEC_U;
             for (int i0 = row0 + threadIdx.x; i0 < row1; i0 += NT * U) {
@@ -199,17 +212,29 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : stage
                         const float ri = fmaf(-af, qv[u], rv[u]);
                         r[i] = ri;
                         loc = __dadd_rn(loc, __dmul_rn((double)ri, (double)ri));
+                        if constexpr (PC) {
+                            const float zi = (float)(dinv[i] * (double)ri);
+                            z[i] = zi;
+                            locz = __dadd_rn(locz, __dmul_rn((double)ri, (double)zi));
+                        }
                     } else {
                         a.xhi[i] = fma(alpha, (double)pv[u], (double)xv[u]);
                         const double ri = fma(-alpha, (double)qv[u], (double)rv[u]);
                         r[i] = ri;
                         loc = __dadd_rn(loc, __dmul_rn(ri, ri));
+                        if constexpr (PC) {
+                            const double zi = dinv[i] * ri;
+                            z[i] = zi;
+                            locz = __dadd_rn(locz, __dmul_rn(ri, zi));
+                        }
                     }
                 }
             }
         }
         MF_MARK(2);
-        double rho_new = grid_sum(a, loc, 3, gc, S);
+        double rho_new, rz_new = 0.0;
+        if constexpr (PC) grid_sum_pair(a, loc, locz, 3, gc, S, rho_new, rz_new);
+        else rho_new = grid_sum(a, loc, 3, gc, S);
         MF_MARK(3);
         if (!gc.ok) break;
         it++;
@@ -227,11 +252,17 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : stage
             loc = 0.0;
             const double *xh = a.xhi;
             auto xsrc = [=](int c) -> double { return xh[c]; };
+            locz = 0.0;
             auto rout = [&](int s, int rw, double y, auto, bool) {
                 const int i = s * MF_TILE + rw;
                 const VT rv = (VT)(a.b[i] - y);
                 r[i] = rv;
                 loc = __dadd_rn(loc, __dmul_rn((double)rv, (double)rv));
+                if constexpr (PC) {
+                    const VT zv = (VT)(dinv[i] * (double)rv);
+                    z[i] = zv;
+                    locz = __dadd_rn(locz, __dmul_rn((double)rv, (double)zv));
+                }
             };
             if constexpr (LAY == 2) {
                 if (!spmv_staged<0, false, double, 1>(a, S, gc, cb, ce, (const double *)a.xs, (const double *)nullptr,
@@ -240,7 +271,8 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : stage
             } else {
                 if (!spmv_any<0, LAY>(a, S, gc, cb, ce, sb0, se0, xsrc, rout, nullptr)) gc.ok = false;
             }
-            rho_new = grid_sum(a, loc, 1, gc, S);
+            if constexpr (PC) grid_sum_pair(a, loc, locz, 0, gc, S, rho_new, rz_new);
+            else rho_new = grid_sum(a, loc, 1, gc, S);
             if (!gc.ok) break;
             rmax = sqrt(rho_new);
             relres_true = sqrt(rho_new) / nb;
@@ -248,7 +280,12 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : stage
             refined = true;
             MF_MARK(4);
         }
-        beta = rho_new / rho;
+        if constexpr (PC) {
+            beta = rz_new / rz;
+            rz = rz_new;
+        } else {
+            beta = rho_new / rho;
+        }
         rho = rho_new;
         if (!MIX) relres_true = sqrt(rho) / nb;
         if (a.hist && g == 0 && threadIdx.x == 0) a.hist[it] = sqrt(rho) / nb;
@@ -276,6 +313,7 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : stage
         st[S_REFS] = (double)refs;
         st[S_EXIT] = (double)exit_reason;
         st[S_RELRES] = relres_true;
+        st[S_RZ] = rz;
     }
 }
 
@@ -392,6 +430,29 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : SMINB) k_cg1(CgArgs a)
     }
 }
 
+// Jacobi: 1 / a_ii of every row from the tile format (the diagonal tile of
+// the row's strip, the row's entry in its column), 1 where the diagonal is
+// missing or zero.
+__global__ void k_jacobi_dinv(MfTiles A, double *__restrict__ dinv)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.rows; i += gridDim.x * blockDim.x) {
+        const int s = i >> 4, rw = i & 15;
+        const int rowlen = (s == A.tilem - 1) ? A.rows - s * MF_TILE : MF_TILE;
+        double d = 0.0;
+        for (int t = A.tile_ptr[s]; t < A.tile_ptr[s + 1]; t++) {
+            if (A.tile_columnidx[t] != s) continue;
+            const int off = A.tile_nnz[t], nz = A.tile_nnz[t + 1] - off;
+            const int po = A.csrptr_offset[t];
+            const int lo = A.ptr[po + rw];
+            const int hi = (rw == rowlen - 1) ? nz : (int)A.ptr[po + rw + 1];
+            for (int q = lo; q < hi; q++)
+                if (A.col[off + q] == rw) d = A.val[off + q];
+            break;
+        }
+        dinv[i] = (d != 0.0) ? 1.0 / d : 1.0;
+    }
+}
+
 // ||b - A x||^2 and ||b||^2 from y = A x, deterministic: per-CTA partials,
 // then one CTA sums them in a fixed tree.
 __global__ void k_resid_partials(int n, const double *__restrict__ b, const double *__restrict__ ax,
@@ -432,6 +493,25 @@ template <int LAY, bool MIX = false>
 constexpr size_t smem_bytes()
 {
     return sizeof(typename CgSmem<MIX, LAY>::type);
+}
+
+// The Jacobi variant of k_cg<MIX, LAY>: its shared-memory attribute set
+// once, and whether as many of its CTAs are resident as of the plain one's
+// (the grid is sized for those).
+template <bool MIX, int LAY>
+bool pc_ready(int G)
+{
+    static int resident = -1;
+    if (resident < 0) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const size_t dyn = smem_bytes<LAY, MIX>();
+        cudaFuncSetAttribute(k_cg<MIX, LAY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg<MIX, LAY, true>, NT, dyn);
+        resident = sms * per;
+    }
+    return G <= resident;
 }
 
 template <bool MIX, int LAY>
@@ -514,6 +594,15 @@ int solver_grid(mf_matrix m, bool mixed, int layout)
     return want < maxc ? want : maxc;
 }
 
+mf_status jacobi_dinv(mf_matrix m, double *dinv, cudaStream_t s)
+{
+    if (m->v.rows == 0) return MF_OK;
+    k_jacobi_dinv<<<std::min(ceil_div(m->v.rows, 256), 148 * 8), 256, 0, s>>>(m->v, dinv);
+    note_launch();
+    MF_CUDA(cudaGetLastError());
+    return MF_OK;
+}
+
 mf_status true_residual(mf_matrix m, const double *b, const double *x, SolverWork &w, double *relres, cudaStream_t s)
 {
     const int n = m->v.rows;
@@ -559,17 +648,29 @@ mf_status launch_cg(bool mixed, CgArgs &a, int G, cudaStream_t s)
         }
         a.one_reduction = 0;  // fall through to the two-reduction kernel
     }
+    const bool pc = a.dinv != nullptr;
+    bool ready = true;
     if (a.spos) {
-        if (mixed) dyn = smem_bytes<2, true>(), max_ctas_for<true, 2>(), fn = (const void *)k_cg<true, 2>;
-        else dyn = smem_bytes<2, false>(), max_ctas_for<false, 2>(), fn = (const void *)k_cg<false, 2>;
+        if (mixed) dyn = smem_bytes<2, true>(), max_ctas_for<true, 2>(),
+                   fn = pc ? (ready = pc_ready<true, 2>(G), (const void *)k_cg<true, 2, true>) : (const void *)k_cg<true, 2>;
+        else dyn = smem_bytes<2, false>(), max_ctas_for<false, 2>(),
+             fn = pc ? (ready = pc_ready<false, 2>(G), (const void *)k_cg<false, 2, true>) : (const void *)k_cg<false, 2>;
     } else if (a.sslot) {
         dyn = smem_bytes<1>();
-        if (mixed) max_ctas_for<true, 1>(), fn = (const void *)k_cg<true, 1>;
-        else max_ctas_for<false, 1>(), fn = (const void *)k_cg<false, 1>;
+        if (mixed) max_ctas_for<true, 1>(),
+            fn = pc ? (ready = pc_ready<true, 1>(G), (const void *)k_cg<true, 1, true>) : (const void *)k_cg<true, 1>;
+        else max_ctas_for<false, 1>(),
+            fn = pc ? (ready = pc_ready<false, 1>(G), (const void *)k_cg<false, 1, true>) : (const void *)k_cg<false, 1>;
     } else {
         dyn = smem_bytes<0>();
-        if (mixed) max_ctas_for<true, 0>(), fn = (const void *)k_cg<true, 0>;
-        else max_ctas_for<false, 0>(), fn = (const void *)k_cg<false, 0>;
+        if (mixed) max_ctas_for<true, 0>(),
+            fn = pc ? (ready = pc_ready<true, 0>(G), (const void *)k_cg<true, 0, true>) : (const void *)k_cg<true, 0>;
+        else max_ctas_for<false, 0>(),
+            fn = pc ? (ready = pc_ready<false, 0>(G), (const void *)k_cg<false, 0, true>) : (const void *)k_cg<false, 0>;
+    }
+    if (!ready) {
+        set_last_error("the Jacobi CG kernel cannot keep %d CTAs resident", G);
+        return MF_ERR_UNSUPPORTED;
     }
     MF_CUDA(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(NT), args, dyn, s));
     return MF_OK;

@@ -132,6 +132,27 @@ __device__ __forceinline__ double grid_sum(const CgArgs &a, double local, int sl
     return block_sum_partials<NT>(a.partials + slot * G, G, S.warp);
 }
 
+// Two sums at once (one barrier): slots slot and slot+1 of the partials;
+// every CTA gets the same two values.  Consecutive reductions must use
+// different slots (a CTA may write the next partials while another still
+// reads these).
+template <class SM>
+__device__ __forceinline__ void grid_sum_pair(const CgArgs &a, double l0, double l1, int slot, GridCtx &gc, SM &S,
+                                              double &o0, double &o1)
+{
+    const int G = gridDim.x;
+    const double c0 = block_sum<NT>(l0, S.warp);
+    const double c1 = block_sum<NT>(l1, S.warp);
+    if (threadIdx.x == 0) {
+        a.partials[slot * G + blockIdx.x] = c0;
+        a.partials[(slot + 1) * G + blockIdx.x] = c1;
+    }
+    gc.epoch++;
+    gc.ok = gc.ok && MF_GRID_BARRIER(a.bar, gc.epoch, a.status, a.budget_ns);
+    o0 = block_sum_partials<NT>(a.partials + slot * G, G, S.warp);
+    o1 = block_sum_partials<NT>(a.partials + (slot + 1) * G, G, S.warp);
+}
+
 // Four sums at once (one barrier, one batch of partial loads): slots
 // slot..slot+3 of the partials; every CTA gets the same four values.
 template <class SM>

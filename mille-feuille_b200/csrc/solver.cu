@@ -26,7 +26,7 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
         const bool small = m->v.rows <= (1 << 19) && (long long)m->v.nnz <= 16LL * m->v.rows;
         const int force = v ? atoi(v) : 0;
         const bool want = force == 1 || (force != 2 && small);
-        one_reduction = !bicg && !mixed && !hook && want;
+        one_reduction = !bicg && !mixed && !hook && want && !o.precond;
     }
     // execution layout: staged row slots for the mixed-precision
     // two-reduction CG kernel and the mixed BiCGSTAB kernel, plain row slots
@@ -139,6 +139,12 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
     a.exit_on_refine = (!bicg && mixed && o.policy != MF_POLICY_STATIC) ? 1 : 0;
     a.checkpoint_every = (hook && !bicg) ? hook->every : 0;
     a.one_reduction = (one_reduction && a.checkpoint_every == 0) ? 1 : 0;
+    if (!bicg && o.precond == 1) {
+        // Jacobi: z in a vector CG does not otherwise use, D^-1 in another
+        a.z = w.rhat;
+        a.dinv = (const double *)w.v1;
+        MF_TRY(jacobi_dinv(m, (double *)w.v1, s));
+    }
     a.budget_ns = (unsigned long long)(o.wait_budget_s * 1e9);
     a.start = 1;
     a.timing = o.phase_times ? w.timing : nullptr;
@@ -212,6 +218,8 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
         rep.bytes_moved = (long long)rep.iterations * (spmv_mixed + 36 * n) +
                           (long long)rep.refinements * (spmv_fp64 + 32 * n);
     }
+    // Jacobi: D^-1 read (FP64) and z written (vector type) every iteration
+    if (!bicg && o.precond) rep.bytes_moved += (long long)rep.iterations * (mixed ? 12 : 16) * n;
     (void)launches;
     if (a.timing) {
         std::vector<unsigned long long> t((size_t)G * 8);

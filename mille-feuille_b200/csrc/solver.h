@@ -61,7 +61,7 @@ __host__ __device__ __forceinline__ int slot_lanes(int K)
 }
 
 // Persistent solver state kept in device memory between launches.
-enum : int { S_RHO = 0, S_BETA, S_NB, S_RMAX, S_ITERS, S_REFS, S_EXIT, S_RELRES, S_ALPHA, S_OMEGA, S_COUNT };
+enum : int { S_RHO = 0, S_BETA, S_NB, S_RMAX, S_ITERS, S_REFS, S_EXIT, S_RELRES, S_ALPHA, S_OMEGA, S_RZ, S_COUNT };
 // Why a launch returned.
 enum : int { EXIT_CONVERGED = 1, EXIT_MAXITER = 2, EXIT_BREAKDOWN = 3, EXIT_CHECKPOINT = 4 };
 
@@ -107,6 +107,9 @@ struct CgArgs {
     const int2 *sdesc;             // [tilem] per strip: first slot within its chunk | slots << 16, and
                                    // the offset from a row to its own staged position (INT_MIN: none)
     double *xs;                    // padded FP64 copy of x that the refinement SpMV stages
+    // Jacobi-preconditioned CG (null otherwise)
+    void *z;                       // z = D^-1 r (solver's vector type)
+    const double *dinv;            // [rows] 1 / diagonal (1 where the diagonal is 0)
 };
 
 struct SolverWork {
@@ -144,6 +147,8 @@ mf_status pack_slots(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s);
 // tells whether every chunk qualified (otherwise the chunks are plain)
 mf_status build_slot_chunks(mf_matrix m, int G, bool staged, cudaStream_t s);
 mf_status true_residual(mf_matrix m, const double *b, const double *x, SolverWork &w, double *relres, cudaStream_t s);
+// Jacobi preconditioner: dinv[i] = 1 / a_ii (1 where the diagonal is 0)
+mf_status jacobi_dinv(mf_matrix m, double *dinv, cudaStream_t s);
 // payload.cu
 mf_status pack_payload(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s);
 mf_status static_working_classes(mf_matrix m, unsigned char *d_wcls, cudaStream_t s);

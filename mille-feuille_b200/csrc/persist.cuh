@@ -737,46 +737,72 @@ struct __align__(16) StagedSmem {
     double res;
 };
 
-// Thread 0: stage chunk c into stage k: slot offsets, positions, the values
-// when STV (FP64 values for PK 0, mixed headers and payload for PK 1), and
-// the chunk's column runs of v0 (and v1 when NV is 2).  The caller has
-// fenced the vectors (see spmv_staged).
+// Warp 0 (all 32 lanes): stage chunk c into stage k: strip descriptors, slot
+// positions, the values when STV (FP64 values for PK 0, mixed headers and
+// payload for PK 1), and the chunk's column runs of v0 (and v1 when NV is 2).
+// One copy per lane: lane 0 the descriptors, 1 the positions, 2 the values or
+// headers, 3 the payload, 4 + j run j of v0, 4 + SC_RUNS + j run j of v1; the
+// byte total is summed across the warp and lane 0 posts it on the stage's
+// mbarrier before any copy is issued.  Lanes 0..27 also copy the chunk record
+// into the stage header.  The caller has fenced the vectors (see
+// spmv_staged).
 template <int PK, bool STV, typename VT, int NV, bool MIX>
-__device__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S, int c, int k, const VT *v0, const VT *v1)
+__device__ __forceinline__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S, int cb, int c, int k, const VT *v0,
+                                             const VT *v1)
 {
     using C = StagedCfg<MIX>;
-    const int cb = a.scta_chunk[blockIdx.x];
+    static_assert(4 + 2 * SC_RUNS <= 32, "one copy per lane");
+    constexpr int RW = (int)(sizeof(SlotChunk) / 4);
+    static_assert(sizeof(SlotChunk) % 4 == 0 && RW <= 32, "the record is copied one word per lane");
+    const int lane = threadIdx.x & 31;
+    const SlotChunk *src = c - cb < TRECS ? &S.recs[c - cb] : &a.schunks[c];
     SlotHdr &h = S.hdr[k];
-    if (c - cb < TRECS) h.rec = S.recs[c - cb];
-    else h.rec = a.schunks[c];
-    const SlotChunk &r = h.rec;  // read in place (shared memory), not copied to local memory
     unsigned char *st = S.stage[k];
-    const long long m0 = 2ll * MF_TILE * r.k0, m1 = 2ll * MF_TILE * r.k1;
-    unsigned total = range_bytes(8ll * r.s0, 8ll * r.s1) + range_bytes(m0, m1);
-    if (STV) {
-        if (PK == 0) total += range_bytes(8ll * MF_TILE * r.k0, 8ll * MF_TILE * r.k1);
-        else total += range_bytes(4ll * r.k0, 4ll * (r.k1 + 1)) + range_bytes(r.y0, r.y1);
+    if (lane < RW) ((int *)&h.rec)[lane] = ((const int *)src)[lane];
+    const unsigned char *g = nullptr;
+    unsigned char *d = nullptr;
+    long long a0 = 0, a1 = 0;
+    int *shift = nullptr;
+    if (lane == 0) {
+        g = (const unsigned char *)a.sdesc, d = st + C::OFF_SDESC, a0 = 8ll * src->s0, a1 = 8ll * src->s1;
+        shift = &h.sh_sslot;
+    } else if (lane == 1) {
+        g = (const unsigned char *)a.spos, d = st + C::OFF_META;
+        a0 = 2ll * MF_TILE * src->k0, a1 = 2ll * MF_TILE * src->k1;
+        shift = &h.sh_meta;
+    } else if (lane == 2 && STV) {
+        d = st + C::OFF_DATA;
+        shift = &h.sh_data;
+        if (PK == 0) g = (const unsigned char *)a.sval, a0 = 8ll * MF_TILE * src->k0, a1 = 8ll * MF_TILE * src->k1;
+        else g = (const unsigned char *)a.shdr, a0 = 4ll * src->k0, a1 = 4ll * (src->k1 + 1);
+    } else if (lane == 3 && STV && PK == 1) {
+        g = a.spay, d = st + C::OFF_PAY, a0 = src->y0, a1 = src->y1;
+        shift = &h.sh_pay;
     }
-    for (int j = 0; j < r.nrun; j++) total += (unsigned)(NV * r.rl[j] * (int)sizeof(VT));
+    // a range copy: whole 16-byte words around [a0, a1), the shift to a0
+    if (shift) {
+        const long long c0 = a0 & ~15ll, c1 = (a1 + 15) & ~15ll;
+        *shift = (int)(a0 - c0);
+        g += c0;
+        a1 = c1 - c0;
+    }
+    const int j = lane - 4 - (lane >= 4 + SC_RUNS ? SC_RUNS : 0);
+    if (lane >= 4 && (NV == 2 || lane < 4 + SC_RUNS) && j < src->nrun) {
+        const VT *v = lane < 4 + SC_RUNS ? v0 : v1;
+        g = (const unsigned char *)(v + src->rg[j]);
+        d = st + C::OFF_VEC + (size_t)((lane < 4 + SC_RUNS ? 0 : SC_XCAP) + src->rs[j]) * sizeof(VT);
+        a1 = (long long)src->rl[j] * (long long)sizeof(VT);
+    }
+    const unsigned bytes = g ? (unsigned)a1 : 0u;
+    unsigned total = bytes;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
     fence_proxy_async_smem();
-    mbar_arrive_expect_tx(&S.bar[k], total);
-    add_range(st + C::OFF_SDESC, (const unsigned char *)a.sdesc, 8ll * r.s0, 8ll * r.s1, &S.bar[k], h.sh_sslot);
-    add_range(st + C::OFF_META, (const unsigned char *)a.spos, m0, m1, &S.bar[k], h.sh_meta);
-    if (STV) {
-        if (PK == 0) {
-            add_range(st + C::OFF_DATA, (const unsigned char *)a.sval, 8ll * MF_TILE * r.k0, 8ll * MF_TILE * r.k1,
-                      &S.bar[k], h.sh_data);
-        } else {
-            add_range(st + C::OFF_DATA, (const unsigned char *)a.shdr, 4ll * r.k0, 4ll * (r.k1 + 1), &S.bar[k],
-                      h.sh_data);
-            add_range(st + C::OFF_PAY, a.spay, r.y0, r.y1, &S.bar[k], h.sh_pay);
-        }
-    }
-    VT *sv = (VT *)(st + C::OFF_VEC);
-    for (int j = 0; j < r.nrun; j++) {
-        const unsigned bytes = (unsigned)(r.rl[j] * (int)sizeof(VT));
-        bulk_g2s(sv + r.rs[j], v0 + r.rg[j], bytes, &S.bar[k]);
-        if (NV == 2) bulk_g2s(sv + SC_XCAP + r.rs[j], v1 + r.rg[j], bytes, &S.bar[k]);
+    if (lane == 0) mbar_arrive_expect_tx(&S.bar[k], total);
+    __syncwarp();
+    if (bytes) {
+        if (shift) bulk_g2s_hint(d, g, bytes, &S.bar[k], l2_policy_evict_first());
+        else bulk_g2s(d, g, bytes, &S.bar[k]);
     }
 }
 
@@ -896,13 +922,13 @@ __device__ bool spmv_staged(const CgArgs &a, StagedSmem<MIX> &S, GridCtx &gc, in
     }
     const MfTiles &A = a.A;
     const int tid = threadIdx.x, hw = tid >> 4, hl = tid & 15;
-    if (tid == 0) {
+    if (tid < 32) {
         // the vectors were written earlier in this kernel by ordinary stores
         // of other CTAs, made visible here by the grid barrier; the proxy
         // fence orders them before the bulk copies, which read through the
         // async proxy.  They do not change during the pass.
         asm volatile("fence.proxy.async.global;\n" ::: "memory");
-        for (int j = 0; j < NSTG && cb + j < ce; j++) issue_staged<PK, STV, VT, NV>(a, S, cb + j, j, v0, v1);
+        for (int j = 0; j < NSTG && cb + j < ce; j++) issue_staged<PK, STV, VT, NV>(a, S, cb, cb + j, j, v0, v1);
     }
     // copies of chunks [c0, c0 + n) may be in flight: wait for them
     // (bounded) before leaving, each with the parity its stage expects
@@ -1004,7 +1030,7 @@ __device__ bool spmv_staged(const CgArgs &a, StagedSmem<MIX> &S, GridCtx &gc, in
         }
         if (c + 1 < ce) gc.par ^= 1u << kn;
         // every thread is done with stage k
-        if (tid == 0 && c + NSTG < ce) issue_staged<PK, STV, VT, NV>(a, S, c + NSTG, k, v0, v1);
+        if (tid < 32 && c + NSTG < ce) issue_staged<PK, STV, VT, NV>(a, S, cb, c + NSTG, k, v0, v1);
         MF_TSUB(7);
     }
 #undef MF_TSUB

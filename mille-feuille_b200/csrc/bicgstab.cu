@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(NT, LAY == 0 ? MINB : LAY == 1 ? SMINB : MF_ST
     gc.par = 0u;
     double *st = a.state;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < (LAY == 0 ? 2 : NSTG); i++) mbar_init(&S.bar[i], 1);
+        for (int i = 0; i < (LAY == 0 ? 2 : NSTG); i++) mbar_init(&S.bar[i], LAY == 2 ? STAGED_ARRIVALS : 1);
         mbar_fence_init();
     }
     if constexpr (LAY == 0) {

@@ -737,63 +737,70 @@ struct __align__(16) StagedSmem {
     double res;
 };
 
-// Warp 0 (all 32 lanes): stage chunk c into stage k: strip descriptors, slot
-// positions, the values when STV (FP64 values for PK 0, mixed headers and
-// payload for PK 1), and the chunk's column runs of v0 (and v1 when NV is 2).
-// One copy per lane: lane 0 the descriptors, 1 the positions, 2 the values or
-// headers, 3 the payload, 4 + j run j of v0, 4 + SC_RUNS + j run j of v1; the
-// byte total is summed across the warp and lane 0 posts it on the stage's
-// mbarrier before any copy is issued.  Lanes 0..27 also copy the chunk record
-// into the stage header.  The caller has fenced the vectors (see
-// spmv_staged).
+// Warps 0 and 1 (all lanes of both): stage chunk c into stage k.  Warp 0
+// copies the chunk record into the stage header and issues the range copies
+// (lane 0 strip descriptors, 1 slot positions, 2 the values (PK 0) or mixed
+// headers (PK 1) when STV, 3 the mixed payload when STV); warp 1 issues the
+// chunk's column runs (lane j < nrun: run j of v0, nrun <= j < 2 nrun when NV
+// is 2: run j - nrun of v1).  Each warp sums its bytes across its lanes and
+// its lane 0 arrives on the stage's mbarrier with them as expected
+// transactions before the warp issues a copy, so the phase (two arrivals)
+// completes only when both warps' copies have landed.  The caller has
+// fenced the vectors (see spmv_staged).
+constexpr int STAGED_ARRIVALS = 2;
 template <int PK, bool STV, typename VT, int NV, bool MIX>
 __device__ __forceinline__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S, int cb, int c, int k, const VT *v0,
                                              const VT *v1)
 {
     using C = StagedCfg<MIX>;
-    static_assert(4 + 2 * SC_RUNS <= 32, "one copy per lane");
+    static_assert(NV * SC_RUNS <= 32, "one run copy per lane");
     constexpr int RW = (int)(sizeof(SlotChunk) / 4);
     static_assert(sizeof(SlotChunk) % 4 == 0 && RW <= 32, "the record is copied one word per lane");
     const int lane = threadIdx.x & 31;
+    const bool runs = threadIdx.x >= 32;
     const SlotChunk *src = c - cb < TRECS ? &S.recs[c - cb] : &a.schunks[c];
-    SlotHdr &h = S.hdr[k];
     unsigned char *st = S.stage[k];
-    if (lane < RW) ((int *)&h.rec)[lane] = ((const int *)src)[lane];
     const unsigned char *g = nullptr;
     unsigned char *d = nullptr;
-    long long a0 = 0, a1 = 0;
-    int *shift = nullptr;
-    if (lane == 0) {
-        g = (const unsigned char *)a.sdesc, d = st + C::OFF_SDESC, a0 = 8ll * src->s0, a1 = 8ll * src->s1;
-        shift = &h.sh_sslot;
-    } else if (lane == 1) {
-        g = (const unsigned char *)a.spos, d = st + C::OFF_META;
-        a0 = 2ll * MF_TILE * src->k0, a1 = 2ll * MF_TILE * src->k1;
-        shift = &h.sh_meta;
-    } else if (lane == 2 && STV) {
-        d = st + C::OFF_DATA;
-        shift = &h.sh_data;
-        if (PK == 0) g = (const unsigned char *)a.sval, a0 = 8ll * MF_TILE * src->k0, a1 = 8ll * MF_TILE * src->k1;
-        else g = (const unsigned char *)a.shdr, a0 = 4ll * src->k0, a1 = 4ll * (src->k1 + 1);
-    } else if (lane == 3 && STV && PK == 1) {
-        g = a.spay, d = st + C::OFF_PAY, a0 = src->y0, a1 = src->y1;
-        shift = &h.sh_pay;
+    unsigned bytes = 0;
+    if (!runs) {
+        SlotHdr &h = S.hdr[k];
+        if (lane < RW) ((int *)&h.rec)[lane] = ((const int *)src)[lane];
+        long long a0 = 0, a1 = 0;
+        int *shift = nullptr;
+        if (lane == 0) {
+            g = (const unsigned char *)a.sdesc, d = st + C::OFF_SDESC, a0 = 8ll * src->s0, a1 = 8ll * src->s1;
+            shift = &h.sh_sslot;
+        } else if (lane == 1) {
+            g = (const unsigned char *)a.spos, d = st + C::OFF_META;
+            a0 = 2ll * MF_TILE * src->k0, a1 = 2ll * MF_TILE * src->k1;
+            shift = &h.sh_meta;
+        } else if (lane == 2 && STV) {
+            d = st + C::OFF_DATA;
+            shift = &h.sh_data;
+            if (PK == 0) g = (const unsigned char *)a.sval, a0 = 8ll * MF_TILE * src->k0, a1 = 8ll * MF_TILE * src->k1;
+            else g = (const unsigned char *)a.shdr, a0 = 4ll * src->k0, a1 = 4ll * (src->k1 + 1);
+        } else if (lane == 3 && STV && PK == 1) {
+            g = a.spay, d = st + C::OFF_PAY, a0 = src->y0, a1 = src->y1;
+            shift = &h.sh_pay;
+        }
+        // whole 16-byte words around [a0, a1); the shift locates a0
+        if (shift) {
+            const long long c0 = a0 & ~15ll, c1 = (a1 + 15) & ~15ll;
+            *shift = (int)(a0 - c0);
+            g += c0;
+            bytes = (unsigned)(c1 - c0);
+        }
+    } else {
+        const int nrun = src->nrun;
+        if (lane < NV * nrun) {
+            const bool second = lane >= nrun;
+            const int j = second ? lane - nrun : lane;
+            g = (const unsigned char *)((second ? v1 : v0) + src->rg[j]);
+            d = st + C::OFF_VEC + (size_t)((second ? SC_XCAP : 0) + src->rs[j]) * sizeof(VT);
+            bytes = (unsigned)src->rl[j] * (unsigned)sizeof(VT);
+        }
     }
-    // a range copy: whole 16-byte words around [a0, a1), the shift to a0
-    if (shift) {
-        const long long c0 = a0 & ~15ll, c1 = (a1 + 15) & ~15ll;
-        *shift = (int)(a0 - c0);
-        g += c0;
-        a1 = c1 - c0;
-    }
-    const int j = lane - 4 - (lane >= 4 + SC_RUNS ? SC_RUNS : 0);
-    if (lane >= 4 && (NV == 2 || lane < 4 + SC_RUNS) && j < src->nrun) {
-        const VT *v = lane < 4 + SC_RUNS ? v0 : v1;
-        g = (const unsigned char *)(v + src->rg[j]);
-        d = st + C::OFF_VEC + (size_t)((lane < 4 + SC_RUNS ? 0 : SC_XCAP) + src->rs[j]) * sizeof(VT);
-        a1 = (long long)src->rl[j] * (long long)sizeof(VT);
-    }
-    const unsigned bytes = g ? (unsigned)a1 : 0u;
     unsigned total = bytes;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
@@ -801,7 +808,7 @@ __device__ __forceinline__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S
     if (lane == 0) mbar_arrive_expect_tx(&S.bar[k], total);
     __syncwarp();
     if (bytes) {
-        if (shift) bulk_g2s_hint(d, g, bytes, &S.bar[k], l2_policy_evict_first());
+        if (!runs) bulk_g2s_hint(d, g, bytes, &S.bar[k], l2_policy_evict_first());
         else bulk_g2s(d, g, bytes, &S.bar[k]);
     }
 }
@@ -922,7 +929,7 @@ __device__ bool spmv_staged(const CgArgs &a, StagedSmem<MIX> &S, GridCtx &gc, in
     }
     const MfTiles &A = a.A;
     const int tid = threadIdx.x, hw = tid >> 4, hl = tid & 15;
-    if (tid < 32) {
+    if (tid < 64) {
         // the vectors were written earlier in this kernel by ordinary stores
         // of other CTAs, made visible here by the grid barrier; the proxy
         // fence orders them before the bulk copies, which read through the
@@ -1030,7 +1037,7 @@ __device__ bool spmv_staged(const CgArgs &a, StagedSmem<MIX> &S, GridCtx &gc, in
         }
         if (c + 1 < ce) gc.par ^= 1u << kn;
         // every thread is done with stage k
-        if (tid < 32 && c + NSTG < ce) issue_staged<PK, STV, VT, NV>(a, S, cb, c + NSTG, k, v0, v1);
+        if (tid < 64 && c + NSTG < ce) issue_staged<PK, STV, VT, NV>(a, S, cb, c + NSTG, k, v0, v1);
         MF_TSUB(7);
     }
 #undef MF_TSUB

@@ -737,17 +737,23 @@ struct __align__(16) StagedSmem {
     double res;
 };
 
-// Warps 0 and 1 (all lanes of both): stage chunk c into stage k.  Warp 0
-// copies the chunk record into the stage header and issues the range copies
-// (lane 0 strip descriptors, 1 slot positions, 2 the values (PK 0) or mixed
-// headers (PK 1) when STV, 3 the mixed payload when STV); warp 1 issues the
-// chunk's column runs (lane j < nrun: run j of v0, nrun <= j < 2 nrun when NV
-// is 2: run j - nrun of v1).  Each warp sums its bytes across its lanes and
-// its lane 0 arrives on the stage's mbarrier with them as expected
-// transactions before the warp issues a copy, so the phase (two arrivals)
-// completes only when both warps' copies have landed.  The caller has
-// fenced the vectors (see spmv_staged).
-constexpr int STAGED_ARRIVALS = 2;
+// The first STAGED_ARRIVALS warps (all their lanes) stage chunk c into
+// stage k.  With 2 warps, warp 0 copies the chunk record into the stage
+// header and issues the range copies (range 0 strip descriptors, 1 slot
+// positions, 2 the values (PK 0) or mixed headers (PK 1) when STV, 3 the
+// mixed payload when STV; lane i issues range i) and warp 1 the chunk's
+// column runs (lane j < nrun: run j of v0, nrun <= j < 2 nrun when NV is 2:
+// run j - nrun of v1).  With 4 warps, warp 0 takes the record and ranges 0-1,
+// warp 1 ranges 2-3, warp 2 the runs of v0 and warp 3 those of v1.  Each
+// warp sums its bytes across its lanes and its lane 0 arrives on the stage's
+// mbarrier with them as expected transactions before the warp issues a copy,
+// so the phase (one arrival per warp) completes only when every warp's
+// copies have landed.  The caller has fenced the vectors (see spmv_staged).
+#ifndef MF_STAGED_ISSUE_WARPS
+#define MF_STAGED_ISSUE_WARPS 4
+#endif
+constexpr int STAGED_ARRIVALS = MF_STAGED_ISSUE_WARPS;
+static_assert(STAGED_ARRIVALS == 2 || STAGED_ARRIVALS == 4, "the refill runs on 2 or 4 warps");
 template <int PK, bool STV, typename VT, int NV, bool MIX>
 __device__ __forceinline__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S, int cb, int c, int k, const VT *v0,
                                              const VT *v1)
@@ -756,8 +762,9 @@ __device__ __forceinline__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S
     static_assert(NV * SC_RUNS <= 32, "one run copy per lane");
     constexpr int RW = (int)(sizeof(SlotChunk) / 4);
     static_assert(sizeof(SlotChunk) % 4 == 0 && RW <= 32, "the record is copied one word per lane");
-    const int lane = threadIdx.x & 31;
-    const bool runs = threadIdx.x >= 32;
+    constexpr int W = STAGED_ARRIVALS;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const bool runs = W == 2 ? wp == 1 : wp >= 2;
     const SlotChunk *src = c - cb < TRECS ? &S.recs[c - cb] : &a.schunks[c];
     unsigned char *st = S.stage[k];
     const unsigned char *g = nullptr;
@@ -765,22 +772,23 @@ __device__ __forceinline__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S
     unsigned bytes = 0;
     if (!runs) {
         SlotHdr &h = S.hdr[k];
-        if (lane < RW) ((int *)&h.rec)[lane] = ((const int *)src)[lane];
+        if (wp == 0 && lane < RW) ((int *)&h.rec)[lane] = ((const int *)src)[lane];
+        const int rid = W == 2 ? lane : wp == 0 ? (lane < 2 ? lane : 4) : lane + 2;  // the range of this lane
         long long a0 = 0, a1 = 0;
         int *shift = nullptr;
-        if (lane == 0) {
+        if (rid == 0) {
             g = (const unsigned char *)a.sdesc, d = st + C::OFF_SDESC, a0 = 8ll * src->s0, a1 = 8ll * src->s1;
             shift = &h.sh_sslot;
-        } else if (lane == 1) {
+        } else if (rid == 1) {
             g = (const unsigned char *)a.spos, d = st + C::OFF_META;
             a0 = 2ll * MF_TILE * src->k0, a1 = 2ll * MF_TILE * src->k1;
             shift = &h.sh_meta;
-        } else if (lane == 2 && STV) {
+        } else if (rid == 2 && STV) {
             d = st + C::OFF_DATA;
             shift = &h.sh_data;
             if (PK == 0) g = (const unsigned char *)a.sval, a0 = 8ll * MF_TILE * src->k0, a1 = 8ll * MF_TILE * src->k1;
             else g = (const unsigned char *)a.shdr, a0 = 4ll * src->k0, a1 = 4ll * (src->k1 + 1);
-        } else if (lane == 3 && STV && PK == 1) {
+        } else if (rid == 3 && STV && PK == 1) {
             g = a.spay, d = st + C::OFF_PAY, a0 = src->y0, a1 = src->y1;
             shift = &h.sh_pay;
         }
@@ -793,9 +801,11 @@ __device__ __forceinline__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S
         }
     } else {
         const int nrun = src->nrun;
-        if (lane < NV * nrun) {
-            const bool second = lane >= nrun;
-            const int j = second ? lane - nrun : lane;
+        // copy q: run q of v0 (q < nrun) or run q - nrun of v1
+        const int q = W == 2 ? lane : wp == 3 ? lane + nrun : lane;
+        if (W == 2 ? lane < NV * nrun : lane < nrun && (wp == 2 || NV == 2)) {
+            const bool second = q >= nrun;
+            const int j = second ? q - nrun : q;
             g = (const unsigned char *)((second ? v1 : v0) + src->rg[j]);
             d = st + C::OFF_VEC + (size_t)((second ? SC_XCAP : 0) + src->rs[j]) * sizeof(VT);
             bytes = (unsigned)src->rl[j] * (unsigned)sizeof(VT);
@@ -805,7 +815,10 @@ __device__ __forceinline__ void issue_staged(const CgArgs &a, StagedSmem<MIX> &S
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
     fence_proxy_async_smem();
-    if (lane == 0) mbar_arrive_expect_tx(&S.bar[k], total);
+    if (lane == 0) {
+        if (total) mbar_arrive_expect_tx(&S.bar[k], total);
+        else mbar_arrive(&S.bar[k]);  // nothing to copy for this warp
+    }
     __syncwarp();
     if (bytes) {
         if (!runs) bulk_g2s_hint(d, g, bytes, &S.bar[k], l2_policy_evict_first());
@@ -929,7 +942,7 @@ __device__ bool spmv_staged(const CgArgs &a, StagedSmem<MIX> &S, GridCtx &gc, in
     }
     const MfTiles &A = a.A;
     const int tid = threadIdx.x, hw = tid >> 4, hl = tid & 15;
-    if (tid < 64) {
+    if (tid < 32 * STAGED_ARRIVALS) {
         // the vectors were written earlier in this kernel by ordinary stores
         // of other CTAs, made visible here by the grid barrier; the proxy
         // fence orders them before the bulk copies, which read through the
@@ -1037,7 +1050,7 @@ __device__ bool spmv_staged(const CgArgs &a, StagedSmem<MIX> &S, GridCtx &gc, in
         }
         if (c + 1 < ce) gc.par ^= 1u << kn;
         // every thread is done with stage k
-        if (tid < 64 && c + NSTG < ce) issue_staged<PK, STV, VT, NV>(a, S, cb, c + NSTG, k, v0, v1);
+        if (tid < 32 * STAGED_ARRIVALS && c + NSTG < ce) issue_staged<PK, STV, VT, NV>(a, S, cb, c + NSTG, k, v0, v1);
         MF_TSUB(7);
     }
 #undef MF_TSUB

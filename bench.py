@@ -69,13 +69,17 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel):
-    """Per-iteration DRAM bytes of `kernel` from the committed ncu summary."""
+def ncu_traffic(kernel, workload, policy):
+    """Per-iteration DRAM bytes of `kernel` from the committed ncu summary,
+    only when that capture ran the same workload and precision policy (the
+    figure belongs to one matrix and one payload)."""
     p = ROOT / "profiles" / "ncu_traffic.json"
     if not p.exists():
         return None
-    d = json.loads(p.read_text())
-    return d.get(kernel)
+    e = json.loads(p.read_text()).get(kernel)
+    if e is None or e.get("workload") != workload or e.get("policy") != policy:
+        return None
+    return e
 
 
 class ClockSampler:
@@ -209,7 +213,7 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"poisson3d_scaled_{GRID}^3 CG to 1e-10", "n": A.n_rows, "nnz": A.nnz, "seed": SEED,
-                   "l2": "inputs larger than L2", "reference_setup_s": cpu.setup_s},
+                   "l2": "host cores only (no device cache involved)", "reference_setup_s": cpu.setup_s},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cpu.threads, "kind": "reference",
                          "sample": f"{per_step} CG iterations per step (reference blockspmv_cpu, serial, "
                                    f"+ OpenMP vector loops), scaled by {iters} FP64 iterations to 1e-10"},
@@ -219,17 +223,39 @@ def run_reference(args):
     return 0
 
 
+L2_FLUSH_BYTES = 256 << 20  # twice the B200's 126 MB L2
+L2_NOTE = "L2 flushed (256 MB write) before every timed step, outside its timed events"
+
+_flush_buf = None
+
+
+def _flush_l2(stream):
+    """Overwrites a buffer twice the L2 size on `stream`, so that no input of
+    the next step is served from L2."""
+    import torch
+
+    global _flush_buf
+    if _flush_buf is None:
+        _flush_buf = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    with torch.cuda.stream(stream):
+        _flush_buf.fill_(1)
+
+
 def _timed(stream, fn, steps):
-    """Device time of `steps` calls of fn (CUDA events on the launching stream)."""
+    """Device time of `steps` calls of fn: CUDA events on the launching stream
+    around each call, L2 flushed before each (outside the events)."""
     import torch
 
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
+    total = 0.0
     for _ in range(steps):
+        _flush_l2(stream)
+        ev0.record(stream)
         fn()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    return ev0.elapsed_time(ev1)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        total += ev0.elapsed_time(ev1)
+    return total
 
 
 def _max_over_ranks(v, world):
@@ -343,7 +369,7 @@ def workload_single(args, mf, world, local):
             "iterations": int(statistics.mean(iters)), "refinements": int(rep.refinements),
             "relres_true": relres_true, "max_abs_err_vs_xstar": x_err, "setup_ms": setup_ms,
             "parallelism": f"replicas x{world}",
-            "l2": "inputs larger than L2 (matrix > 126 MB L2); no flush"}
+            "l2": L2_NOTE}
     # the plain FP64 tiled solve of the same system, same box, same run
     if args.policy != "fp64" and not args.iters:
         rep64 = mf.SolveReport()
@@ -371,13 +397,17 @@ def workload_single(args, mf, world, local):
     fn_host(M.h, b_pin.data_ptr(), x_pin.data_ptr(), C.byref(o), C.byref(erep))
     torch.cuda.synchronize()
     _barrier(world)
-    t0 = time.perf_counter()
+    e2e_s = 0.0
     for _ in range(args.steps):
+        _flush_l2(stream)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         st = fn_host(M.h, b_pin.data_ptr(), x_pin.data_ptr(), C.byref(o), C.byref(erep))
         if st != 0:
             mf.check(st)
-    torch.cuda.synchronize()
-    e2e_s = _max_over_ranks(time.perf_counter() - t0, world)
+        torch.cuda.synchronize()
+        e2e_s += time.perf_counter() - t0
+    e2e_s = _max_over_ranks(e2e_s, world)
     result["e2e"] = {"value": args.steps * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                      "d2h_bytes_per_step": 8 * n}
     mean_ms = statistics.mean(kernel_ms)
@@ -452,7 +482,7 @@ def workload_batched(args, mf, world, local):
             "iterations_mean": float(its.mean()), "iterations_max": int(its.max()),
             "relres_true_max": float(rep.relres_true_max), "failed": int(rep.failed), "setup_ms": setup_ms,
             "lanes_per_row": int(rep.lanes_per_row), "cluster_ctas": int(rep.cluster_ctas),
-            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2; no flush"}
+            "parallelism": f"replicas x{world}", "l2": L2_NOTE}
     # the plain FP64 tiled solves of the same systems, one after another
     if not args.no_fp64_baseline:
         dbs = [torch.from_numpy(bv).cuda() for bv in bs]
@@ -477,13 +507,17 @@ def workload_batched(args, mf, world, local):
     b_pin = torch.from_numpy(bstack).pin_memory()
     x_pin = torch.zeros_like(b_pin).pin_memory()
     _barrier(world)
-    t0 = time.perf_counter()
+    e2e_s = 0.0
     for _ in range(args.steps):
+        _flush_l2(stream)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         db.copy_(b_pin, non_blocking=True)
         solve()
         x_pin.copy_(dx, non_blocking=True)
         torch.cuda.synchronize()
-    e2e_s = _max_over_ranks(time.perf_counter() - t0, world)
+        e2e_s += time.perf_counter() - t0
+    e2e_s = _max_over_ranks(e2e_s, world)
     result["e2e"] = {"value": N * args.steps * world / e2e_s, "unit": UNIT,
                      "h2d_bytes_per_step": 8 * len(bstack), "d2h_bytes_per_step": 8 * len(bstack)}
     result["roofline_in"] = (alg, statistics.mean(kernel_ms), "k_batched_cg", None)
@@ -522,7 +556,7 @@ def run_mf(args):
     peak, peak_kind = load_peaks()
     per_launch, mean_ms, kname, mean_iters = res["roofline_in"]
     achieved = per_launch / (mean_ms * 1e-3) / 1e9
-    tr = ncu_traffic(kname)
+    tr = ncu_traffic(kname, args.workload, args.policy)
     traffic = None
     if tr is not None and mean_iters is not None:
         traffic = tr["dram_bytes_per_iteration"] * mean_iters

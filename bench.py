@@ -527,6 +527,102 @@ def workload_batched(args, mf, world, local):
     return result, info
 
 
+def workload_multi(args, mf, world, local):
+    """k right-hand sides of the poisson3d system solved together by
+    mf_cg_solve_multi (FP64, one pass over the matrix per iteration for all
+    of them); value = right-hand sides solved per second."""
+    import torch
+
+    L = mf.lib()
+    k = args.rhs
+    A = mf.synth_poisson3d_scaled(GRID, SEED)
+    n = A.n_rows
+    B = np.stack([A.matvec(mf.synth_xstar(SEED + j, n)) for j in range(k)])  # k x n: column-major n x k
+    t0 = time.perf_counter()
+    M = mf.Matrix(A)
+    torch.cuda.synchronize()
+    setup_ms = (time.perf_counter() - t0) * 1e3
+    dB = torch.from_numpy(B).cuda()
+    dX = torch.zeros((k, n), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    reps = (mf.SolveReport * k)()
+    o = (mf.solve_opts(tol=-1.0, maxiter=args.iters) if args.iters else mf.solve_opts(tol=TOL, maxiter=50000))
+
+    def solve():
+        st = L.mf_cg_solve_multi(M.h, k, dB.data_ptr(), n, dX.data_ptr(), n, C.byref(o), reps, stream.cuda_stream)
+        if st != 0:
+            mf.check(st)
+
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize()
+    _barrier(world)
+    launches0 = L.mf_kernel_launches()
+    kernel_ms, bytes_moved, iters = [], [], []
+
+    def step():
+        solve()
+        kernel_ms.append(reps[0].kernel_ms)
+        bytes_moved.append(reps[0].bytes_moved)
+        iters.append(max(r.iterations for r in reps))
+
+    with ClockSampler(local) as clk:
+        ms = _timed(stream, step, args.steps)
+    launches = L.mf_kernel_launches() - launches0
+    ms = _max_over_ranks(ms, world)
+    value = k * args.steps * world / (ms * 1e-3)
+    result = {"ms": ms, "value": value, "launches": launches, "clocks": clk.summary()}
+    if args.profile:
+        return result, None
+    its = [r.iterations for r in reps]
+    info = {"workload": f"poisson3d_scaled_{GRID}^3, {k} right-hand sides (x* seeds {SEED}-{SEED + k - 1}) "
+                        f"CG to 1e-10 together", "n": n, "nnz": A.nnz, "rhs": k, "policy": "fp64",
+            "iterations_min": min(its), "iterations_max": max(its),
+            "relres_true_max": max(r.relres_true for r in reps), "setup_ms": setup_ms,
+            "parallelism": f"replicas x{world}", "l2": L2_NOTE}
+    if not args.no_fp64_baseline:
+        rep1 = mf.SolveReport()
+        db1 = dB[0].contiguous()
+        dx1 = torch.zeros(n, dtype=torch.float64, device="cuda")
+        o1 = mf.solve_opts(tol=TOL, maxiter=50000, policy="fp64")
+
+        def s1():
+            st = L.mf_cg_solve(M.h, db1.data_ptr(), dx1.data_ptr(), C.byref(o1), C.byref(rep1), None,
+                               stream.cuda_stream)
+            if st != 0:
+                mf.check(st)
+
+        s1()
+        torch.cuda.synchronize()
+        ms1 = _max_over_ranks(_timed(stream, s1, 3), world)
+        info["fp64_single"] = {"value": 3 * world / (ms1 * 1e-3), "unit": UNIT, "iterations": rep1.iterations,
+                               "what": "the first right-hand side alone by the single-vector FP64 CG"}
+    # e2e: pinned host B in and X out every step through mf_cg_solve_multi_host
+    b_pin = torch.from_numpy(B).pin_memory()
+    x_pin = torch.zeros((k, n), dtype=torch.float64).pin_memory()
+    ereps = (mf.SolveReport * k)()
+    L.mf_cg_solve_multi_host(M.h, k, b_pin.data_ptr(), x_pin.data_ptr(), C.byref(o), ereps)
+    _barrier(world)
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        _flush_l2(stream)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = L.mf_cg_solve_multi_host(M.h, k, b_pin.data_ptr(), x_pin.data_ptr(), C.byref(o), ereps)
+        if st != 0:
+            mf.check(st)
+        e2e_s += time.perf_counter() - t0
+    e2e_s = _max_over_ranks(e2e_s, world)
+    result["e2e"] = {"value": k * args.steps * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * n * k,
+                     "d2h_bytes_per_step": 8 * n * k}
+    result["roofline_in"] = (statistics.mean(bytes_moved), statistics.mean(kernel_ms), "k_mr_spmm+k_mr_update+"
+                             "k_mr_pupdate (multi-RHS FP64 CG)", statistics.mean(iters))
+    result["dtype"] = "f64"
+    result["cpu"] = None
+    M.close()
+    return result, info
+
+
 def run_mf(args):
     import torch
     import torch.distributed as dist
@@ -544,6 +640,8 @@ def run_mf(args):
     mf = ge.load_package()
     if args.workload == "batched":
         res, info = workload_batched(args, mf, world, local)
+    elif args.workload == "multirhs":
+        res, info = workload_multi(args, mf, world, local)
     else:
         res, info = workload_single(args, mf, world, local)
     if args.profile:
@@ -594,7 +692,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mf", "reference"], default="mf")
-    ap.add_argument("--workload", default="poisson3d", choices=["poisson3d", "lap2d", "batched", "convdiff", "aniso"])
+    ap.add_argument("--workload", default="poisson3d",
+                    choices=["poisson3d", "lap2d", "batched", "convdiff", "aniso", "multirhs"])
+    ap.add_argument("--rhs", type=int, default=16, help="multirhs workload: right-hand sides (1-16)")
     ap.add_argument("--policy", default="static", choices=["fp64", "static", "rule", "learned"])
     ap.add_argument("--policy-file", default=None, help="learned policy (mf_policy_save format)")
     ap.add_argument("--no-fp64-baseline", action="store_true")

@@ -221,6 +221,36 @@ mf_status mf_bicgstab_solve_host(mf_matrix m, const double *b_host, double *x_ho
                                  const mf_solve_opts *opts, mf_solve_report *report);
 
 /* ---------------------------------------------------------------------- */
+/* Several right-hand sides at once (no reference counterpart)             */
+/* ---------------------------------------------------------------------- */
+
+/* Y = A X for k columns (1 <= k <= 16) in FP64, one pass over the matrix for
+ * all of them.  X (cols x k) and Y (rows x k) are device arrays, column-major
+ * with leading dimensions ldx >= cols and ldy >= rows.  Column j of Y equals
+ * mf_spmv of column j of X bit for bit (the same blockspmv_cpu summation
+ * order).  k outside 1..16 or a short leading dimension is
+ * MF_ERR_INVALID_ARG. */
+mf_status mf_spmm(mf_matrix m, int k, const double *X, int ldx, double *Y, int ldy, void *stream);
+
+/* Solves A X = B for k right-hand sides (1 <= k <= 16) with k independent
+ * FP64 CG recurrences that share every SpMM (the matrix is read once per
+ * iteration for all columns).  B and X are device arrays, column-major,
+ * ldb / ldx >= rows; X is overwritten (the solve starts from x = 0).
+ * opts: tol (per column, relative to ||b_j||; negative runs exactly maxiter
+ * iterations), maxiter; the FP64 policy only (others MF_ERR_UNSUPPORTED),
+ * no preconditioner.  reports (k entries): per column iterations, status,
+ * relres (recurrence) and relres_true (FP64 ||b_j - A x_j|| / ||b_j||);
+ * kernel_ms and bytes_moved are those of the whole solve.  Returns MF_OK
+ * when every column converged, else the first failing column's status
+ * (MF_ERR_NOT_CONVERGED, MF_ERR_BREAKDOWN); the other columns still hold
+ * their solutions. */
+mf_status mf_cg_solve_multi(mf_matrix m, int k, const double *B, int ldb, double *X, int ldx,
+                            const mf_solve_opts *opts, mf_solve_report *reports, void *stream);
+/* The same with host arrays (column-major, leading dimension rows). */
+mf_status mf_cg_solve_multi_host(mf_matrix m, int k, const double *B_host, double *X_host,
+                                 const mf_solve_opts *opts, mf_solve_report *reports);
+
+/* ---------------------------------------------------------------------- */
 /* Learned precision policy                                                */
 /* ---------------------------------------------------------------------- */
 

@@ -103,6 +103,10 @@ def lib() -> C.CDLL:
         L.mf_cg_solve_host.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]
         L.mf_bicgstab_solve.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport), vp, vp]
         L.mf_bicgstab_solve_host.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]
+        L.mf_spmm.argtypes = [vp, C.c_int, vp, C.c_int, vp, C.c_int, vp]
+        L.mf_cg_solve_multi.argtypes = [vp, C.c_int, vp, C.c_int, vp, C.c_int, C.POINTER(SolveOpts),
+                                        C.POINTER(SolveReport), vp]
+        L.mf_cg_solve_multi_host.argtypes = [vp, C.c_int, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]
         L.mf_read_matrix_market.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
         L.mf_read_matrix.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
         L.mf_read_cbd.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp)]
@@ -326,6 +330,21 @@ class Matrix:
         if st not in (MF_OK, 6):
             check(st)
         return x, rep
+
+
+def solve_multi_host(M, B, **opts):
+    """k <= 16 right-hand sides at once (mf_cg_solve_multi_host): B is
+    rows x k; returns (status, X rows x k, list of k SolveReport)."""
+    B = np.asarray(B, np.float64)
+    if B.ndim == 1:
+        B = B[:, None]
+    n, k = B.shape
+    Bc = np.asfortranarray(B)
+    X = np.zeros((n, k), np.float64, order="F")
+    reps = (SolveReport * max(k, 1))()
+    o = solve_opts(**opts)
+    st = lib().mf_cg_solve_multi_host(M.h, k, Bc.ctypes.data, X.ctypes.data, C.byref(o), reps)
+    return st, np.ascontiguousarray(X), list(reps)[:k]
 
 
 class Batch:

@@ -70,6 +70,9 @@ mf_status cg_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts 
                    double *history, cudaStream_t s);
 mf_status bicgstab_solve(mf_matrix m, const double *b, double *x, const mf_solve_opts &o, mf_solve_report &rep,
                          double *history, cudaStream_t s);
+mf_status spmm_multi(mf_matrix m, int k, const double *X, int ldx, double *Y, int ldy, cudaStream_t s);
+mf_status cg_multi(mf_matrix m, int k, const double *B, int ldb, double *X, int ldx, const mf_solve_opts &o,
+                   mf_solve_report *reports, cudaStream_t s);
 
 static mf_status check_device()
 {
@@ -169,7 +172,8 @@ mf_status mf_matrix_destroy(mf_matrix m)
                     m->d_tile_rowidx, m->d_block_signal, m->d_blockrowid_new, m->d_blockcsr_ptr_new, m->d_rbb_rowidx,
                     m->d_rbb_colstart, m->d_rbb_colstop, m->d_part, m->d_cta_chunk, m->d_chunks, m->work, m->host_io,
                     m->d_wcls, m->d_poff, m->d_pay, m->d_resid, m->d_pol, m->d_sslot, m->d_smeta, m->d_sval,
-                    m->d_shdr, m->d_spay, m->d_scta_chunk, m->d_schunks, m->d_spos, m->d_sdesc};
+                    m->d_shdr, m->d_spay, m->d_scta_chunk, m->d_schunks, m->d_spos, m->d_sdesc, m->mr_work,
+                    m->mr_io};
     for (void *p : bufs)
         if (p) cudaFree(p);
     delete m;
@@ -399,6 +403,87 @@ mf_status mf_bicgstab_solve_host(mf_matrix m, const double *b_host, double *x_ho
                                  mf_solve_report *report)
 {
     return solve_host_common(true, m, b_host, x_host, opts, report);
+}
+
+mf_status mf_spmm(mf_matrix m, int k, const double *X, int ldx, double *Y, int ldy, void *stream)
+{
+    g_err[0] = 0;
+    if (!m || k < 1 || k > 16) {
+        set_last_error("spmm: null matrix or k = %d outside 1..16", k);
+        return MF_ERR_INVALID_ARG;
+    }
+    if (ldx < m->v.cols || ldy < m->v.rows || (m->v.rows > 0 && (!X || !Y))) {
+        set_last_error("spmm: null array or leading dimension shorter than the matrix");
+        return MF_ERR_INVALID_ARG;
+    }
+    if (m->v.rows == 0) return MF_OK;
+    return spmm_multi(m, k, X, ldx, Y, ldy, (cudaStream_t)stream);
+}
+
+mf_status mf_cg_solve_multi(mf_matrix m, int k, const double *B, int ldb, double *X, int ldx,
+                            const mf_solve_opts *opts, mf_solve_report *reports, void *stream)
+{
+    g_err[0] = 0;
+    if (!m || k < 1 || k > 16 || !reports) {
+        set_last_error("multi-RHS solve: null matrix or reports, or k = %d outside 1..16", k);
+        return MF_ERR_INVALID_ARG;
+    }
+    mf_solve_opts o;
+    mf_solve_opts_default(&o);
+    if (opts) o = *opts;
+    if (o.maxiter < 0 || o.policy < 0 || o.policy > MF_POLICY_LEARNED || o.precond < 0 || o.precond > 1) {
+        set_last_error("multi-RHS solve: maxiter < 0, unknown policy or unknown preconditioner");
+        return MF_ERR_INVALID_ARG;
+    }
+    if (o.policy != MF_POLICY_FP64 || o.precond) {
+        set_last_error("multi-RHS solve: FP64 policy without preconditioner only");
+        return MF_ERR_UNSUPPORTED;
+    }
+    if (m->v.rows != m->v.cols) {
+        set_last_error("multi-RHS solve: matrix is %d x %d, a square system is required", m->v.rows, m->v.cols);
+        return MF_ERR_INVALID_ARG;
+    }
+    if (ldb < m->v.rows || ldx < m->v.rows || (m->v.rows > 0 && (!B || !X))) {
+        set_last_error("multi-RHS solve: null array or leading dimension shorter than the matrix");
+        return MF_ERR_INVALID_ARG;
+    }
+    for (int j = 0; j < k; j++) memset(&reports[j], 0, sizeof(mf_solve_report));
+    if (m->v.rows == 0) return MF_OK;
+    return cg_multi(m, k, B, ldb, X, ldx, o, reports, (cudaStream_t)stream);
+}
+
+mf_status mf_cg_solve_multi_host(mf_matrix m, int k, const double *B_host, double *X_host,
+                                 const mf_solve_opts *opts, mf_solve_report *reports)
+{
+    g_err[0] = 0;
+    if (!m || !B_host || !X_host || k < 1 || k > 16) {
+        set_last_error("multi-RHS solve: null argument or k = %d outside 1..16", k);
+        return MF_ERR_INVALID_ARG;
+    }
+    const size_t n = m->v.rows, bytes = sizeof(double) * n * (size_t)k;
+    if (n == 0) return mf_cg_solve_multi(m, k, nullptr, 0, nullptr, 0, opts, reports, nullptr);
+    cudaStream_t s = 0;
+    if (m->mr_io_bytes < 2 * bytes) {
+        if (m->mr_io) cudaFree(m->mr_io);
+        m->mr_io = nullptr;
+        m->mr_io_bytes = 0;
+        MF_CUDA(cudaMalloc(&m->mr_io, 2 * bytes));
+        m->mr_io_bytes = 2 * bytes;
+    }
+    double *dB = (double *)m->mr_io, *dX = dB + n * (size_t)k;
+    cudaError_t e = cudaMemcpyAsync(dB, B_host, bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        set_last_error("H2D: %s", cudaGetErrorString(e));
+        return MF_ERR_CUDA;
+    }
+    const mf_status st = mf_cg_solve_multi(m, k, dB, (int)n, dX, (int)n, opts, reports, s);
+    e = cudaMemcpyAsync(X_host, dX, bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_last_error("D2H: %s", cudaGetErrorString(e));
+        return MF_ERR_CUDA;
+    }
+    return st;
 }
 
 }  // extern "C"

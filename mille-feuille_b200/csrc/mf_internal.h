@@ -94,6 +94,13 @@ struct mf_matrix_s {
     // device staging of b and x for the host-buffer solve entry points
     double *host_io = nullptr;
     size_t host_io_n = 0;
+    // multi-right-hand-side solves (multi.cu): interleaved vectors, partials
+    // and state, and the staging of the host-array entry point; kept between
+    // calls (one solve per matrix at a time, as the buffers above)
+    void *mr_work = nullptr;
+    size_t mr_work_bytes = 0;
+    void *mr_io = nullptr;
+    size_t mr_io_bytes = 0;
 };
 
 namespace mf {

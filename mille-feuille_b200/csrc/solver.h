@@ -142,6 +142,10 @@ mf_status launch_bicgstab(bool mixed, CgArgs &a, int G, cudaStream_t s);
 int bicgstab_grid(mf_matrix m, bool mixed, int layout);  // layout as solver_grid (2: mixed only)
 // slots.cu: the row-slot layout (built once; state -1 = not describable)
 mf_status build_slots(mf_matrix m, cudaStream_t s);
+// multi.cu: k <= 16 right-hand sides, row-interleaved vectors
+mf_status spmm_multi(mf_matrix m, int k, const double *X, int ldx, double *Y, int ldy, cudaStream_t s);
+mf_status cg_multi(mf_matrix m, int k, const double *B, int ldb, double *X, int ldx, const mf_solve_opts &o,
+                   mf_solve_report *reports, cudaStream_t s);
 mf_status pack_slots(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s);
 // staged = true builds staged chunks and the positions; m->schunk_staged
 // tells whether every chunk qualified (otherwise the chunks are plain)

@@ -41,7 +41,10 @@ constexpr int MR_GRID = 148 * 8;           // fixed grid: the partial sums do no
 constexpr int MR_MAXK = 16;
 constexpr int MR_BATCH = 16;               // iterations queued between stop-flag reads
 constexpr int MR_VEC_MINB = 8;             // streaming kernels: 8 blocks per SM (32 registers)
-constexpr int MR_SPMM_MINB = 5;            // the SpMM: 5 blocks per SM (48 registers)
+#ifndef MF_MR_SPMM_MINB
+#define MF_MR_SPMM_MINB 5
+#endif
+constexpr int MR_SPMM_MINB = MF_MR_SPMM_MINB;  // SpMM blocks per SM (4: 64 registers, 5: 48)
 
 // Per-solve device state (one struct, zeroed before the solve).
 struct MrState {

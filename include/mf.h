@@ -243,7 +243,10 @@ mf_status mf_spmm(mf_matrix m, int k, const double *X, int ldx, double *Y, int l
  * kernel_ms and bytes_moved are those of the whole solve.  Returns MF_OK
  * when every column converged, else the first failing column's status
  * (MF_ERR_NOT_CONVERGED, MF_ERR_BREAKDOWN); the other columns still hold
- * their solutions. */
+ * their solutions.  The workspace (5 x rows x 16 doubles at most, and for
+ * the host entry point 2 x rows x k for the staging) stays allocated in the
+ * matrix handle until mf_matrix_destroy; like the other solves on one
+ * handle, calls on the same matrix must not run concurrently. */
 mf_status mf_cg_solve_multi(mf_matrix m, int k, const double *B, int ldb, double *X, int ldx,
                             const mf_solve_opts *opts, mf_solve_report *reports, void *stream);
 /* The same with host arrays (column-major, leading dimension rows). */

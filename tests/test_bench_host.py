@@ -1,0 +1,28 @@
+"""Host logic of bench.py that needs no GPU: which committed ncu traffic
+figure a bench line may carry, and the timing notes it reports."""
+import json
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+sys.path.insert(0, str(ROOT))
+
+import bench  # noqa: E402
+
+
+def test_traffic_only_for_the_captured_workload_and_policy():
+    d = json.loads((ROOT / "profiles" / "ncu_traffic.json").read_text())
+    for kernel, e in d.items():
+        assert e["dram_bytes_per_iteration"] > 0 and e["workload"] and e["policy"]
+        got = bench.ncu_traffic(kernel, e["workload"], e["policy"])
+        assert got is not None and got["dram_bytes_per_iteration"] == e["dram_bytes_per_iteration"]
+        # the figure of one matrix and payload is not reused for another
+        assert bench.ncu_traffic(kernel, "lap2d" if e["workload"] != "lap2d" else "poisson3d", e["policy"]) is None
+        other = "rule" if e["policy"] != "rule" else "static"
+        assert bench.ncu_traffic(kernel, e["workload"], other) is None
+    assert bench.ncu_traffic("k_no_such_kernel", "poisson3d", "static") is None
+
+
+def test_l2_flush_is_larger_than_l2():
+    assert bench.L2_FLUSH_BYTES >= 2 * 126 * 10**6
+    assert "flushed" in bench.L2_NOTE

@@ -55,6 +55,15 @@ def test_invalid_arguments_rejected_without_device(mf):
     st = mf.lib().mf_matrix_export(None, b"tile_ptr", None, 0)
     assert st == 1
 
+    # the multi-right-hand-side entry points: null handle, k outside 1..16
+    L = mf.lib()
+    reps = (mf.SolveReport * 16)()
+    o = mf.solve_opts()
+    assert L.mf_spmm(None, 4, None, 8, None, 8, None) == 1
+    assert L.mf_cg_solve_multi(None, 4, None, 8, None, 8, ctypes.byref(o), reps, None) == 1
+    assert L.mf_cg_solve_multi_host(None, 4, None, None, ctypes.byref(o), reps) == 1
+    assert b"null" in L.mf_last_error()
+
 
 @pytest.mark.parametrize("libname", ["libmf_solvers.so", "libmf_solvers_mixed.so"])
 def test_solver_entry_libraries_export_reference_names(mf, libname):

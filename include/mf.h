@@ -151,8 +151,13 @@ typedef enum mf_policy {
     MF_POLICY_FP64 = 0,    /* plain FP64 tiles and vectors */
     MF_POLICY_STATIC = 1,  /* value-range tile classes, FP32 accumulate,
                               FP64 reliable-update refinement */
-    MF_POLICY_RULE = 2,    /* STATIC + the partial-convergence rule per segment */
-    MF_POLICY_LEARNED = 3  /* STATIC + the learned per-tile policy */
+    MF_POLICY_RULE = 2,    /* STATIC + the reference's partial-convergence
+                              rule per segment (absolute thresholds on
+                              |p_new - p_old|, src/main-cg-mixed.cu:415-460) */
+    MF_POLICY_LEARNED = 3, /* STATIC + the learned per-tile policy */
+    MF_POLICY_RULE_SCALED = 4 /* the rule's thresholds on the change relative
+                              to max |p| (no reference counterpart: does not
+                              depend on the scale of b) */
 } mf_policy;
 
 typedef struct mf_solve_opts {
@@ -196,6 +201,24 @@ typedef struct mf_solve_report {
                               1 row slots, 2 staged row slots (the chunk's
                               vector entries copied to shared memory) */
 } mf_solve_report;
+
+/* The classes a rule policy gives every tile for the FP32 direction vectors
+ * p_new and p_old (device arrays of cols entries; p_old is the direction of
+ * the previous iteration).  It replaces the reference's in-kernel decision
+ * (src/main-cg-mixed.cu:415-460, d_vis): MF_POLICY_RULE takes, per 16-row
+ * segment s of p, v = max |p_new - p_old| over the segment in FP64 and
+ * decides MF_CLASS_FP64 (v > 1e-5), FP32 (1e-6 < v <= 1e-5), FP16
+ * (1e-7 < v <= 1e-6), INT8 (1e-8 < v <= 1e-7) or BYPASS; a tile takes the
+ * decision of its column segment.  The reference's lanes race on the
+ * segment's word; the most precise demand wins here.  MF_POLICY_RULE_SCALED
+ * applies the thresholds 1e-6 / 1e-7 / 1e-8 to v / max |p_new| in FP32.
+ * decision (device, tilenum bytes, may be NULL) receives the decisions,
+ * working (device, tilenum bytes, may be NULL) the class the mixed solver
+ * runs each tile in: FP32 for FP64 and FP32 decisions, FP16 for FP16 and for
+ * INT8 decisions on non-integer tiles, a narrower exact (value-range) class
+ * kept.  Any other policy is MF_ERR_INVALID_ARG. */
+mf_status mf_rule_classes(mf_matrix m, int policy, const float *p_new, const float *p_old, unsigned char *decision,
+                          unsigned char *working, void *stream);
 
 /* Fills opts with the defaults (maxiter 20000, tol 1e-10, FP64 policy). */
 void mf_solve_opts_default(mf_solve_opts *opts);

@@ -21,7 +21,7 @@ STATUS_NAMES = {
     5: "MF_ERR_BREAKDOWN", 6: "MF_ERR_NOT_CONVERGED", 7: "MF_ERR_IO", 8: "MF_ERR_UNSUPPORTED",
     9: "MF_ERR_NO_DEVICE",
 }
-POLICY = {"fp64": 0, "static": 1, "rule": 2, "learned": 3}
+POLICY = {"fp64": 0, "static": 1, "rule": 2, "learned": 3, "rule_scaled": 4}
 CLASS_NAMES = {0: "fp64", 1: "bypass", 2: "int8", 3: "fp16", 4: "fp32"}
 
 
@@ -97,6 +97,7 @@ def lib() -> C.CDLL:
         L.mf_spmv.argtypes = [vp, vp, vp, vp]
         L.mf_residual_norm.argtypes = [vp, vp, vp, vp, vp]
         L.mf_residual_norm_noalloc.argtypes = [vp, vp, vp, vp, vp]
+        L.mf_rule_classes.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp]
         L.mf_solve_opts_default.argtypes = [C.POINTER(SolveOpts)]
         L.mf_solve_opts_default.restype = None
         L.mf_cg_solve.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport), vp, vp]

@@ -148,31 +148,84 @@ __global__ void k_seg_change(int nseg, int n, const VT *__restrict__ pn, const V
     }
 }
 
-// The reference's per-segment partial-convergence rule
-// (src/main-cg-mixed.cu:415-460), race-free (the segment's largest change
-// decides) and normalised by max |p| so that it does not depend on the
-// scale of b: v = max_seg |p_new - p_old| / max |p_new|;
-//   v > 1e-5 -> FP32 (the inner solver's highest class), 1e-6 < v <= 1e-5 ->
-//   FP32, 1e-7 < v <= 1e-6 -> FP16, 1e-8 < v <= 1e-7 -> INT8 where the tile's
-//   values are integers (else FP16), v <= 1e-8 -> bypass.
-// A tile never gets a class above its exact (value-range) class.
-__global__ void k_rule_classes(int T, const int *__restrict__ tile_col, const unsigned char *__restrict__ cls,
-                               const float *__restrict__ seg_dp, const unsigned *__restrict__ pmax_bits,
-                               unsigned char *__restrict__ w)
+// The reference's partial-convergence decision (src/main-cg-mixed.cu:415-460)
+// per 16-row segment of p, after the p update: v = |p_new - p_old| of every
+// element, in FP64;  v > 1e-5 -> FP64, 1e-6 < v <= 1e-5 -> FP32,
+// 1e-7 < v <= 1e-6 -> FP16, 1e-8 < v <= 1e-7 -> INT8, else BYPASS.  The
+// reference's lanes race on one shared word; here the most precise class any
+// element of the segment demands wins (the class of the largest v).
+template <typename VT>
+__global__ void k_seg_rule(int nseg, int n, const VT *__restrict__ pn, const VT *__restrict__ po,
+                           unsigned char *__restrict__ seg_cls)
+{
+    const int lane = threadIdx.x & 15;
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; s < nseg; s += (gridDim.x * blockDim.x) >> 4) {
+        const int j = s * MF_TILE + lane;
+        double v = 0.0;
+        if (j < n) v = fabs((double)pn[j] - (double)po[j]);
+        for (int o = 8; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xFFFFu << (threadIdx.x & 16), v, o, 16));
+        if (lane == 0) {
+            int c;
+            if (v > 1e-5) c = MF_CLASS_FP64;
+            else if (v > 1e-6) c = MF_CLASS_FP32;
+            else if (v > 1e-7) c = MF_CLASS_FP16;
+            else if (v > 1e-8) c = MF_CLASS_INT8;
+            else c = MF_CLASS_BYPASS;
+            seg_cls[s] = (unsigned char)c;
+        }
+    }
+}
+
+// The class the mixed solver executes a tile in, for a decided class d and
+// the tile's exact (value-range) class c: the FP32 payload for FP64 / FP32
+// decisions (the inner solver's vectors and sums are FP32; FP64 accuracy
+// comes from the reliable updates), FP16 for FP16 and for INT8 decisions on
+// tiles that are not integers, and an exact class narrower than the decided
+// one is kept.
+__device__ __forceinline__ int exec_class(int d, int c)
+{
+    int w;
+    if (d == MF_CLASS_FP64 || d == MF_CLASS_FP32) w = MF_CLASS_FP32;
+    else if (d == MF_CLASS_FP16) w = MF_CLASS_FP16;
+    else if (d == MF_CLASS_INT8) w = (c == MF_CLASS_INT8) ? MF_CLASS_INT8 : MF_CLASS_FP16;
+    else w = MF_CLASS_BYPASS;
+    if (w == MF_CLASS_FP32 && (c == MF_CLASS_FP16 || c == MF_CLASS_INT8)) w = c;
+    if (w == MF_CLASS_FP16 && c == MF_CLASS_INT8) w = c;
+    return w;
+}
+
+// Tile t takes the decision of its column segment (the p segment it
+// multiplies), as the reference's SpMV reads d_vis[tile column].
+__global__ void k_rule_tiles(int T, const int *__restrict__ tile_col, const unsigned char *__restrict__ cls,
+                             const unsigned char *__restrict__ seg_cls, unsigned char *__restrict__ decision,
+                             unsigned char *__restrict__ w)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+        const int d = seg_cls[tile_col[t]];
+        if (decision) decision[t] = (unsigned char)d;
+        if (w) w[t] = (unsigned char)exec_class(d, cls[t]);
+    }
+}
+
+// MF_POLICY_RULE_SCALED: the same thresholds on the change relative to the
+// largest |p| (float), so that the decision does not depend on the scale of
+// b: v = max_seg |p_new - p_old| / max |p_new|;  v > 1e-6 -> FP32,
+// 1e-7 < v <= 1e-6 -> FP16, 1e-8 < v <= 1e-7 -> INT8, else BYPASS (no FP64
+// decision: FP32 is the inner solver's widest class).
+__global__ void k_rule_scaled_classes(int T, const int *__restrict__ tile_col, const unsigned char *__restrict__ cls,
+                                      const float *__restrict__ seg_dp, const unsigned *__restrict__ pmax_bits,
+                                      unsigned char *__restrict__ decision, unsigned char *__restrict__ w)
 {
     const float pmax = __uint_as_float(*pmax_bits);
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
         const float v = pmax > 0.f ? seg_dp[tile_col[t]] / pmax : 0.f;
-        const int c = cls[t];
         int d;
         if (v > 1e-6f) d = MF_CLASS_FP32;
         else if (v > 1e-7f) d = MF_CLASS_FP16;
-        else if (v > 1e-8f) d = (c == MF_CLASS_INT8) ? MF_CLASS_INT8 : MF_CLASS_FP16;
+        else if (v > 1e-8f) d = MF_CLASS_INT8;
         else d = MF_CLASS_BYPASS;
-        // exact classes below the demanded one stay exact
-        if (d == MF_CLASS_FP32 && (c == MF_CLASS_FP16 || c == MF_CLASS_INT8)) d = c;
-        if (d == MF_CLASS_FP16 && c == MF_CLASS_INT8) d = c;
-        w[t] = (unsigned char)d;
+        if (decision) decision[t] = (unsigned char)d;
+        if (w) w[t] = (unsigned char)exec_class(d, cls[t]);
     }
 }
 
@@ -186,21 +239,41 @@ int grid_for2(long long work, int nt)
 
 }  // namespace
 
-mf_status rule_working_classes(mf_matrix m, const void *p_new, const void *p_old, unsigned char *d_wcls,
-                               cudaStream_t s)
+mf_status rule_classes(mf_matrix m, int policy, const void *p_new, const void *p_old, unsigned char *d_decision,
+                       unsigned char *d_wcls, cudaStream_t s)
 {
     const int T = m->v.tilenum, n = m->v.cols;
     const int nseg = m->v.tilen;
+    if (policy == MF_POLICY_RULE) {
+        unsigned char *seg = nullptr;
+        MF_CUDA(pool_malloc_async(&seg, (size_t)nseg + 16, s));
+        if (nseg > 0) {
+            k_seg_rule<float><<<grid_for2((long long)nseg * 16, 256), 256, 0, s>>>(nseg, n, (const float *)p_new,
+                                                                                  (const float *)p_old, seg);
+            note_launch();
+            MF_CUDA(cudaGetLastError());
+        }
+        if (T > 0) {
+            k_rule_tiles<<<grid_for2(T, 256), 256, 0, s>>>(T, m->d_tile_columnidx, m->d_class, seg, d_decision, d_wcls);
+            note_launch();
+            MF_CUDA(cudaGetLastError());
+        }
+        cudaFreeAsync(seg, s);
+        return MF_OK;
+    }
     float *seg = nullptr;
     MF_CUDA(pool_malloc_async(&seg, sizeof(float) * nseg + sizeof(unsigned) * 4, s));
     unsigned *pmax = (unsigned *)(seg + nseg);
     MF_CUDA(cudaMemsetAsync(pmax, 0, sizeof(unsigned), s));
-    k_seg_change<float><<<grid_for2((long long)nseg * 16, 256), 256, 0, s>>>(nseg, n, (const float *)p_new,
-                                                                             (const float *)p_old, seg, pmax);
-    note_launch();
-    MF_CUDA(cudaGetLastError());
+    if (nseg > 0) {
+        k_seg_change<float><<<grid_for2((long long)nseg * 16, 256), 256, 0, s>>>(nseg, n, (const float *)p_new,
+                                                                                 (const float *)p_old, seg, pmax);
+        note_launch();
+        MF_CUDA(cudaGetLastError());
+    }
     if (T > 0) {
-        k_rule_classes<<<grid_for2(T, 256), 256, 0, s>>>(T, m->d_tile_columnidx, m->d_class, seg, pmax, d_wcls);
+        k_rule_scaled_classes<<<grid_for2(T, 256), 256, 0, s>>>(T, m->d_tile_columnidx, m->d_class, seg, pmax,
+                                                                 d_decision, d_wcls);
         note_launch();
         MF_CUDA(cudaGetLastError());
     }
@@ -209,3 +282,14 @@ mf_status rule_working_classes(mf_matrix m, const void *p_new, const void *p_old
 }
 
 }  // namespace mf
+
+extern "C" mf_status mf_rule_classes(mf_matrix m, int policy, const float *p_new, const float *p_old,
+                                     unsigned char *decision, unsigned char *working, void *stream)
+{
+    if (!m || (policy != MF_POLICY_RULE && policy != MF_POLICY_RULE_SCALED) ||
+        (m->v.cols > 0 && (!p_new || !p_old))) {
+        mf::set_last_error("mf_rule_classes: null argument or policy other than RULE / RULE_SCALED");
+        return MF_ERR_INVALID_ARG;
+    }
+    return mf::rule_classes(m, policy, p_new, p_old, decision, working, (cudaStream_t)stream);
+}

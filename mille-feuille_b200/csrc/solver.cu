@@ -176,8 +176,8 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
             a.start = 0;
             continue;
         }
-        if (o.policy == MF_POLICY_RULE) {
-            MF_TRY(rule_working_classes(m, pnew, pold, m->d_wcls, s));
+        if (o.policy == MF_POLICY_RULE || o.policy == MF_POLICY_RULE_SCALED) {
+            MF_TRY(rule_classes(m, o.policy, pnew, pold, nullptr, m->d_wcls, s));
         } else {
             MF_TRY(learned_working_classes(m, w, pnew, pold, m->d_wcls, s));
         }
@@ -270,7 +270,8 @@ mf_status bicgstab_solve(mf_matrix m, const double *b, double *x, const mf_solve
     mf_solve_opts oo = o;
     // BiCGSTAB has no checkpoint policies: dynamic policies run with the
     // value-range (static) classes
-    if (oo.policy == MF_POLICY_RULE || oo.policy == MF_POLICY_LEARNED) oo.policy = MF_POLICY_STATIC;
+    if (oo.policy == MF_POLICY_RULE || oo.policy == MF_POLICY_RULE_SCALED || oo.policy == MF_POLICY_LEARNED)
+        oo.policy = MF_POLICY_STATIC;
     return persistent_solve(true, m, b, x, oo, rep, history, s);
 }
 

@@ -158,7 +158,9 @@ mf_status pack_payload(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s)
 mf_status static_working_classes(mf_matrix m, unsigned char *d_wcls, cudaStream_t s);
 mf_status learned_working_classes(mf_matrix m, SolverWork &w, const void *p_new, const void *p_old,
                                   unsigned char *d_wcls, cudaStream_t s);
-mf_status rule_working_classes(mf_matrix m, const void *p_new, const void *p_old, unsigned char *d_wcls,
-                               cudaStream_t s);
+// RULE / RULE_SCALED classes for the FP32 directions p_new / p_old: the
+// per-tile decision (may be null) and the working classes (may be null)
+mf_status rule_classes(mf_matrix m, int policy, const void *p_new, const void *p_old, unsigned char *d_decision,
+                       unsigned char *d_wcls, cudaStream_t s);
 
 }  // namespace mf

@@ -76,6 +76,7 @@ void configure(mf_solve_opts &o, int fixed_iters, bool bicg)
         const char *p = getenv("MF_SHIM_POLICY");
         if (p && !strcmp(p, "static")) o.policy = MF_POLICY_STATIC;
         if (p && !strcmp(p, "rule")) o.policy = MF_POLICY_RULE;
+        if (p && !strcmp(p, "rule_scaled")) o.policy = MF_POLICY_RULE_SCALED;
         if (p && !strcmp(p, "learned")) o.policy = MF_POLICY_LEARNED;
     }
 }

@@ -419,6 +419,56 @@ int orc_rule_class(double v)
     return 1;
 }
 
+/* The rule's per-tile decision and working class for FP32 directions
+ * pn / po (n entries), as the library computes them: scaled = 0 takes the
+ * reference's absolute thresholds on v = max_seg |pn - po| in FP64
+ * (src/main-cg-mixed.cu:415-460, most precise demand wins), scaled = 1 the
+ * same thresholds (without the FP64 class) on max_seg |pn - po| / max |pn|
+ * in FP32.  A tile takes its column segment's decision; the working class
+ * maps FP64 / FP32 decisions to FP32, FP16 to FP16, INT8 to INT8 on integer
+ * tiles (static class INT8) and FP16 otherwise, BYPASS to BYPASS, and keeps
+ * a narrower exact static class (INT8, FP16). */
+void orc_rule_tiles(int n, int tilen, int T, const int *tile_col, const unsigned char *static_cls, const float *pn,
+                    const float *po, int scaled, unsigned char *decision, unsigned char *working)
+{
+    int *seg = (int *)malloc(sizeof(int) * (tilen > 0 ? tilen : 1));
+    float pmax = 0.f;
+    for (int j = 0; j < n; j++) {
+        float a = fabsf(pn[j]);
+        if (a > pmax) pmax = a;
+    }
+    for (int s = 0; s < tilen; s++) {
+        if (!scaled) {
+            double v = 0.0;
+            for (int j = s * 16; j < s * 16 + 16 && j < n; j++) {
+                double d = fabs((double)pn[j] - (double)po[j]);
+                if (d > v) v = d;
+            }
+            seg[s] = orc_rule_class(v);
+        } else {
+            float dp = 0.f;
+            for (int j = s * 16; j < s * 16 + 16 && j < n; j++) {
+                float d = fabsf(pn[j] - po[j]);
+                if (d > dp) dp = d;
+            }
+            float v = pmax > 0.f ? dp / pmax : 0.f;
+            seg[s] = v > 1e-6f ? 4 : v > 1e-7f ? 3 : v > 1e-8f ? 2 : 1;
+        }
+    }
+    for (int t = 0; t < T; t++) {
+        int d = seg[tile_col[t]], c = static_cls[t], w;
+        if (d == 0 || d == 4) w = 4;
+        else if (d == 3) w = 3;
+        else if (d == 2) w = (c == 2) ? 2 : 3;
+        else w = 1;
+        if (w == 4 && (c == 3 || c == 2)) w = c;
+        if (w == 3 && c == 2) w = c;
+        decision[t] = (unsigned char)d;
+        working[t] = (unsigned char)w;
+    }
+    free(seg);
+}
+
 /* ---- FP64 solvers (textbook order) --------------------------------------- */
 
 void orc_csr_spmv(int n, const int *rp, const int *ci, const double *v, const double *x, double *y)

@@ -69,6 +69,9 @@ void     orc_payload_casts(const double *v, int n, float *f32, uint16_t *f16, in
 /* Per-segment precision rule, race-free restatement of
  * src/main-cg-mixed.cu:415-460. */
 int  orc_rule_class(double max_abs_dp);
+/* Per-tile rule decision and working class for FP32 directions (see .c). */
+void orc_rule_tiles(int n, int tilen, int T, const int *tile_col, const unsigned char *static_cls, const float *pn,
+                    const float *po, int scaled, unsigned char *decision, unsigned char *working);
 
 /* CSR SpMV and FP64 solvers (textbook order; sequential sums). */
 void orc_csr_spmv(int n, const int *rowptr, const int *colidx, const double *val,

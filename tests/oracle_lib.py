@@ -91,6 +91,8 @@ def oracle() -> C.CDLL:
         lib.orc_f32_to_f16_bits.restype = C.c_uint16
         lib.orc_payload_casts.argtypes = [_f64p, C.c_int, _f32p, _u16p, _i8p]
         lib.orc_rule_class.argtypes = [C.c_double]
+        lib.orc_rule_tiles.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _u8p, _f32p, _f32p, C.c_int, _u8p, _u8p]
+        lib.orc_rule_tiles.restype = None
         lib.orc_csr_spmv.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
         lib.orc_cg.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int, C.c_double,
                                C.POINTER(C.c_double), C.c_void_p]
@@ -251,3 +253,15 @@ def oracle_bicgstab(csr: Csr, b, maxiter, tol):
 def oracle_true_relres(csr: Csr, b, x) -> float:
     return oracle().orc_true_relres(csr.n_rows, csr.rowptr, csr.colidx, csr.val,
                                     np.ascontiguousarray(b, np.float64), np.ascontiguousarray(x, np.float64))
+
+
+def oracle_rule_tiles(n, tilen, tile_col, static_cls, pn, po, scaled=False):
+    """Per-tile rule decision and working class (the restatement of the
+    reference's partial-convergence rule, src/main-cg-mixed.cu:415-460)."""
+    T = len(tile_col)
+    dec = np.zeros(max(T, 1), np.uint8)
+    work = np.zeros(max(T, 1), np.uint8)
+    oracle().orc_rule_tiles(n, tilen, T, np.ascontiguousarray(tile_col, np.int32),
+                            np.ascontiguousarray(static_cls, np.uint8), np.ascontiguousarray(pn, np.float32),
+                            np.ascontiguousarray(po, np.float32), 1 if scaled else 0, dec, work)
+    return dec[:T], work[:T]

@@ -151,6 +151,32 @@ def test_rule_classes():
     assert [lib.orc_rule_class(v) for v in (1.0, 2e-6, 2e-7, 2e-8, 1e-9, 0.0)] == [0, 4, 3, 2, 1, 1]
 
 
+def test_rule_tiles_restatement():
+    """orc_rule_tiles (the checker of the GPU rule classes) against a NumPy
+    restatement of the same rule on seeded directions and tile columns."""
+    rng = np.random.default_rng(5)
+    n, tilen, T = 200, 13, 60
+    po = rng.uniform(-1, 1, n).astype(np.float32)
+    d = rng.uniform(-1, 1, n) * np.repeat(10.0 ** rng.uniform(-10, -3, tilen), 16)[:n]
+    pn = (po.astype(np.float64) + d).astype(np.float32)
+    tile_col = rng.integers(0, tilen, T).astype(np.int32)
+    static = rng.choice([0, 2, 3, 4], T).astype(np.uint8)
+    dec, work = ol.oracle_rule_tiles(n, tilen, tile_col, static, pn, po)
+    v = np.zeros(tilen)
+    np.maximum.at(v, np.arange(n) // 16, np.abs(pn.astype(np.float64) - po.astype(np.float64)))
+    seg = np.select([v > 1e-5, v > 1e-6, v > 1e-7, v > 1e-8], [0, 4, 3, 2], 1)
+    assert dec.tolist() == seg[tile_col].tolist()
+    want = []
+    for dd, c in zip(seg[tile_col], static):
+        w = {0: 4, 4: 4, 3: 3, 2: 2 if c == 2 else 3, 1: 1}[int(dd)]
+        if w == 4 and c in (2, 3):
+            w = int(c)
+        if w == 3 and c == 2:
+            w = 2
+        want.append(w)
+    assert work.tolist() == want
+
+
 def test_oracle_cg_on_laplacian(mf):
     A = mf.synth_laplace2d(16, 16)
     Ac = ol.Csr(A.n_rows, A.n_cols, A.rowptr, A.colidx, A.val)

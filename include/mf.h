@@ -329,10 +329,18 @@ typedef struct mf_batch_report {
     int lanes_per_row;       /* schedule used: lanes per row in the SpMV */
     int cluster_ctas;        /* schedule used: CTAs per system (thread-block cluster) */
     int status;
+    long long bytes_moved;   /* algorithmic bytes of the batch: the chunk passes
+                                in their working classes, the vector streams,
+                                the FP64 reliable updates */
+    double fp16_share;       /* share of the chunk passes run from FP16 values */
 } mf_batch_report;
 
 /* count systems; system s has n[s] rows, CSR rowptr[s] (rowptr[s][0] = 0),
- * colidx[s] in [0, n[s]), val[s] (host pointers). */
+ * colidx[s] in [0, n[s]), val[s] (host pointers).  Storage: column indices
+ * as 16-bit words when every system has at most 65,536 rows (32-bit
+ * otherwise); values in FP64, FP32 and FP16 scaled per row by a power of two
+ * (diagonal kept apart in FP32); rows cut into chunks of at most 256 rows
+ * and 2048 entries, each with a precision class. */
 mf_status mf_batch_create(int count, const int *n, const int *const *rowptr, const int *const *colidx,
                           const double *const *val, mf_batch *out);
 mf_status mf_batch_destroy(mf_batch bt);
@@ -342,12 +350,53 @@ mf_status mf_batch_info(mf_batch bt, long long *rows_total, long long *nnz_total
 /* CG on every system (b, x: device arrays of rows_total doubles, stacked in
  * system order).  One launch; use_graph != 0 captures the solve (queue reset,
  * the batched kernel, the FP64 residual check) in a CUDA graph, replayed on
- * later calls with the same buffers and options.  Policies: FP64 or any mixed
- * policy (FP32 values/vectors, FP64 reliable updates). */
+ * later calls with the same buffers and options.  Policies: FP64 (FP64
+ * values and vectors), and the mixed policies (FP32 vectors and sums, each
+ * chunk read in FP32 or FP16, FP64 reliable updates, convergence on the FP64
+ * residual) whose classes are chosen inside the kernel: STATIC (FP16 only
+ * for chunks exact in FP16), RULE (every iteration, the reference's
+ * thresholds on the chunk rows' |p_new - p_old|: above 1e-6 FP32, else
+ * FP16), LEARNED (the attached policy at the first iteration and at every
+ * reliable update; MF_ERR_UNSUPPORTED without one).  RULE and LEARNED return
+ * to the static classes for the rest of a system's solve when a reliable
+ * update finds the FP64 residual above half of the previous one.
+ * MF_POLICY_RULE_SCALED and the preconditioner are MF_ERR_UNSUPPORTED. */
 mf_status mf_batch_cg_solve(mf_batch bt, const double *b, double *x, const mf_solve_opts *opts, int use_graph,
                             mf_batch_report *report, void *stream);
 /* Per-system iterations and FP64 true relative residuals of the last solve. */
 mf_status mf_batch_results(mf_batch bt, int *iterations, double *relres_true);
+/* Chunks of the batch, chunks exact in FP16 (the STATIC class), chunks whose
+ * rows can be held in FP16 at all (row scales within FP32's range). */
+mf_status mf_batch_chunk_count(mf_batch bt, int *chunks, int *static_fp16, int *fp16_capable);
+/* Copies one array of the batch to host memory: chunk_class (u8 per chunk:
+ * 0 FP32, 1 FP16, the classes at the end of the last solve), chunk_static
+ * (u8: bit 0 exact in FP16, bit 1 FP16-capable), chunk_features_static
+ * (6 floats per chunk: features 0-4 and the chunk's max |a|), chunk_start
+ * (int32, count+1: first chunk of each system), chunk_rows (int32: per
+ * system its chunks' first rows and the row count), chunk_ends (int32: the
+ * same chunks' first entries and the entry count), val16 (FP16 bits), val32, row_scale, diag32 (float), col (u16 or
+ * int32 as stored).  `bytes` must equal the array's size. */
+mf_status mf_batch_export(mf_batch bt, const char *name, void *host_dst, size_t bytes);
+/* MF_POLICY_LEARNED batched solves use p (NULL detaches). */
+mf_status mf_batch_attach_policy(mf_batch bt, mf_learned p);
+/* Runs a plain FP64 batched solve of every system (b on the device) and, at
+ * iterations 1, 1 + k, 1 + 2k, ... (k = checkpoint_every), adds (chunk
+ * features, label) samples of about one chunk in sample_stride to p's
+ * training set (at most max_samples in all).  Label 1 (FP16) when the FP16
+ * values perturb the chunk's part of A p by at most 2^-6 of it (2-norms over
+ * its rows), else 2 (FP32). */
+mf_status mf_batch_policy_collect(mf_learned p, mf_batch bt, const double *b, int checkpoint_every,
+                                  int sample_stride, long long max_samples, long long *samples_out);
+/* The attached policy's class for every chunk, for given device vectors r,
+ * p_new, p_old, q (rows_total doubles each, stacked), per-system relative
+ * residuals and reliable-update counts (device arrays of `systems` entries):
+ * the classifier the LEARNED solve runs at its checkpoints.  classes
+ * (device, one byte per chunk); features (device, 16 floats per chunk, may
+ * be NULL).  have_prev = 0 takes the history features from the current
+ * checkpoint; every call stores them for the next.  Synchronous. */
+mf_status mf_batch_policy_classify(mf_batch bt, const double *r, const double *p_new, const double *p_old,
+                                   const double *q, const double *relres, const int *refinements, int have_prev,
+                                   unsigned char *classes, float *features);
 /* Autotuner: times each schedule (lanes per row 4/8/16/32 x cluster size
  * 1/2/4/8/16) on this batch, keeps the fastest on the handle.  Default
  * schedule: 8 lanes, clusters of 4 CTAs.  Clusters of 16 CTAs exceed the

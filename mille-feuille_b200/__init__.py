@@ -47,7 +47,7 @@ class BatchReport(C.Structure):
     _fields_ = [("systems", C.c_int), ("failed", C.c_int), ("iterations_total", C.c_longlong),
                 ("iterations_max", C.c_int), ("refinements_total", C.c_int), ("relres_true_max", C.c_double),
                 ("kernel_ms", C.c_double), ("lanes_per_row", C.c_int), ("cluster_ctas", C.c_int),
-                ("status", C.c_int)]
+                ("status", C.c_int), ("bytes_moved", C.c_longlong), ("fp16_share", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -128,6 +128,11 @@ def lib() -> C.CDLL:
         L.mf_batch_results.argtypes = [vp, vp, vp]
         L.mf_batch_tune.argtypes = [vp, vp, vp, C.POINTER(SolveOpts), C.POINTER(C.c_int), C.POINTER(C.c_int), vp]
         L.mf_batch_set_schedule.argtypes = [vp, C.c_int, C.c_int]
+        L.mf_batch_chunk_count.argtypes = [vp, ip, ip, ip]
+        L.mf_batch_export.argtypes = [vp, C.c_char_p, vp, C.c_size_t]
+        L.mf_batch_attach_policy.argtypes = [vp, vp]
+        L.mf_batch_policy_collect.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_longlong, C.POINTER(C.c_longlong)]
+        L.mf_batch_policy_classify.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.c_int, vp, vp]
         L.mf_policy_param_count.restype = C.c_int
         L.mf_policy_create.argtypes = [C.c_uint64, C.POINTER(vp)]
         L.mf_policy_destroy.argtypes = [vp]
@@ -399,6 +404,37 @@ class Batch:
         la, cl = C.c_int(), C.c_int()
         check(lib().mf_batch_tune(self.h, db_ptr, dx_ptr, C.byref(o), C.byref(la), C.byref(cl), None))
         return la.value, cl.value
+
+    def chunk_count(self):
+        """(chunks, chunks exact in FP16, chunks that can be held in FP16)."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().mf_batch_chunk_count(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def export(self, name):
+        nch = self.chunk_count()[0]
+        nz = int(sum(A.nnz for A in self.systems))
+        rows = int(self.offsets[-1])
+        spec = {"chunk_class": (np.uint8, nch), "chunk_static": (np.uint8, nch),
+                "chunk_features_static": (np.float32, 6 * nch), "chunk_start": (np.int32, len(self.systems) + 1),
+                "chunk_rows": (np.int32, nch + len(self.systems)), "chunk_ends": (np.int32, nch + len(self.systems)),
+                "val16": (np.uint16, nz),
+                "val32": (np.float32, nz), "val": (np.float64, nz), "row_scale": (np.float32, rows),
+                "diag32": (np.float32, rows), "col": (np.uint16, nz)}
+        dt, cnt = spec[name]
+        out = np.zeros(cnt, dt)
+        check(lib().mf_batch_export(self.h, name.encode(), out.ctypes.data if cnt else None, out.nbytes))
+        return out
+
+    def attach_policy(self, policy):
+        check(lib().mf_batch_attach_policy(self.h, None if policy is None else policy.h))
+        self._policy = policy
+
+    def collect(self, policy, db_ptr, checkpoint_every=20, sample_stride=1, max_samples=1 << 20):
+        got = C.c_longlong()
+        check(lib().mf_batch_policy_collect(policy.h, self.h, db_ptr, checkpoint_every, sample_stride, max_samples,
+                                            C.byref(got)))
+        return got.value
 
 
 class Policy:

@@ -27,12 +27,13 @@
 #include <cstring>
 #include <vector>
 
+#include "policy_net.cuh"
 #include "solver.h"
 
 namespace mf {
-constexpr int NF = 16, H1 = 32, H2 = 32, NO = 4;
-constexpr int OW1 = 0, OB1 = OW1 + H1 * NF, OW2 = OB1 + H1, OB2 = OW2 + H2 * H1, OW3 = OB2 + H2, OB3 = OW3 + NO * H2;
-constexpr int NPARAM = OB3 + NO;  // 1732
+constexpr int NF = PN_NF, H1 = PN_H1, H2 = PN_H2, NO = PN_NO;
+constexpr int OW1 = PN_OW1, OB1 = PN_OB1, OW2 = PN_OW2, OB2 = PN_OB2, OW3 = PN_OW3, OB3 = PN_OB3;
+constexpr int NPARAM = PN_NPARAM;  // 1732
 }  // namespace mf
 
 struct mf_policy_s {
@@ -214,21 +215,7 @@ __device__ __forceinline__ void load_weights(const __nv_bfloat16 *__restrict__ w
 
 __device__ __forceinline__ void mlp_forward(const float *w, const float *x, float *h1, float *h2, float *out)
 {
-    for (int j = 0; j < H1; j++) {
-        float s = w[OB1 + j];
-        for (int k = 0; k < NF; k++) s = fmaf(w[OW1 + j * NF + k], x[k], s);
-        h1[j] = fmaxf(s, 0.f);
-    }
-    for (int j = 0; j < H2; j++) {
-        float s = w[OB2 + j];
-        for (int k = 0; k < H1; k++) s = fmaf(w[OW2 + j * H1 + k], h1[k], s);
-        h2[j] = fmaxf(s, 0.f);
-    }
-    for (int o = 0; o < NO; o++) {
-        float s = w[OB3 + o];
-        for (int k = 0; k < H2; k++) s = fmaf(w[OW3 + o * H2 + k], h2[k], s);
-        out[o] = s;
-    }
+    pn_forward(w, x, h1, h2, out);
 }
 
 __global__ void k_mlp_classify(FeatIn f, const __nv_bfloat16 *__restrict__ wq, unsigned char *__restrict__ wcls)
@@ -536,6 +523,42 @@ static mf_status collect_hook(void *ctx, mf_matrix m, SolverWork &w, const void 
 
 using namespace mf;
 
+// Sample storage of the training set for the batched solver's collector:
+// grows the buffers to max_samples (keeping the samples held) and returns
+// them with the current sample count.
+namespace mf {
+mf_status policy_sample_buffers(mf_learned p, long long max_samples, float **x, unsigned char **y, long long *n)
+{
+    if (max_samples > p->cap) {
+        float *nx = nullptr;
+        unsigned char *ny = nullptr;
+        MF_CUDA(cudaMalloc(&nx, sizeof(float) * NF * (size_t)max_samples));
+        MF_CUDA(cudaMalloc(&ny, (size_t)max_samples + 16));
+        if (p->n) {
+            MF_CUDA(cudaMemcpy(nx, p->d_x, sizeof(float) * NF * (size_t)p->n, cudaMemcpyDeviceToDevice));
+            MF_CUDA(cudaMemcpy(ny, p->d_y, (size_t)p->n, cudaMemcpyDeviceToDevice));
+        }
+        if (p->d_x) cudaFree(p->d_x);
+        if (p->d_y) cudaFree(p->d_y);
+        p->d_x = nx;
+        p->d_y = ny;
+        p->cap = max_samples;
+    }
+    *x = p->d_x;
+    *y = p->d_y;
+    *n = p->n;
+    return MF_OK;
+}
+
+mf_status policy_sample_commit(mf_learned p, long long n_total)
+{
+    p->n = std::min(n_total, p->cap);
+    return MF_OK;
+}
+
+const __nv_bfloat16 *policy_weights(mf_learned p) { return p->d_w; }
+}  // namespace mf
+
 extern "C" {
 
 mf_status mf_policy_create(uint64_t seed, mf_learned *out)
@@ -650,20 +673,11 @@ mf_status mf_policy_collect(mf_learned p, mf_matrix m, const double *b, int chec
 {
     if (!p || !m || !b || checkpoint_every <= 0 || sample_stride <= 0) return MF_ERR_INVALID_ARG;
     if (m->v.rows != m->v.cols) return MF_ERR_INVALID_ARG;
-    if (max_samples > p->cap) {
-        float *nx = nullptr;
-        unsigned char *ny = nullptr;
-        MF_CUDA(cudaMalloc(&nx, sizeof(float) * NF * (size_t)max_samples));
-        MF_CUDA(cudaMalloc(&ny, (size_t)max_samples + 16));
-        if (p->n) {
-            MF_CUDA(cudaMemcpy(nx, p->d_x, sizeof(float) * NF * (size_t)p->n, cudaMemcpyDeviceToDevice));
-            MF_CUDA(cudaMemcpy(ny, p->d_y, (size_t)p->n, cudaMemcpyDeviceToDevice));
-        }
-        if (p->d_x) cudaFree(p->d_x);
-        if (p->d_y) cudaFree(p->d_y);
-        p->d_x = nx;
-        p->d_y = ny;
-        p->cap = max_samples;
+    {
+        float *bx;
+        unsigned char *by;
+        long long have;
+        MF_TRY(policy_sample_buffers(p, max_samples, &bx, &by, &have));
     }
     double *x = nullptr;
     MF_CUDA(cudaMalloc(&x, sizeof(double) * (m->v.rows + 1)));

@@ -1,7 +1,15 @@
-"""Trains the learned per-tile precision policy on plain FP64 CG traces.
+"""Trains the learned precision policies on plain FP64 CG traces.
 
     python mille-feuille_b200/train_policy.py --grid 64 --instances 200 --seed0 1000 \
         --out aniso64.mfpol
+    python mille-feuille_b200/train_policy.py --family batched --instances 64 --seed0 2000 \
+        --every 25 --stride 4 --out randspd_batched.mfpol
+
+Family batched: the chunk policy of the batched solver.  The instances are
+random SPD systems of the batched configuration's family (n ~
+log-uniform[1k, 64k], seeds seed0 ...), solved together by one plain FP64
+batched solve that samples (chunk features, label) every `--every`
+iterations (mf_batch_policy_collect).
 
 Each instance is a seeded 3D anisotropic diffusion system (lognormal
 coefficients, log-sigma 2, correlation length 8 cells, k_z = 100 k; family
@@ -44,7 +52,19 @@ def train(grid=64, instances=200, seed0=1000, every=500, stride=256, max_samples
     P = mf.Policy(seed=init_seed)
     t0 = time.time()
     n = 0
-    for k in range(instances):
+    if family == "batched":
+        systems = [mf.synth_random_spd(seed0 + k) for k in range(instances)]
+        B = mf.Batch(systems)
+        b = B.stack([A.matvec(mf.synth_xstar(seed0 + k, A.n_rows)) for k, A in enumerate(systems)])
+        db = torch.from_numpy(b).cuda()
+        n = B.collect(P, db.data_ptr(), checkpoint_every=every, sample_stride=stride, max_samples=max_samples)
+        torch.cuda.synchronize()
+        B.close()
+        grid = int(sum(A.n_rows for A in systems))
+        instances_done = instances
+    else:
+        instances_done = 0
+    for k in range(instances_done, instances):
         seed = seed0 + k
         A = make_system(mf, family, grid, seed)
         b = torch.tensor(A.matvec(mf.synth_xstar(seed, A.n_rows)), dtype=torch.float64, device="cuda")
@@ -67,7 +87,7 @@ def train(grid=64, instances=200, seed0=1000, every=500, stride=256, max_samples
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--family", choices=["aniso", "randspd"], default="aniso")
+    ap.add_argument("--family", choices=["aniso", "randspd", "batched"], default="aniso")
     ap.add_argument("--grid", type=int, default=64, help="grid side (aniso) or rows (randspd)")
     ap.add_argument("--instances", type=int, default=200)
     ap.add_argument("--seed0", type=int, default=1000)

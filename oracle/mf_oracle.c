@@ -469,6 +469,180 @@ void orc_rule_tiles(int n, int tilen, int T, const int *tile_col, const unsigned
     free(seg);
 }
 
+/* ---- batched solver: storage and the chunk policy ------------------------- */
+
+/* IEEE binary16 bits of a double, rounded to nearest even directly from the
+ * double (no intermediate float rounding). */
+uint16_t orc_f64_to_f16_bits(double v)
+{
+    uint64_t x; memcpy(&x, &v, 8);
+    uint16_t sign = (uint16_t)((x >> 48) & 0x8000u);
+    int ex = (int)((x >> 52) & 0x7ffu);
+    uint64_t man = x & 0xfffffffffffffull;
+    if (ex == 0x7ff) return (uint16_t)(sign | 0x7c00u | (man ? 0x200u : 0u));
+    if (ex == 0 && man == 0) return sign;
+    int e = ex - 1023;                      /* unbiased exponent (normal doubles) */
+    uint64_t m = man | (1ull << 52);        /* 53-bit significand */
+    if (ex == 0) return sign;               /* double subnormals are far below half's range */
+    if (e > 15) return (uint16_t)(sign | 0x7c00u);
+    int shift;                              /* bits dropped from the 53-bit significand */
+    uint32_t base;
+    if (e >= -14) { shift = 42; base = (uint32_t)(e + 15) << 10; }
+    else { shift = 42 + (-14 - e); base = 0; if (shift > 63) return sign; }
+    uint64_t q = m >> shift, rem = m & ((1ull << shift) - 1ull), half = 1ull << (shift - 1);
+    if (e >= -14) q &= 0x3ffu;              /* implicit bit lives in the exponent field */
+    uint32_t h = base + (uint32_t)q;
+    if (rem > half || (rem == half && (h & 1u))) h++;   /* carries into the exponent as IEEE does */
+    return (uint16_t)(sign | h);
+}
+
+/* Per row of one system (CSR rp/ci/val, n rows): the FP16 copy of the
+ * off-diagonal values scaled by 2^-e (e = exponent of the row's largest
+ * off-diagonal magnitude - 14; diagonal entries 0), the row scale 2^e as a
+ * float (0 when e leaves FP32's normal range or the diagonal is not finite
+ * within FP32), the FP32 diagonal (sum of the row's diagonal entries), and
+ * the flag bit 0 = every value exact in that storage, bit 1 = FP16-capable;
+ * rowstat[4] per row: max |a| (diagonal included), min nonzero |a|,
+ * S / max(a_ii - S, 1e-30 S) with S the off-diagonal |a| sum, and the
+ * off-diagonal max / min (1 without off-diagonals). */
+void orc_batch_rows(int n, const int *rp, const int *ci, const double *val, uint16_t *val16, float *rscale,
+                    float *diag32, unsigned char *flag, float *rowstat)
+{
+    for (int i = 0; i < n; i++) {
+        double offmax = 0.0, offmin = 0.0, S = 0.0, d = 0.0, amin = 0.0;
+        for (int k = rp[i]; k < rp[i + 1]; k++) {
+            double v = val[k], av = fabs(v);
+            if (av > 0.0 && (amin == 0.0 || av < amin)) amin = av;
+            if (ci[k] == i) d += v;
+            else {
+                S += av;
+                if (av > offmax) offmax = av;
+                if (av > 0.0 && (offmin == 0.0 || av < offmin)) offmin = av;
+            }
+        }
+        int e = offmax > 0.0 ? ilogb(offmax) - 14 : 0;
+        int ok = e >= -126 && e <= 127 && isfinite(d) && fabs(d) <= 3.0e38;
+        int exact = ok && (double)(float)d == d;
+        for (int k = rp[i]; k < rp[i + 1]; k++) {
+            uint16_t h = 0;
+            if (ok && ci[k] != i) {
+                h = orc_f64_to_f16_bits(ldexp(val[k], -e));
+                if ((double)orc_f16_bits_to_f32(h) * ldexp(1.0, e) != val[k]) exact = 0;
+            }
+            val16[k] = h;
+        }
+        rscale[i] = ok ? ldexpf(1.f, e) : 0.f;
+        diag32[i] = (float)d;
+        double margin = d - S;
+        double lo = 1e-30 * (S > 1e-300 ? S : 1e-300);
+        rowstat[4 * i + 0] = (float)(offmax > fabs(d) ? offmax : fabs(d));
+        rowstat[4 * i + 1] = (float)amin;
+        rowstat[4 * i + 2] = (float)(S / (margin > lo ? margin : lo));
+        rowstat[4 * i + 3] = offmin > 0.0 ? (float)(offmax / offmin) : 1.f;
+        flag[i] = (unsigned char)((exact ? 1 : 0) | (ok ? 2 : 0));
+    }
+}
+
+static float slog10f(float v) { return log10f(v > 1e-30f ? v : 1e-30f); }
+
+/* The network: one unit at a time from its bias, products added in input
+ * order with fused multiply-adds (FP32). */
+void orc_pn_forward(const float *w, const float *x, float *out)
+{
+    float h1[32], h2[32];
+    for (int j = 0; j < 32; j++) {
+        float s = w[512 + j];
+        for (int k = 0; k < 16; k++) s = fmaf(w[j * 16 + k], x[k], s);
+        h1[j] = s > 0.f ? s : 0.f;
+    }
+    for (int j = 0; j < 32; j++) {
+        float s = w[1568 + j];
+        for (int k = 0; k < 32; k++) s = fmaf(w[544 + j * 32 + k], h1[k], s);
+        h2[j] = s > 0.f ? s : 0.f;
+    }
+    for (int o = 0; o < 4; o++) {
+        float s = w[1728 + o];
+        for (int k = 0; k < 32; k++) s = fmaf(w[1600 + o * 32 + k], h2[k], s);
+        out[o] = s;
+    }
+}
+
+/* The chunk policy of the batched solver on one system: static chunk
+ * features from the rows (chunk c = rows [crow[c], crow[c+1]), entries
+ * [cent[c], cent[c+1])), checkpoint features from r, pn, po, q, relres and
+ * refs (history from prev[4 * c] when have_prev, else the current ones;
+ * prev receives the current features 6-9), the network with weights w, and
+ * the class: 1 (FP16) when P(label <= 1) >= 0.9 or the chunk is exact in
+ * FP16, 0 (FP32) when it is not FP16-capable or otherwise.  feat: 16 floats
+ * per chunk.  margin (may be NULL): the decision's distance from its
+ * threshold, (e0 + e1) / z - 0.9. */
+void orc_batch_classify(int n, const int *rp, const int *ci, const double *val, int nch, const int *crow,
+                        const int *cent, const double *r, const double *pn, const double *po, const double *q,
+                        double relres, int refs, int have_prev, float *prev, const float *w, float *feat,
+                        unsigned char *cls, double *margin)
+{
+    uint16_t *v16 = (uint16_t *)malloc(sizeof(uint16_t) * (rp[n] > 0 ? rp[n] : 1));
+    float *rs = (float *)malloc(sizeof(float) * (n + 1)), *d32 = (float *)malloc(sizeof(float) * (n + 1));
+    float *rst = (float *)malloc(sizeof(float) * 4 * (n + 1));
+    unsigned char *fl = (unsigned char *)malloc((size_t)n + 1);
+    orc_batch_rows(n, rp, ci, val, v16, rs, d32, fl, rst);
+    float gr = 0.f, gp = 0.f;
+    float *mx = (float *)malloc(sizeof(float) * 4 * (nch + 1));
+    for (int c = 0; c < nch; c++) {
+        float mr = 0.f, mp = 0.f, mdp = 0.f, mq = 0.f;
+        for (int i = crow[c]; i < crow[c + 1]; i++) {
+            float a;
+            a = (float)fabs(r[i]); if (a > mr) mr = a;
+            a = (float)fabs(pn[i]); if (a > mp) mp = a;
+            a = (float)fabs(pn[i] - po[i]); if (a > mdp) mdp = a;
+            a = (float)fabs(q[i]); if (a > mq) mq = a;
+        }
+        mx[4 * c] = mr; mx[4 * c + 1] = mp; mx[4 * c + 2] = mdp; mx[4 * c + 3] = mq;
+        if (mr > gr) gr = mr;
+        if (mp > gp) gp = mp;
+    }
+    for (int c = 0; c < nch; c++) {
+        float amax = 0.f, amin = 3e38f, dd = 0.f, rng = 1.f;
+        unsigned fg = 3u;
+        for (int i = crow[c]; i < crow[c + 1]; i++) {
+            const float *s = rst + 4 * i;
+            if (s[0] > amax) amax = s[0];
+            if (s[1] > 0.f && s[1] < amin) amin = s[1];
+            if (s[2] > dd) dd = s[2];
+            if (s[3] > rng) rng = s[3];
+            fg &= fl[i];
+        }
+        float *x = feat + 16 * (size_t)c;
+        const float *d = mx + 4 * c;
+        x[0] = slog10f(amax) * 0.1f;
+        x[1] = slog10f(amin < 3e38f ? amin : 0.f) * 0.1f;
+        x[2] = (float)(cent[c + 1] - cent[c]) * (1.f / 2048.f);
+        x[3] = slog10f(dd) * 0.1f;
+        x[4] = slog10f(rng) * 0.1f;
+        x[5] = slog10f((float)relres) * 0.1f;
+        x[6] = slog10f(gr > 0.f ? d[0] / gr : 0.f) * 0.1f;
+        x[7] = slog10f(gp > 0.f ? d[1] / gp : 0.f) * 0.1f;
+        x[8] = slog10f(d[1] > 0.f ? d[2] / d[1] : 0.f) * 0.1f;
+        x[9] = slog10f(d[1] > 0.f && amax > 0.f ? d[3] / (d[1] * amax) : 0.f) * 0.1f;
+        for (int k = 0; k < 4; k++) x[10 + k] = have_prev ? prev[4 * c + k] : x[6 + k];
+        x[14] = (float)refs * (1.f / 16.f);
+        x[15] = 1.f;
+        for (int k = 0; k < 4; k++) prev[4 * c + k] = x[6 + k];
+        float o[4];
+        orc_pn_forward(w, x, o);
+        float m = o[0];
+        for (int k = 1; k < 4; k++) if (o[k] > m) m = o[k];
+        float e[4], z = 0.f;
+        for (int k = 0; k < 4; k++) { e[k] = expf(o[k] - m); z += e[k]; }
+        int c16 = (e[0] + e[1] >= 0.9f * z) ? 1 : 0;
+        if (fg & 1u) c16 = 1;
+        if (!(fg & 2u)) c16 = 0;
+        cls[c] = (unsigned char)c16;
+        if (margin) margin[c] = (double)(e[0] + e[1]) / (double)z - 0.9;
+    }
+    free(mx); free(v16); free(rs); free(d32); free(rst); free(fl);
+}
+
 /* ---- FP64 solvers (textbook order) --------------------------------------- */
 
 void orc_csr_spmv(int n, const int *rp, const int *ci, const double *v, const double *x, double *y)

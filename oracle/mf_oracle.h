@@ -69,6 +69,15 @@ void     orc_payload_casts(const double *v, int n, float *f32, uint16_t *f16, in
 /* Per-segment precision rule, race-free restatement of
  * src/main-cg-mixed.cu:415-460. */
 int  orc_rule_class(double max_abs_dp);
+/* Batched solver storage and chunk policy (see .c). */
+uint16_t orc_f64_to_f16_bits(double v);
+void orc_batch_rows(int n, const int *rp, const int *ci, const double *val, uint16_t *val16, float *rscale,
+                    float *diag32, unsigned char *flag, float *rowstat);
+void orc_pn_forward(const float *w, const float *x, float *out);
+void orc_batch_classify(int n, const int *rp, const int *ci, const double *val, int nch, const int *crow,
+                        const int *cent, const double *r, const double *pn, const double *po, const double *q,
+                        double relres, int refs, int have_prev, float *prev, const float *w, float *feat,
+                        unsigned char *cls, double *margin);
 /* Per-tile rule decision and working class for FP32 directions (see .c). */
 void orc_rule_tiles(int n, int tilen, int T, const int *tile_col, const unsigned char *static_cls, const float *pn,
                     const float *po, int scaled, unsigned char *decision, unsigned char *working);

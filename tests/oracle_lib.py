@@ -93,6 +93,16 @@ def oracle() -> C.CDLL:
         lib.orc_rule_class.argtypes = [C.c_double]
         lib.orc_rule_tiles.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _u8p, _f32p, _f32p, C.c_int, _u8p, _u8p]
         lib.orc_rule_tiles.restype = None
+        lib.orc_f64_to_f16_bits.argtypes = [C.c_double]
+        lib.orc_f64_to_f16_bits.restype = C.c_uint16
+        lib.orc_batch_rows.argtypes = [C.c_int, _i32p, _i32p, _f64p, _u16p, _f32p, _f32p, _u8p, _f32p]
+        lib.orc_batch_rows.restype = None
+        lib.orc_pn_forward.argtypes = [_f32p, _f32p, _f32p]
+        lib.orc_pn_forward.restype = None
+        lib.orc_batch_classify.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_int, _i32p, _i32p, _f64p, _f64p,
+                                           _f64p, _f64p, C.c_double, C.c_int, C.c_int, _f32p, _f32p, _f32p, _u8p,
+                                           _f64p]
+        lib.orc_batch_classify.restype = None
         lib.orc_csr_spmv.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
         lib.orc_cg.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int, C.c_double,
                                C.POINTER(C.c_double), C.c_void_p]
@@ -265,3 +275,32 @@ def oracle_rule_tiles(n, tilen, tile_col, static_cls, pn, po, scaled=False):
                             np.ascontiguousarray(static_cls, np.uint8), np.ascontiguousarray(pn, np.float32),
                             np.ascontiguousarray(po, np.float32), 1 if scaled else 0, dec, work)
     return dec[:T], work[:T]
+
+
+def oracle_batch_rows(csr: Csr):
+    """The batched solver's per-row storage of one system: FP16 bits of the
+    row-scaled off-diagonals, row scales, FP32 diagonal, flags, row stats."""
+    n = csr.n_rows
+    nz = int(csr.rowptr[-1])
+    v16 = np.zeros(max(nz, 1), np.uint16)
+    rs = np.zeros(n, np.float32)
+    d32 = np.zeros(n, np.float32)
+    fl = np.zeros(n, np.uint8)
+    st = np.zeros(4 * n, np.float32)
+    oracle().orc_batch_rows(n, csr.rowptr, csr.colidx, csr.val, v16, rs, d32, fl, st)
+    return v16[:nz], rs, d32, fl, st.reshape(n, 4)
+
+
+def oracle_batch_classify(csr: Csr, crow, cent, r, pn, po, q, relres, refs, have_prev, prev, w):
+    """The batched chunk policy on one system (see orc_batch_classify);
+    returns (features [nch, 16], classes, decision margins); prev (float32,
+    4 per chunk) is read when have_prev and overwritten."""
+    nch = len(crow) - 1
+    feat = np.zeros((max(nch, 1), 16), np.float32)
+    cls = np.zeros(max(nch, 1), np.uint8)
+    mar = np.zeros(max(nch, 1), np.float64)
+    oracle().orc_batch_classify(csr.n_rows, csr.rowptr, csr.colidx, csr.val, nch,
+                                np.ascontiguousarray(crow, np.int32), np.ascontiguousarray(cent, np.int32),
+                                *(np.ascontiguousarray(v, np.float64) for v in (r, pn, po, q)), float(relres),
+                                int(refs), int(have_prev), prev, np.ascontiguousarray(w, np.float32), feat, cls, mar)
+    return feat[:nch], cls[:nch], mar[:nch]

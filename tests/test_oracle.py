@@ -220,3 +220,38 @@ def test_mlp_oracle_gradient_matches_finite_differences():
         lm = lib.orc_mlp_grad(wm.astype(np.float32), X, Y, 40, gg)
         fd = (lp - lm) / ((np.float32(wp[p]) - np.float32(wm[p])))
         assert abs(fd - g[p]) <= 2e-3 * max(1.0, abs(g[p])) + 1e-4, (p, fd, g[p])
+
+
+def test_f64_to_f16_restatement_matches_numpy():
+    """The oracle's direct double -> binary16 rounding (the batched solver's
+    FP16 copy) against NumPy's conversion, normal, subnormal and overflow
+    ranges included."""
+    import warnings
+
+    lib = ol.oracle()
+    rng = np.random.default_rng(0)
+    v = np.concatenate([rng.normal(size=4000) * 10.0 ** rng.uniform(-9, 6, 4000),
+                        [65504.0, 65519.99, 65520.0, 6e-8, 2.9802322387695312e-08, 5.96e-8, -0.0, 1e-30, 1e30]])
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        want = v.astype(np.float16).view(np.uint16)
+    got = np.array([lib.orc_f64_to_f16_bits(float(x)) for x in v], np.uint16)
+    assert np.array_equal(got, want)
+
+
+def test_pn_forward_restatement():
+    """The oracle's policy network forward pass against a float64 NumPy
+    evaluation of the same weights (FP32 rounding only)."""
+    lib = ol.oracle()
+    rng = np.random.default_rng(2)
+    w = (rng.normal(size=NPARAM) * 0.3).astype(np.float32)
+    x = rng.normal(size=16).astype(np.float32)
+    out = np.zeros(4, np.float32)
+    lib.orc_pn_forward(w, x, out)
+    W1, b1 = w[:512].reshape(32, 16).astype(np.float64), w[512:544]
+    W2, b2 = w[544:1568].reshape(32, 32).astype(np.float64), w[1568:1600]
+    W3, b3 = w[1600:1728].reshape(4, 32).astype(np.float64), w[1728:1732]
+    h1 = np.maximum(W1 @ x + b1, 0)
+    h2 = np.maximum(W2 @ h1 + b2, 0)
+    o = W3 @ h2 + b3
+    assert np.allclose(out, o, rtol=1e-5, atol=1e-5)

@@ -2,7 +2,19 @@
 """Benchmark: CG solves/s to relative residual 1e-10 on one B200.
 
 Workloads (--workload):
-  poisson3d (default) 3D 7-point 128^3 (n = 2,097,152, nnz = 14,581,760;
+  batched (default) 512 random SPD systems, n ~ log-uniform[1k, 64k], seeds
+                  100-611 (random symmetric pattern, 8-32 draws per row,
+                  values N(0,1) x row scale 10^U[-4,4], diagonal row |sum| +
+                  1; b = A x*, x* ~ U[-1,1] from the system's seed), solved
+                  by one graph-captured batched launch per step with the
+                  learned per-chunk precision policy (--policy learned,
+                  policy file mille-feuille_b200/policies/randspd_batched.mfpol,
+                  trained on seeds 2000-2063); the static and rule policies
+                  of the same batched solver and the plain FP64 tiled solves
+                  of the same 512 systems one after another are timed in the
+                  same run (static, rule and fp64 keys).  One step = every
+                  system from x0 = 0 to ||b - A x|| / ||b|| <= 1e-10.
+  poisson3d       3D 7-point 128^3 (n = 2,097,152, nnz = 14,581,760;
                   off-diagonals -(f_i+f_j)/2 with f = 10^U[-3,0], diagonal
                   row |sum| + 1e-3, b = A x*, x* ~ U[-1,1], seed 1), solved
                   with tile mixed precision and FP64 refinement (--policy
@@ -10,10 +22,6 @@ Workloads (--workload):
                   timed in the same run (fp64 key).  One step = one solve
                   from x0 = 0 to ||b - A x|| / ||b|| <= 1e-10, matrix
                   resident in HBM.
-  batched         512 random SPD systems, n ~ log-uniform[1k, 64k], seeds
-                  100-611, one graph-captured batched launch per step; the
-                  plain FP64 tiled solves of the same systems one after
-                  another are timed beside it (fp64 key).
   lap2d           CG on the 2D 5-point Laplacian 128^2 (seed 0) to 1e-10: small
                   enough to live in L2; reports the latency-bound regime.
   convdiff        BiCGSTAB on the 96^3 convection-diffusion system to 1e-9.
@@ -27,8 +35,10 @@ Workloads (--workload):
                  every step)
 --impl reference the reference's own CPU tiled path (Tile_create +
                  blockspmv_cpu from the reference sources, with a CG loop
-                 around it) on the default workload, timed on the host cores
-                 on a bounded sample
+                 around it) on the chosen workload, timed on the host cores
+                 on a bounded sample (batched: a sample of the systems, one
+                 per host core at once, scaled by the FP64 oracle's
+                 iteration counts of all 512 systems)
 
 N > 1 runs independent replicas, one per GPU (a single system does not
 shard), timed with CUDA events and reported as the max over ranks.
@@ -56,9 +66,18 @@ UNIT = "solves/s"
 GRID = 128
 SEED = 1
 TOL = 1e-10
-# FP64 CG iterations to 1e-10 on this configuration, from the CPU oracle
-# (tests/test_config_iterations.py pins it); used to scale the CPU sample.
-FP64_ITERS_ORACLE = 598
+# FP64 CG iterations to 1e-10 of the FP64 CPU oracle on the single-system
+# configurations (tests/golden/config_iterations.json, recomputed by
+# tests/test_config_iterations.py); they scale the CPU-baseline samples.
+CONFIG_ITERS = json.loads((ROOT / "tests" / "golden" / "config_iterations.json").read_text())
+FP64_ITERS_ORACLE = CONFIG_ITERS["poisson3d_scaled_128"]["iterations"]
+
+
+def oracle_iterations(workload):
+    """The FP64 oracle's iteration count for a single-system workload (None
+    where no CPU baseline is scaled)."""
+    key = {"poisson3d": "poisson3d_scaled_128", "lap2d": "laplace2d_128"}.get(workload)
+    return CONFIG_ITERS[key]["iterations"] if key else None
 
 
 def load_peaks():
@@ -186,9 +205,117 @@ class CpuReference:
         return int(max(3, min(500, budget_s / max(one, 1e-6))))
 
 
+BATCH_ORACLE = ROOT / "tests" / "golden" / "batched_oracle.json"
+BATCH_POLICY = ROOT / "mille-feuille_b200" / "policies" / "randspd_batched.mfpol"
+
+
+def _ref_batch_worker(task):
+    """One sampled system of the batched configuration on one host thread:
+    the reference's Tile_create and blockspmv_cpu (compiled from its sources
+    into oracle/_ref) inside a CG loop, for about `budget_s` seconds; returns
+    (seed, n, nnz, seconds per iteration).  The system comes from the
+    oracle's restatement of the generator (no product library loaded)."""
+    seed, budget_s = task
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as ol  # CPU-baseline leg only
+
+    ref = ol.reference()
+    ref.ref_cg_iterations.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    ref.ref_cg_iterations.restype = C.c_double
+    A = ol.oracle_random_spd(seed)
+    b = A.to_scipy() @ ol.oracle_xstar(seed, A.n_rows)
+    sizes, _ = ol.reference_tiles(A)
+    ref.ref_encode_last()
+    nx = sizes["tilen"] * 16
+    x, r, p, q, bb = (np.zeros(nx) for _ in range(5))
+    bb[: A.n_rows] = b
+    rho = C.c_double(0.0)
+
+    def run(k, start=0):
+        return ref.ref_cg_iterations(A.n_rows, A.n_cols, A.nnz, bb.ctypes.data, x.ctypes.data, r.ctypes.data,
+                                     p.ctypes.data, q.ctypes.data, k, 1, start, C.byref(rho))
+
+    one = run(1, start=1)
+    k = int(max(3, min(5000, budget_s / max(one, 1e-7))))
+    return seed, A.n_rows, A.nnz, run(k) / k
+
+
+class CpuBatchReference:
+    """The reference CPU tiled path on the batched configuration, timed on a
+    sample of its systems (evenly spaced in size), one system per host core
+    at once (each on one thread, as blockspmv_cpu is serial), and scaled to
+    the whole batch by the FP64 oracle's iteration counts of all 512 systems
+    (tests/golden/batched_oracle.json): seconds per (entry x iteration) under
+    that load times the batch's sum of iterations x entries, divided by the
+    cores used.  The reference Tile_create is not timed (matrices resident,
+    as on the GPU)."""
+
+    def __init__(self, sample=16, budget_s=4.0, workers=None):
+        import multiprocessing as mp
+
+        fixture = json.loads(BATCH_ORACLE.read_text())
+        self.systems = fixture["systems"]
+        order = sorted(self.systems, key=lambda s: s["nnz"])
+        idx = np.unique(np.linspace(0, len(order) - 1, sample).round().astype(int))
+        self.seeds = [order[i]["seed"] for i in idx]
+        self.cores = max(1, min(workers or os.cpu_count() or 1, len(self.seeds)))
+        self.budget_s = budget_s
+        self.work = sum(s["iterations"] * s["nnz"] for s in self.systems)
+        self.pool = mp.get_context("spawn").Pool(self.cores)
+
+    def measure(self, budget_s=None):
+        """Seconds for the whole batch on the cores (one sample)."""
+        b = budget_s or self.budget_s
+        res = self.pool.map(_ref_batch_worker, [(s, b) for s in self.seeds])
+        alpha = statistics.median(t / nnz for _, _, nnz, t in res)
+        self.last = res
+        return alpha * self.work / self.cores
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+    def describe(self):
+        return (f"{len(self.seeds)} of the 512 systems (evenly spaced in size), one per host core at once, each "
+                f"timed for ~{self.budget_s:.0f} s of reference blockspmv_cpu CG iterations on one thread; seconds "
+                f"per entry-iteration (median) x the batch's {self.work:.3e} entry-iterations (FP64 oracle "
+                f"iteration counts) / {self.cores} cores; reference Tile_create not timed")
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
+        return 0
+    if args.workload == "batched":
+        sys.path.insert(0, str(ROOT / "tests"))
+        import oracle_lib as ol  # reference arm: the reference's own CPU code
+
+        if ol.reference() is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU code not built (oracle/_ref)"}))
+            return 0
+        steps = args.warmup + args.steps
+        cpu = CpuBatchReference(budget_s=max(0.5, min(8.0, 60.0 / max(1, steps))))
+        vals = []
+        try:
+            for s in range(steps):
+                t = cpu.measure()
+                if s >= args.warmup:
+                    vals.append(len(cpu.systems) / t)
+        finally:
+            cpu.close()
+        v = statistics.median(vals)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v * len(cpu.systems),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": BATCH_NAME, "systems": len(cpu.systems),
+                       "l2": "host cores only (no device cache involved)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cpu.cores, "kind": "reference",
+                             "sample": cpu.describe()},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
         return 0
     import __graft_entry__ as ge
 
@@ -416,10 +543,14 @@ def workload_single(args, mf, world, local):
     result["roofline_in"] = (per_launch, mean_ms, kname, statistics.mean(iters))
     result["dtype"] = "f64" if args.policy == "fp64" else "mixed(f32/f16/i8 tiles, f32 accumulate, f64 refinement)"
     # FP64 CG iterations to 1e-10 from the CPU oracle (scale of the CPU sample)
-    oracle_iters = {"poisson3d": FP64_ITERS_ORACLE, "lap2d": 380}.get(args.workload)
+    oracle_iters = oracle_iterations(args.workload)
     result["cpu"] = (A, b, oracle_iters) if oracle_iters else None
     M.close()
     return result, info
+
+
+BATCH_NAME = ("batched random SPD x512 (n ~ log-uniform[1k,64k], seeds 100-611, 8-32 draws per row, "
+              "row scale 10^U[-4,4]) CG to 1e-10")
 
 
 def workload_batched(args, mf, world, local):
@@ -436,29 +567,38 @@ def workload_batched(args, mf, world, local):
     t0 = time.perf_counter()
     B = mf.Batch(systems)
     setup_ms = (time.perf_counter() - t0) * 1e3
+    pol = None
+    if args.policy == "learned":
+        pol = mf.Policy.load(args.policy_file or BATCH_POLICY)
+        B.attach_policy(pol)
     bstack = B.stack(bs)
     db = torch.from_numpy(bstack).cuda()
     dx = torch.zeros_like(db)
     stream = torch.cuda.current_stream()
-    o = mf.solve_opts(tol=TOL, maxiter=50000, policy=args.policy)
+
+    def make_solve(policy, rep):
+        o = mf.solve_opts(tol=TOL, maxiter=50000, policy=policy)
+
+        def solve():
+            st = L.mf_batch_cg_solve(B.h, db.data_ptr(), dx.data_ptr(), C.byref(o), 1, C.byref(rep),
+                                     stream.cuda_stream)
+            if st != 0:
+                mf.check(st)
+        return solve
+
     rep = mf.BatchReport()
-
-    def solve():
-        st = L.mf_batch_cg_solve(B.h, db.data_ptr(), dx.data_ptr(), C.byref(o), 1, C.byref(rep),
-                                 stream.cuda_stream)
-        if st != 0:
-            mf.check(st)
-
+    solve = make_solve(args.policy, rep)
     for _ in range(args.warmup):
         solve()
     torch.cuda.synchronize()
     _barrier(world)
     launches0 = L.mf_kernel_launches()
-    kernel_ms = []
+    kernel_ms, bytes_moved = [], []
 
     def step():
         solve()
         kernel_ms.append(rep.kernel_ms)
+        bytes_moved.append(rep.bytes_moved)
 
     with ClockSampler(local) as clk:
         ms = _timed(stream, step, args.steps)
@@ -469,20 +609,47 @@ def workload_batched(args, mf, world, local):
     result = {"rep": rep, "ms": ms, "value": value, "launches": launches, "clocks": clk.summary()}
     if args.profile:
         return result, None
-    # algorithmic bytes of the launch: per system and iteration, the FP64
-    # tiled SpMV (or its FP32 counterpart) plus the CG vector streams
-    sb = 8 if args.policy == "fp64" else 4
-    vb = 72 if args.policy == "fp64" else 36
-    alg = 0
-    for A, it in zip(systems, its):
-        alg += int(it) * (A.nnz * (sb + 1) + 24 * tiles_of(A) + 16 * A.n_rows + vb * A.n_rows)
-    info = {"workload": f"batched random SPD x{N} (n ~ log-uniform[1k,64k], seeds 100-{99 + N}) CG to 1e-10",
-            "systems": N, "rows_total": int(sum(A.n_rows for A in systems)),
+    # accuracy: FP64 true residual of every system, the error against x*,
+    # and against the FP64 CPU oracle's solution on the four smallest systems
+    x = dx.cpu().numpy()
+    xparts = B.split(x)
+    err_xs = max(float(np.max(np.abs(xp - xv))) for xp, xv in zip(xparts, xs))
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as ol  # checker only
+
+    fixture = json.loads(BATCH_ORACLE.read_text())["systems"] if BATCH_ORACLE.exists() else None
+    small = sorted(range(N), key=lambda k: systems[k].n_rows)[:4]
+    err_or = 0.0
+    for k in small:
+        A = systems[k]
+        _, x_o, _ = ol.oracle_cg(ol.Csr(A.n_rows, A.n_cols, A.rowptr, A.colidx, A.val), bs[k], 50000, TOL)
+        err_or = max(err_or, float(np.max(np.abs(xparts[k] - x_o))))
+    info = {"workload": BATCH_NAME, "systems": N, "rows_total": int(sum(A.n_rows for A in systems)),
             "nnz_total": int(sum(A.nnz for A in systems)), "policy": args.policy,
-            "iterations_mean": float(its.mean()), "iterations_max": int(its.max()),
-            "relres_true_max": float(rep.relres_true_max), "failed": int(rep.failed), "setup_ms": setup_ms,
+            "policy_file": str(Path(args.policy_file or BATCH_POLICY).relative_to(ROOT)) if pol else None,
+            "iterations_total": int(its.sum()), "iterations_max": int(its.max()),
+            "relres_true_max": float(rep.relres_true_max), "failed": int(rep.failed),
+            "fp16_share": float(rep.fp16_share), "max_abs_err_vs_xstar": err_xs,
+            "max_abs_err_vs_fp64_oracle_4_smallest": err_or, "setup_ms": setup_ms,
             "lanes_per_row": int(rep.lanes_per_row), "cluster_ctas": int(rep.cluster_ctas),
             "parallelism": f"replicas x{world}", "l2": L2_NOTE}
+    if fixture is not None and N == len(fixture):
+        it_o = np.array([s["iterations"] for s in fixture])
+        info["iterations_vs_fp64_oracle"] = float(its.sum() / it_o.sum())
+        info["oracle_max_abs_err_vs_xstar"] = max(s["max_abs_err_vs_xstar"] for s in fixture)
+    # the other policies of the same batched solver, same run
+    k = max(2, args.steps // 4)
+    for other in ("static", "rule"):
+        if other == args.policy:
+            continue
+        orep = mf.BatchReport()
+        osolve = make_solve(other, orep)
+        osolve()
+        torch.cuda.synchronize()
+        oms = _max_over_ranks(_timed(stream, osolve, k), world)
+        info[other] = {"value": N * k * world / (oms * 1e-3), "unit": UNIT, "iterations_total": int(orep.iterations_total),
+                       "relres_true_max": float(orep.relres_true_max), "fp16_share": float(orep.fp16_share),
+                       "steps": k}
     # the plain FP64 tiled solves of the same systems, one after another
     if not args.no_fp64_baseline:
         dbs = [torch.from_numpy(bv).cuda() for bv in bs]
@@ -490,16 +657,19 @@ def workload_batched(args, mf, world, local):
         o64 = mf.solve_opts(tol=TOL, maxiter=50000, policy="fp64")
         r64 = mf.SolveReport()
         xk = torch.zeros(max(A.n_rows for A in systems), dtype=torch.float64, device="cuda")
+        it64 = []
 
         def seq():
+            it64.clear()
             for M_, d in zip(mats, dbs):
                 L.mf_cg_solve(M_.h, d.data_ptr(), xk.data_ptr(), C.byref(o64), C.byref(r64), None,
                               stream.cuda_stream)
+                it64.append(r64.iterations)
 
         seq()
         torch.cuda.synchronize()
         ms64 = _max_over_ranks(_timed(stream, seq, 1), world)
-        info["fp64"] = {"value": N * world / (ms64 * 1e-3), "unit": UNIT,
+        info["fp64"] = {"value": N * world / (ms64 * 1e-3), "unit": UNIT, "iterations_total": int(sum(it64)),
                         "what": "the same 512 systems solved one after another by the plain FP64 tiled CG"}
         for M_ in mats:
             M_.close()
@@ -520,8 +690,14 @@ def workload_batched(args, mf, world, local):
     e2e_s = _max_over_ranks(e2e_s, world)
     result["e2e"] = {"value": N * args.steps * world / e2e_s, "unit": UNIT,
                      "h2d_bytes_per_step": 8 * len(bstack), "d2h_bytes_per_step": 8 * len(bstack)}
-    result["roofline_in"] = (alg, statistics.mean(kernel_ms), "k_batched_cg", None)
-    result["dtype"] = "f64" if args.policy == "fp64" else "mixed(f32 values, f32 accumulate, f64 refinement)"
+    # roofline numerator: the kernel's own count of the bytes its passes
+    # stream (each chunk in its working class: values + 16-bit columns + row
+    # pointers, + row scale and diagonal for FP16 chunks), the vector
+    # streams of each iteration and the FP64 reliable updates
+    result["roofline_in"] = (statistics.mean(bytes_moved), statistics.mean(kernel_ms), "k_batched_cg", None)
+    result["dtype"] = ("f64" if args.policy == "fp64" else
+                       "mixed(fp32 / row-scaled fp16 chunks, f32 accumulate, f64 refinement)")
+    result["cpu_batch"] = N == 512
     result["cpu"] = None
     B.close()
     return result, info
@@ -679,6 +855,18 @@ def run_mf(args):
                                               f"loops on {cpu.threads} threads), scaled by {oracle_iters} "
                                               f"FP64 iterations to 1e-10; reference Tile_create {cpu.setup_s:.1f} s "
                                               f"not timed"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and res.get("cpu_batch"):
+        sys.path.insert(0, str(ROOT / "tests"))
+        import oracle_lib as ol  # CPU-baseline leg only
+
+        if ol.reference() is not None:
+            cpu = CpuBatchReference(budget_s=8.0)
+            try:
+                t = cpu.measure()
+            finally:
+                cpu.close()
+            line["cpu_baseline"] = {"value": len(cpu.systems) / t, "unit": UNIT, "cores": cpu.cores,
+                                    "kind": "reference", "sample": cpu.describe()}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -692,11 +880,14 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mf", "reference"], default="mf")
-    ap.add_argument("--workload", default="poisson3d",
-                    choices=["poisson3d", "lap2d", "batched", "convdiff", "aniso", "multirhs"])
+    ap.add_argument("--workload", default="batched",
+                    choices=["batched", "poisson3d", "lap2d", "convdiff", "aniso", "multirhs"])
     ap.add_argument("--rhs", type=int, default=16, help="multirhs workload: right-hand sides (1-16)")
-    ap.add_argument("--policy", default="static", choices=["fp64", "static", "rule", "learned"])
-    ap.add_argument("--policy-file", default=None, help="learned policy (mf_policy_save format)")
+    ap.add_argument("--policy", default=None, choices=["fp64", "static", "rule", "learned"],
+                    help="precision policy (default: learned for batched, static otherwise)")
+    ap.add_argument("--policy-file", default=None,
+                    help="learned policy (mf_policy_save format; batched default: "
+                         "mille-feuille_b200/policies/randspd_batched.mfpol)")
     ap.add_argument("--no-fp64-baseline", action="store_true")
     ap.add_argument("--systems", type=int, default=512, help="batched workload: number of systems (seeds 100..)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -705,6 +896,8 @@ def main():
     ap.add_argument("--iters", type=int, default=0,
                     help="run a fixed number of CG iterations per solve instead of stopping at 1e-10 (profiling)")
     args = ap.parse_args()
+    if args.policy is None:
+        args.policy = "learned" if args.workload == "batched" else "static"
     if args.impl == "reference":
         return run_reference(args)
     return run_mf(args)

@@ -398,9 +398,10 @@ mf_status mf_batch_policy_classify(mf_batch bt, const double *r, const double *p
                                    const double *q, const double *relres, const int *refinements, int have_prev,
                                    unsigned char *classes, float *features);
 /* Autotuner: times each schedule (lanes per row 4/8/16/32 x cluster size
- * 1/2/4/8/16) on this batch, keeps the fastest on the handle.  Default
- * schedule: 8 lanes, clusters of 4 CTAs.  Clusters of 16 CTAs exceed the
- * portable cluster size and are enabled explicitly on the kernel. */
+ * 1/2/4/8/16; one 512-thread CTA per SM) on this batch, keeps the fastest
+ * on the handle.  Default schedule: 4 lanes, clusters of 2 CTAs.  Clusters
+ * of 16 CTAs exceed the portable cluster size and are enabled explicitly on
+ * the kernel. */
 mf_status mf_batch_tune(mf_batch bt, const double *b, double *x, const mf_solve_opts *opts, int *lanes_out,
                         int *cluster_out, void *stream);
 /* lanes in {4, 8, 16, 32}, cluster in {1, 2, 4, 8, 16}. */

@@ -75,7 +75,7 @@ namespace cg = cooperative_groups;
 namespace mf {
 namespace {
 constexpr int PW = 32768;   // columns per storage panel (16-bit offsets)
-constexpr int BCE = 2048;   // entries of a (chunk, panel) stage
+constexpr int BCE = 4096;   // entries of a (chunk, panel) stage
 constexpr int BCR = 256;    // rows of a chunk
 }  // namespace
 }  // namespace mf
@@ -244,14 +244,14 @@ __device__ __forceinline__ void cluster_max2(cg::cluster_group &cl, float &a, fl
 struct BHdr {
     int r0, r1, e0, direct;   // rows [r0, r1), first entry e0 (relative to the panel)
     int sh_rp, sh_col, sh_val, cls;
-    int panel, pad0;
+    int panel, sh_rs, sh_dg, pad0;
     long long ebase;          // the panel's first entry (global)
 };
 
 // Stages in flight per CTA.  The mixed kernels stage at most 4 + 2 bytes
 // per entry (FP32 values, 16-bit columns).
 #ifndef MF_BATCH_STAGES_MIX
-#define MF_BATCH_STAGES_MIX 4
+#define MF_BATCH_STAGES_MIX 3
 #endif
 #ifndef MF_BATCH_STAGES_FP64
 #define MF_BATCH_STAGES_FP64 3
@@ -266,7 +266,9 @@ struct Stage {
     static constexpr int OFF_RP = 0;
     static constexpr int OFF_COL = 1072;
     static constexpr int OFF_VAL = OFF_COL + ((BCE * 2 + 32 + 15) & ~15);
-    static constexpr int SIZE = OFF_VAL + ((BCE * VB + 32 + 15) & ~15);
+    static constexpr int OFF_RS = OFF_VAL + ((BCE * VB + 32 + 15) & ~15);  // FP16 passes: row scales
+    static constexpr int OFF_DG = OFF_RS + ((BCR * 4 + 32 + 15) & ~15);    // FP16 passes: FP32 diagonals
+    static constexpr int SIZE = OFF_DG + ((BCR * 4 + 32 + 15) & ~15);
     static_assert(OFF_COL % 16 == 0 && OFF_VAL % 16 == 0 && SIZE % 16 == 0, "stage regions 16-byte aligned");
     static_assert((BCR + 1) * 4 + 32 <= OFF_COL, "row pointers fit");
     static_assert(NS >= 1 && NS <= 8, "stage phases kept in a byte");
@@ -311,7 +313,7 @@ __device__ __forceinline__ unsigned b_range_bytes(long long a0, long long a1)
 // the panel (relative to its first entry ebase), the chunk's class.
 struct BChunk {
     int r0, r1, e0, e1, cls, panel;
-    long long ebase, rpbase;
+    long long ebase, rpbase, rowbase;
 };
 
 __device__ __forceinline__ BChunk b_chunk(const BatchArgs &a, int sys, const SysView &v, int c, int k, bool mix)
@@ -325,6 +327,7 @@ __device__ __forceinline__ BChunk b_chunk(const BatchArgs &a, int sys, const Sys
     ch.e0 = a.prow[ch.rpbase + ch.r0];
     ch.e1 = a.prow[ch.rpbase + ch.r1];
     ch.cls = mix ? (int)a.ccls[c] : 0;
+    ch.rowbase = v.r0;
     return ch;
 }
 
@@ -334,7 +337,7 @@ __device__ __forceinline__ unsigned long long chunk_bytes(const BChunk &ch)
 {
     const unsigned long long ne = (unsigned long long)(ch.e1 - ch.e0), nr = (unsigned long long)(ch.r1 - ch.r0);
     const unsigned vb = MIX ? (ch.cls ? 2u : 4u) : 8u;
-    return ne * (vb + 2) + (nr + 1) * 4 + ((ch.cls && ch.panel == 0) ? nr * 8 : 0);
+    return ne * (vb + 2) + (nr + 1) * 4 + (ch.cls ? nr * 8 : 0);
 }
 
 // Thread 0: stage pair `ch` into stage k.
@@ -352,14 +355,20 @@ __device__ void b_issue(const BatchArgs &a, BSmem<MIX> &S, const BChunk &ch, int
     h.panel = ch.panel;
     h.ebase = ch.ebase;
     const int vb = MIX ? (ch.cls ? 2 : 4) : 8;
-    const long long z0 = ch.ebase;
+    const long long z0 = ch.ebase, rw = ch.rowbase;
+    const bool rsdg = MIX && ch.cls == 1;  // FP16 rows also need their scale and diagonal
     unsigned total = b_range_bytes(4 * (ch.rpbase + r0), 4 * (ch.rpbase + r1 + 1));
     if (!h.direct) total += b_range_bytes(2 * (z0 + e0), 2 * (z0 + e1)) + b_range_bytes(vb * (z0 + e0), vb * (z0 + e1));
+    if (rsdg) total += 2 * b_range_bytes(4 * (rw + r0), 4 * (rw + r1));
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(&S.bar[k], total);
     unsigned char *st = S.stage[k];
     b_add_range(st + SG::OFF_RP, (const unsigned char *)a.prow, 4 * (ch.rpbase + r0), 4 * (ch.rpbase + r1 + 1),
                 &S.bar[k], h.sh_rp);
+    if (rsdg) {
+        b_add_range(st + SG::OFF_RS, (const unsigned char *)a.rscale, 4 * (rw + r0), 4 * (rw + r1), &S.bar[k], h.sh_rs);
+        b_add_range(st + SG::OFF_DG, (const unsigned char *)a.diag32, 4 * (rw + r0), 4 * (rw + r1), &S.bar[k], h.sh_dg);
+    }
     if (h.direct) return;
     b_add_range(st + SG::OFF_COL, (const unsigned char *)a.col, 2 * (z0 + e0), 2 * (z0 + e1), &S.bar[k], h.sh_col);
     const unsigned char *vsrc = MIX ? (ch.cls ? (const unsigned char *)a.val16 : (const unsigned char *)a.val32)
@@ -372,7 +381,7 @@ __device__ void b_issue(const BatchArgs &a, BSmem<MIX> &S, const BChunk &ch, int
 // tree, so every run gives the same bits.  Two rows per lane group are in
 // flight at once (a row with no entries: bounds 0, 0).
 #ifndef MF_BATCH_BU
-#define MF_BATCH_BU 8
+#define MF_BATCH_BU 4
 #endif
 constexpr int BU = MF_BATCH_BU;
 
@@ -447,6 +456,34 @@ __device__ __forceinline__ void row_dot2(const RowPair &rb, const uint16_t *__re
     y1 = d1;
 }
 
+// One row's sum from a staged pass: lanes stride over the row's entries, BU
+// per lane per trip, loaded without predicates -- columns past the row's end
+// are read from the stage and masked into the p window (which holds finite
+// values: zeros before its first copy), their weights are zero.  Lane sums
+// combine in a fixed xor tree.
+template <int L, typename V, class Src>
+__device__ __forceinline__ double row_dot1_smem(int a, int e, const uint16_t *__restrict__ col,
+                                                const V *__restrict__ val, int lane, Src src)
+{
+    constexpr bool D = std::is_same<V, double>::value;
+    using AT = typename std::conditional<D, double, float>::type;
+    AT s = 0;
+    const int n = e - a;
+    for (int k = lane; k < n; k += L * BU) {
+#pragma unroll
+        for (int u = 0; u < BU; u++) {
+            const int kk = k + u * L;
+            const int c = (int)col[a + kk] & (PW - 1);
+            const AT v = kk < n ? (AT)val[a + kk] : (AT)0;
+            s = vfma(v, (AT)src(c), s);
+        }
+    }
+    double d = (double)s;
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o, L);
+    return d;
+}
+
 // FP64 row sums of rows i0, i1 (-1: none) of a system over all its panels,
 // read from global memory, panels added in order; x in FP64.
 template <int L>
@@ -503,7 +540,7 @@ __device__ void chunk_stats_warp(const BatchArgs &a, const SysView &v, int c, in
         mr = fmaxf(mr, (float)fabs((double)r[i]));
         mp = fmaxf(mp, (float)fabs(pv));
         mdp = fmaxf(mdp, (float)fabs(pv - (double)po[i]));
-        mq = fmaxf(mq, (float)fabs((double)q[i]));
+        mq = fmaxf(mq, (float)fabs((double)__ldcg(q + i)));
         if (label) {
             const double s = (double)rscale[i];
             double dq = 0.0, qq = 0.0;
@@ -643,6 +680,10 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
     }
     if (learned)
         for (int k = threadIdx.x; k < PN_NPARAM; k += BNT) s_w[k] = __bfloat162float(a.mlp_w[k]);
+    // the p window holds finite values from the start (padded slots of the
+    // row loop read it with zero weight)
+    if (MIX)
+        for (int k = threadIdx.x; k < (int)(SL::PWIN_BYTES / 4); k += BNT) ((float *)s_win)[k] = 0.f;
     __syncthreads();
     // mbarrier phase parities, one bit per stage (registers: an array indexed
     // by the stage number would live in local memory).  Producer (thread 0):
@@ -669,7 +710,7 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
         const long long r0 = V.r0;
         const double *b = a.b + r0;
         double *x = a.x + r0;
-        const float *rscale = a.rscale + r0, *diag32 = a.diag32 + r0;
+        const float *rscale = a.rscale + r0;
         VT *r = (VT *)a.r + r0, *q = (VT *)a.q + r0, *xlo = (VT *)a.xlo + r0;
         VT *pb[2] = {(VT *)a.p0 + r0, (VT *)a.p1 + r0};
         // this CTA's chunks and rows
@@ -718,6 +759,7 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                     for (int i = c0 + wl; i < c1; i += 32) {
                         const VT pv = vfma(bt, pold[i], r[i]);
                         pnew[i] = pv;
+                        if (npan == 2) q[i] = (VT)0;
                         v = fmax(v, fabs((double)pv - (double)pold[i]));
                     }
 #pragma unroll
@@ -735,9 +777,15 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                         r4[u] = r[i + u * BNT];
                     }
 #pragma unroll
-                    for (int u = 0; u < 4; u++) pnew[i + u * BNT] = vfma(bt, po4[u], r4[u]);
+                    for (int u = 0; u < 4; u++) {
+                        pnew[i + u * BNT] = vfma(bt, po4[u], r4[u]);
+                        if (npan == 2) q[i + u * BNT] = (VT)0;
+                    }
                 }
-                for (; i < rb; i += BNT) pnew[i] = vfma(bt, pold[i], r[i]);
+                for (; i < rb; i += BNT) {
+                    pnew[i] = vfma(bt, pold[i], r[i]);
+                    if (npan == 2) q[i] = (VT)0;
+                }
             }
             cl.sync();
             double loc = 0.0;
@@ -753,10 +801,16 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
             bool fail = false;
             if (J > 0) {
                 if (wid == 0) {
+                    // descriptors of the next 32 passes load while the current
+                    // ones are issued
+                    BChunk dn;
+                    memset(&dn, 0, sizeof(dn));
+                    if (wl < J) dn = b_chunk(a, sys, V, cl0 + wl % nchl, wl / nchl, MIX);
                     for (int jb = 0; jb < J && !fail; jb += 32) {
-                        BChunk d;
-                        memset(&d, 0, sizeof(d));
-                        if (jb + wl < J) d = b_chunk(a, sys, V, cl0 + (jb + wl) % nchl, (jb + wl) / nchl, MIX);
+                        const BChunk d = dn;
+                        memset(&dn, 0, sizeof(dn));
+                        if (jb + 32 + wl < J)
+                            dn = b_chunk(a, sys, V, cl0 + (jb + 32 + wl) % nchl, (jb + 32 + wl) / nchl, MIX);
                         const int cnt = min(32, J - jb);
                         for (int t = 0; t < cnt; t++) {
                             BChunk ch;
@@ -768,11 +822,12 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                             ch.panel = __shfl_sync(0xffffffffu, d.panel, t);
                             ch.ebase = __shfl_sync(0xffffffffu, d.ebase, t);
                             ch.rpbase = __shfl_sync(0xffffffffu, d.rpbase, t);
+                            ch.rowbase = __shfl_sync(0xffffffffu, d.rowbase, t);
                             const int j = jb + t, k = j % NS;
                             int ok = 1;
                             if (wl == 0) {
                                 if (MIX && j % nchl == 0) {
-                                    if (wstarted) ok = mbar_wait_bounded(&S.wempty, wpar ^ 1u, a.queue + 1, a.budget_ns);
+                                    if (wstarted) ok = mbar_wait_sleep_bounded(&S.wempty, wpar ^ 1u, a.queue + 1, a.budget_ns);
                                     if (ok) {
                                         issue_pwin(&S.pbar, s_win, (const float *)pnew, V.n, j / nchl, s_pshift);
                                         wpar ^= 1u;
@@ -780,7 +835,7 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                                     }
                                 }
                                 if (ok && ((pstarted >> k) & 1u))
-                                    ok = mbar_wait_bounded(&S.empty[k], ((pfill >> k) & 1u) ^ 1u, a.queue + 1,
+                                    ok = mbar_wait_sleep_bounded(&S.empty[k], ((pfill >> k) & 1u) ^ 1u, a.queue + 1,
                                                            a.budget_ns);
                                 if (ok) {
                                     b_issue<MIX>(a, S, ch, k);
@@ -807,10 +862,10 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                         const int jp = j % nchl;
                         bool w = true;
                         if (MIX && jp == 0) {
-                            w = mbar_wait_bounded(&S.pbar, cwpar, a.queue + 1, a.budget_ns);
+                            w = mbar_wait_sleep_bounded(&S.pbar, cwpar, a.queue + 1, a.budget_ns);
                             cwpar ^= 1u;
                         }
-                        w = mbar_wait_bounded(&S.bar[k], (cfull >> k) & 1u, a.queue + 1, a.budget_ns) && w;
+                        w = mbar_wait_sleep_bounded(&S.bar[k], (cfull >> k) & 1u, a.queue + 1, a.budget_ns) && w;
                         cfull ^= 1u << k;
                         if (!__all_sync(0xffffffffu, w)) {
                             fail = true;
@@ -821,45 +876,22 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                         const int *rps = (const int *)(st + SG::OFF_RP + h.sh_rp);  // panel row pointers of h.r0 ..
                         const int nr = h.r1 - h.r0;
                         const bool h16 = MIX && h.cls == 1;
-                        const bool firstp = h.panel == 0, lastp = h.panel == npan - 1;
+                        const bool firstp = h.panel == 0;
                         const VT *pwin = MIX ? (const VT *)s_win + s_pshift : (const VT *)pnew + (long long)h.panel * PW;
                         auto psrc = [=](int c) -> VT { return pwin[c]; };
-                        // the trip count is the same for every lane (shuffles inside)
-                        for (int qb = 0; qb < nr; qb += 2 * GPC) {
-                            const int q0 = qb + cgrp, q1 = qb + GPC + cgrp;
-                            // the rows' own p values, their partial sums so far
-                            // and for FP16 rows their scale and FP32 diagonal are
-                            // loaded before the row sums
-                            VT pn0 = (VT)0, pn1 = (VT)0, qo0 = (VT)0, qo1 = (VT)0;
-                            float rs0 = 0.f, rs1 = 0.f, dg0 = 0.f, dg1 = 0.f;
-                            if (clane == 0) {
-                                if (q0 < nr) {
-                                    pn0 = pnew[h.r0 + q0];
-                                    if (!firstp) qo0 = q[h.r0 + q0];
-                                }
-                                if (q1 < nr) {
-                                    pn1 = pnew[h.r0 + q1];
-                                    if (!firstp) qo1 = q[h.r0 + q1];
-                                }
-                                if (h16) {
-                                    if (q0 < nr) {
-                                        rs0 = __ldg(rscale + h.r0 + q0);
-                                        dg0 = firstp ? __ldg(diag32 + h.r0 + q0) : 0.f;
-                                    }
-                                    if (q1 < nr) {
-                                        rs1 = __ldg(rscale + h.r0 + q1);
-                                        dg1 = firstp ? __ldg(diag32 + h.r0 + q1) : 0.f;
-                                    }
-                                }
-                            }
-                            RowPair rr;
-                            rr.a0 = q0 < nr ? rps[q0] : 0;
-                            rr.e0 = q0 < nr ? rps[q0 + 1] : 0;
-                            rr.a1 = q1 < nr ? rps[q1] : 0;
-                            rr.e1 = q1 < nr ? rps[q1 + 1] : 0;
-                            double y0, y1;
+                        const uint16_t *scol = (const uint16_t *)(st + SG::OFF_COL + h.sh_col);
+                        const unsigned char *sval = st + SG::OFF_VAL + h.sh_val;
+                        // one row per lane group; the trip count is the same
+                        // for every lane of a warp (shuffles inside)
+                        for (int qb = 0; qb < nr; qb += GPC) {
+                            const int q0 = qb + cgrp;
+                            const bool in = q0 < nr;
+                            const int ra0 = in ? rps[q0] : 0, re0 = in ? rps[q0 + 1] : 0;
+                            double y0;
                             if (h.direct) {
+                                RowPair rr{ra0, re0, 0, 0};
                                 const uint16_t *gcol = a.col + h.ebase;
+                                double y1;
                                 if constexpr (MIX) {
                                     if (h16)
                                         row_dot2<L, __half, decltype(psrc), true>(rr, gcol, a.val16 + h.ebase, clane,
@@ -871,44 +903,39 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                                     row_dot2<L, double, decltype(psrc), true>(rr, gcol, a.val + h.ebase, clane, psrc,
                                                                                y0, y1);
                                 }
+                            } else if constexpr (MIX) {
+                                if (h16)
+                                    y0 = row_dot1_smem<L, __half>(ra0 - h.e0, re0 - h.e0, scol, (const __half *)sval,
+                                                                  clane, psrc);
+                                else
+                                    y0 = row_dot1_smem<L, float>(ra0 - h.e0, re0 - h.e0, scol, (const float *)sval,
+                                                                 clane, psrc);
                             } else {
-                                rr.a0 -= h.e0;
-                                rr.e0 -= h.e0;
-                                rr.a1 -= h.e0;
-                                rr.e1 -= h.e0;
-                                const uint16_t *scol = (const uint16_t *)(st + SG::OFF_COL + h.sh_col);
-                                const unsigned char *sval = st + SG::OFF_VAL + h.sh_val;
-                                if constexpr (MIX) {
-                                    if (h16)
-                                        row_dot2<L, __half, decltype(psrc), false>(rr, scol, (const __half *)sval,
-                                                                                    clane, psrc, y0, y1);
-                                    else
-                                        row_dot2<L, float, decltype(psrc), false>(rr, scol, (const float *)sval, clane,
-                                                                                   psrc, y0, y1);
-                                } else {
-                                    row_dot2<L, double, decltype(psrc), false>(rr, scol, (const double *)sval, clane,
-                                                                                psrc, y0, y1);
-                                }
+                                y0 = row_dot1_smem<L, double>(ra0 - h.e0, re0 - h.e0, scol, (const double *)sval,
+                                                              clane, psrc);
                             }
-                            if (clane == 0) {
+                            if (clane == 0 && in) {
+                                // no global load on this path: FP16 rows take
+                                // their scale and FP32 diagonal from the stage,
+                                // the diagonal's p from the window of the panel
+                                // that holds the diagonal column
+                                const int i0 = h.r0 + q0;
                                 if (h16) {
-                                    // FP16 rows: scaled off-diagonal sum, the FP32
-                                    // diagonal added with the first panel
-                                    y0 = (double)fmaf(rs0, (float)y0, dg0 * (float)pn0);
-                                    y1 = (double)fmaf(rs1, (float)y1, dg1 * (float)pn1);
+                                    const float *srs = (const float *)(st + SG::OFF_RS + h.sh_rs);
+                                    const float *sdg = (const float *)(st + SG::OFF_DG + h.sh_dg);
+                                    const float dt = (i0 / PW == h.panel) ? sdg[q0] * (float)pwin[i0 - h.panel * PW] : 0.f;
+                                    y0 = (double)fmaf(srs[q0], (float)y0, dt);
                                 }
-                                // panels after the first add to the partial sum in
-                                // q (the same thread handles a row in every panel)
-                                const VT t0 = firstp ? (VT)y0 : (VT)((double)qo0 + y0);
-                                const VT t1 = firstp ? (VT)y1 : (VT)((double)qo1 + y1);
-                                if (q0 < nr) {
-                                    q[h.r0 + q0] = t0;
-                                    if (lastp) loc += (double)pn0 * (double)t0;
-                                }
-                                if (q1 < nr) {
-                                    q[h.r0 + q1] = t1;
-                                    if (lastp) loc += (double)pn1 * (double)t1;
-                                }
+                                // one panel: the row sum is q; two panels: both
+                                // partial sums are added to q (zeroed by the p
+                                // update; two additions onto zero give the same
+                                // bits in either order); more panels: the same
+                                // thread handles a row in every panel and adds
+                                // in panel order
+                                VT *qi = q + i0;
+                                if (npan == 1) *qi = (VT)y0;
+                                else if (npan == 2) atomicAdd(qi, (VT)y0);
+                                else *qi = firstp ? (VT)y0 : (VT)((double)*qi + y0);
                             }
                         }
                         __syncwarp();
@@ -928,6 +955,22 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                 if (MIX && wstarted) mbar_drain(&S.pbar, wpar ^ 1u, a.queue + 1, a.budget_ns);
             }
             if (tid == 0) s_fail = fail ? 1 : 0;
+            // p.q over this CTA's rows (q read past L1: partial sums arrive by
+            // reductions in L2)
+            if (!fail) {
+                int i = ra + tid;
+                for (; i + 3 * BNT < rb; i += 4 * BNT) {
+                    VT p4[4], q4[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        p4[u] = pnew[i + u * BNT];
+                        q4[u] = __ldcg(q + i + u * BNT);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; u++) loc += (double)p4[u] * (double)q4[u];
+                }
+                for (; i < rb; i += BNT) loc += (double)pnew[i] * (double)__ldcg(q + i);
+            }
             const double pq = cluster_sum(cl, loc, &s_slot[2], s_warp);
             int any_fail = 0;
             for (unsigned kk = 0; kk < ncta; kk++) any_fail |= *cl.map_shared_rank(&s_fail, kk);
@@ -950,7 +993,7 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
 #pragma unroll
                     for (int u = 0; u < 4; u++) {
                         p4[u] = pnew[i + u * BNT];
-                        q4[u] = q[i + u * BNT];
+                        q4[u] = __ldcg(q + i + u * BNT);
                         r4[u] = r[i + u * BNT];
                         x4[u] = MIX ? (double)xlo[i + u * BNT] : x[i + u * BNT];
                     }
@@ -972,12 +1015,12 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                 for (; i < rb; i += BNT) {
                     if (MIX) {
                         xlo[i] = fmaf((float)alpha, (float)pnew[i], (float)xlo[i]);
-                        const float ri = fmaf(-(float)alpha, (float)q[i], (float)r[i]);
+                        const float ri = fmaf(-(float)alpha, (float)__ldcg(q + i), (float)r[i]);
                         r[i] = ri;
                         loc += (double)ri * (double)ri;
                     } else {
                         x[i] = fma(alpha, (double)pnew[i], x[i]);
-                        const double ri = fma(-alpha, (double)q[i], (double)r[i]);
+                        const double ri = fma(-alpha, (double)__ldcg(q + i), (double)r[i]);
                         r[i] = ri;
                         loc += ri * ri;
                     }
@@ -1728,11 +1771,11 @@ static mf_status batch_check_opts(mf_batch bt, const mf_solve_opts &o)
 
 static void batch_schedule(mf_batch bt, int &lanes, int &cluster)
 {
-    lanes = bt->tuned_lanes ? bt->tuned_lanes : 8;
+    lanes = bt->tuned_lanes ? bt->tuned_lanes : 4;
     cluster = bt->tuned_cluster ? bt->tuned_cluster : 2;
     if (const char *e = getenv("MF_BATCH_LANES")) lanes = atoi(e);
     if (const char *e = getenv("MF_BATCH_CLUSTER")) cluster = atoi(e);
-    if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) lanes = 8;
+    if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32) lanes = 4;
     if (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8 && cluster != 16) cluster = 2;
 }
 

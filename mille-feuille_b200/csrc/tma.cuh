@@ -71,6 +71,36 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
     return ok != 0;
 }
 
+// try_wait with a suspend-time hint: the thread sleeps until the phase
+// completes or about `hint_ns` nanoseconds pass, instead of polling (idle
+// warps then take no issue slots from the working ones).
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, unsigned parity, unsigned hint_ns)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait that sleeps between tries (mbar_try_wait_sleep); false (and
+// status set) when the budget ran out.
+__device__ __forceinline__ bool mbar_wait_sleep_bounded(uint64_t *bar, unsigned parity, int *status,
+                                                        unsigned long long budget_ns)
+{
+    if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (;;) {
+        if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
+        if (globaltimer_ns() - t0 > budget_ns) {
+            atomicCAS(status, DEV_OK, DEV_TIMEOUT);
+            return false;
+        }
+    }
+}
+
 // Bounded wait for phase `parity` of `bar`; false (and status set) when the
 // budget ran out.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, int *status,

@@ -643,6 +643,107 @@ void orc_batch_classify(int n, const int *rp, const int *ci, const double *val, 
     free(mx); free(v16); free(rs); free(d32); free(rst); free(fl);
 }
 
+/* ---- the batched configuration's generator --------------------------------- */
+
+/* A C restatement of the library's seeded random SPD generator (SplitMix64
+ * counter streams; the written definition the Python mirror also follows),
+ * so that the CPU baseline builds its systems without the product library.
+ * Row i draws k_i = 8 + floor(25 U) columns uniform in [0, n) (self
+ * references dropped) with values N(0,1) 10^U[-4,4] / 2, mirrored; duplicates
+ * summed in draw order; diagonal = row |sum| + 1.  Arrays malloc'd (free
+ * with orc_free). */
+#define ORC_GAMMA 0x9E3779B97F4A7C15ull
+
+static uint64_t orc_mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static uint64_t orc_key(uint64_t seed, uint64_t stream) { return orc_mix64(seed * ORC_GAMMA ^ orc_mix64(stream + ORC_GAMMA)); }
+static double orc_u01(uint64_t key, uint64_t i) { return (double)(orc_mix64(key + (i + 1) * ORC_GAMMA) >> 11) * 0x1.0p-53; }
+static double orc_normal01(uint64_t key, uint64_t m)
+{
+    double a = orc_u01(key, 2 * m), b = orc_u01(key, 2 * m + 1);
+    return sqrt(-2.0 * log(1.0 - a)) * cos(6.283185307179586 * b);
+}
+
+int orc_random_spd_size(uint64_t seed)
+{
+    double u = orc_u01(orc_key(seed, 3), 0);
+    return (int)llround(exp(log(1000.0) + u * (log(64000.0) - log(1000.0))));
+}
+
+void orc_xstar(uint64_t seed, int n, double *out)
+{
+    uint64_t k = orc_key(seed, 1);
+    for (int i = 0; i < n; i++) out[i] = -1.0 + 2.0 * orc_u01(k, i);
+}
+
+typedef struct { long long key, ord; double v; } orc_trip;
+
+static int orc_trip_cmp(const void *pa, const void *pb)
+{
+    const orc_trip *a = (const orc_trip *)pa, *b = (const orc_trip *)pb;
+    if (a->key != b->key) return a->key < b->key ? -1 : 1;
+    return a->ord < b->ord ? -1 : (a->ord > b->ord ? 1 : 0);
+}
+
+int orc_random_spd(uint64_t seed, int n, int *nnz_out, int **rowptr, int **colidx, double **val)
+{
+    if (n <= 0) n = orc_random_spd_size(seed);
+    uint64_t kl = orc_key(seed, 4), ks = orc_key(seed, 2), kc = orc_key(seed, 5), kv = orc_key(seed, 6);
+    size_t cap = (size_t)n * 66 + 16, nt = 0;
+    orc_trip *tr = (orc_trip *)malloc(sizeof(orc_trip) * cap);
+    long long ord = 0;
+    for (int i = 0; i < n; i++) {
+        int k = 8 + (int)floor(25.0 * orc_u01(kl, i));
+        double sc = pow(10.0, -4.0 + 8.0 * orc_u01(ks, i));
+        for (int e = 0; e < k; e++) {
+            int j = (int)floor(orc_u01(kc, (uint64_t)i * 32 + e) * n);
+            if (j >= n) j = n - 1;
+            if (j == i) continue;
+            double a = orc_normal01(kv, (uint64_t)i * 32 + e) * sc * 0.5;
+            tr[nt].key = (long long)i * n + j; tr[nt].ord = ord++; tr[nt].v = a; nt++;
+            tr[nt].key = (long long)j * n + i; tr[nt].ord = ord++; tr[nt].v = a; nt++;
+        }
+    }
+    qsort(tr, nt, sizeof(orc_trip), orc_trip_cmp);
+    size_t nk = 0;
+    for (size_t q = 0; q < nt; q++) {
+        if (nk > 0 && tr[nk - 1].key == tr[q].key) tr[nk - 1].v += tr[q].v;
+        else tr[nk++] = tr[q];
+    }
+    double *rowabs = (double *)calloc((size_t)n, sizeof(double));
+    for (size_t q = 0; q < nk; q++) rowabs[tr[q].key / n] += fabs(tr[q].v);
+    int *rp = (int *)malloc(sizeof(int) * ((size_t)n + 1));
+    int *ci = (int *)malloc(sizeof(int) * (nk + (size_t)n + 1));
+    double *v = (double *)malloc(sizeof(double) * (nk + (size_t)n + 1));
+    size_t q = 0, z = 0;
+    rp[0] = 0;
+    for (int i = 0; i < n; i++) {
+        int diag_done = 0;
+        while (q < nk && tr[q].key / n == i) {
+            int j = (int)(tr[q].key % n);
+            if (!diag_done && j > i) { ci[z] = i; v[z] = rowabs[i] + 1.0; z++; diag_done = 1; }
+            ci[z] = j; v[z] = tr[q].v; z++;
+            q++;
+        }
+        if (!diag_done) { ci[z] = i; v[z] = rowabs[i] + 1.0; z++; }
+        rp[i + 1] = (int)z;
+    }
+    free(tr);
+    free(rowabs);
+    *nnz_out = (int)z;
+    *rowptr = rp;
+    *colidx = ci;
+    *val = v;
+    return n;
+}
+
+void orc_free(void *p) { free(p); }
+
 /* ---- FP64 solvers (textbook order) --------------------------------------- */
 
 void orc_csr_spmv(int n, const int *rp, const int *ci, const double *v, const double *x, double *y)

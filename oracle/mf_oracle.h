@@ -69,6 +69,11 @@ void     orc_payload_casts(const double *v, int n, float *f32, uint16_t *f16, in
 /* Per-segment precision rule, race-free restatement of
  * src/main-cg-mixed.cu:415-460. */
 int  orc_rule_class(double max_abs_dp);
+/* The batched configuration's random SPD generator (see .c); returns n. */
+int  orc_random_spd_size(uint64_t seed);
+int  orc_random_spd(uint64_t seed, int n, int *nnz_out, int **rowptr, int **colidx, double **val);
+void orc_xstar(uint64_t seed, int n, double *out);
+void orc_free(void *p);
 /* Batched solver storage and chunk policy (see .c). */
 uint16_t orc_f64_to_f16_bits(double v);
 void orc_batch_rows(int n, const int *rp, const int *ci, const double *val, uint16_t *val16, float *rscale,

@@ -103,6 +103,15 @@ def oracle() -> C.CDLL:
                                            _f64p, _f64p, C.c_double, C.c_int, C.c_int, _f32p, _f32p, _f32p, _u8p,
                                            _f64p]
         lib.orc_batch_classify.restype = None
+        lib.orc_random_spd_size.argtypes = [C.c_uint64]
+        lib.orc_random_spd_size.restype = C.c_int
+        lib.orc_random_spd.argtypes = [C.c_uint64, C.c_int, C.POINTER(C.c_int), C.POINTER(C.POINTER(C.c_int)),
+                                       C.POINTER(C.POINTER(C.c_int)), C.POINTER(C.POINTER(C.c_double))]
+        lib.orc_random_spd.restype = C.c_int
+        lib.orc_xstar.argtypes = [C.c_uint64, C.c_int, _f64p]
+        lib.orc_xstar.restype = None
+        lib.orc_free.argtypes = [C.c_void_p]
+        lib.orc_free.restype = None
         lib.orc_csr_spmv.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
         lib.orc_cg.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int, C.c_double,
                                C.POINTER(C.c_double), C.c_void_p]
@@ -304,3 +313,24 @@ def oracle_batch_classify(csr: Csr, crow, cent, r, pn, po, q, relres, refs, have
                                 *(np.ascontiguousarray(v, np.float64) for v in (r, pn, po, q)), float(relres),
                                 int(refs), int(have_prev), prev, np.ascontiguousarray(w, np.float32), feat, cls, mar)
     return feat[:nch], cls[:nch], mar[:nch]
+
+
+def oracle_random_spd(seed, n=0) -> Csr:
+    """The batched configuration's random SPD system of `seed` (the C
+    restatement of the library's generator)."""
+    lib = oracle()
+    nnz = C.c_int()
+    rp, ci, v = C.POINTER(C.c_int)(), C.POINTER(C.c_int)(), C.POINTER(C.c_double)()
+    n = lib.orc_random_spd(seed, n, C.byref(nnz), C.byref(rp), C.byref(ci), C.byref(v))
+    out = Csr(n, n, np.ctypeslib.as_array(rp, shape=(n + 1,)).copy(),
+              np.ctypeslib.as_array(ci, shape=(max(nnz.value, 1),))[: nnz.value].copy(),
+              np.ctypeslib.as_array(v, shape=(max(nnz.value, 1),))[: nnz.value].copy())
+    for p in (rp, ci, v):
+        lib.orc_free(C.cast(p, C.c_void_p))
+    return out
+
+
+def oracle_xstar(seed, n):
+    out = np.zeros(n, np.float64)
+    oracle().orc_xstar(seed, n, out)
+    return out

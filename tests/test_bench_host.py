@@ -26,3 +26,24 @@ def test_traffic_only_for_the_captured_workload_and_policy():
 def test_l2_flush_is_larger_than_l2():
     assert bench.L2_FLUSH_BYTES >= 2 * 126 * 10**6
     assert "flushed" in bench.L2_NOTE
+
+
+def test_batched_reference_baseline_runs_on_host():
+    """The reference arm of the batched workload: the reference's own CPU
+    code on a sample of the systems, scaled by the committed FP64 oracle
+    iteration counts (no product library loaded in its workers)."""
+    import pytest
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as ol
+
+    if ol.reference() is None:
+        pytest.skip("reference CPU code not built")
+    cpu = bench.CpuBatchReference(sample=2, budget_s=0.2, workers=2)
+    try:
+        t = cpu.measure()
+    finally:
+        cpu.close()
+    assert t > 0 and len(cpu.systems) == 512 and cpu.cores == 2
+    assert all(nnz > 0 and s > 0 for _, _, nnz, s in cpu.last)
+    assert "512 systems" in cpu.describe() or "of the 512" in cpu.describe()

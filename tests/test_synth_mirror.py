@@ -44,3 +44,18 @@ def test_random_spd(mf, seed):
 
 def test_aniso3d(mf):
     _same(mf.synth_aniso3d(6, 3), sm.aniso3d(6, 3))
+
+
+@pytest.mark.parametrize("seed,n", [(100, 0), (101, 0), (3001, 2000), (611, 0)])
+def test_oracle_random_spd_matches_library(mf, seed, n):
+    """The oracle's C restatement of the random SPD generator (used by the
+    CPU baseline, which loads no product library) equals the library's."""
+    import oracle_lib as ol
+
+    A = mf.synth_random_spd(seed, n)
+    B = ol.oracle_random_spd(seed, n)
+    assert A.n_rows == B.n_rows
+    assert np.array_equal(A.rowptr, B.rowptr) and np.array_equal(A.colidx, B.colidx)
+    assert np.array_equal(A.val, B.val)
+    assert np.array_equal(mf.synth_xstar(seed, A.n_rows), ol.oracle_xstar(seed, A.n_rows))
+    assert ol.oracle().orc_random_spd_size(seed) == mf.lib().mf_synth_random_spd_size(seed)

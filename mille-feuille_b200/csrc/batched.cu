@@ -97,6 +97,7 @@ struct mf_batch_s {
     double *d_val = nullptr;
     float *d_val32 = nullptr;
     __half *d_val16 = nullptr;    // row-scaled, diagonal entries 0
+    uint32_t *d_cv16 = nullptr;   // FP16 value bits << 16 | column offset (one word per entry)
     float *d_rscale = nullptr;    // per row: scale of the FP16 values
     float *d_diag32 = nullptr;    // per row: diagonal (sum of the row's diagonal entries)
     // row chunks of every system
@@ -150,6 +151,7 @@ struct BatchArgs {
     const double *val;
     const float *val32;
     const __half *val16;
+    const uint32_t *cv16;
     const float *rscale, *diag32;
     const double *b;
     double *x;
@@ -354,24 +356,28 @@ __device__ void b_issue(const BatchArgs &a, BSmem<MIX> &S, const BChunk &ch, int
     h.cls = ch.cls;
     h.panel = ch.panel;
     h.ebase = ch.ebase;
-    const int vb = MIX ? (ch.cls ? 2 : 4) : 8;
     const long long z0 = ch.ebase, rw = ch.rowbase;
-    const bool rsdg = MIX && ch.cls == 1;  // FP16 rows also need their scale and diagonal
+    const bool h16 = MIX && ch.cls == 1;  // FP16 rows: packed (value, column) words, row scales and diagonals
+    const int vb = MIX ? 4 : 8;  // FP16 passes: one 4-byte word per entry
     unsigned total = b_range_bytes(4 * (ch.rpbase + r0), 4 * (ch.rpbase + r1 + 1));
-    if (!h.direct) total += b_range_bytes(2 * (z0 + e0), 2 * (z0 + e1)) + b_range_bytes(vb * (z0 + e0), vb * (z0 + e1));
-    if (rsdg) total += 2 * b_range_bytes(4 * (rw + r0), 4 * (rw + r1));
+    if (!h.direct) {
+        total += b_range_bytes(vb * (z0 + e0), vb * (z0 + e1));
+        if (!h16) total += b_range_bytes(2 * (z0 + e0), 2 * (z0 + e1));
+    }
+    if (h16) total += 2 * b_range_bytes(4 * (rw + r0), 4 * (rw + r1));
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(&S.bar[k], total);
     unsigned char *st = S.stage[k];
     b_add_range(st + SG::OFF_RP, (const unsigned char *)a.prow, 4 * (ch.rpbase + r0), 4 * (ch.rpbase + r1 + 1),
                 &S.bar[k], h.sh_rp);
-    if (rsdg) {
+    if (h16) {
         b_add_range(st + SG::OFF_RS, (const unsigned char *)a.rscale, 4 * (rw + r0), 4 * (rw + r1), &S.bar[k], h.sh_rs);
         b_add_range(st + SG::OFF_DG, (const unsigned char *)a.diag32, 4 * (rw + r0), 4 * (rw + r1), &S.bar[k], h.sh_dg);
     }
     if (h.direct) return;
-    b_add_range(st + SG::OFF_COL, (const unsigned char *)a.col, 2 * (z0 + e0), 2 * (z0 + e1), &S.bar[k], h.sh_col);
-    const unsigned char *vsrc = MIX ? (ch.cls ? (const unsigned char *)a.val16 : (const unsigned char *)a.val32)
+    if (!h16)
+        b_add_range(st + SG::OFF_COL, (const unsigned char *)a.col, 2 * (z0 + e0), 2 * (z0 + e1), &S.bar[k], h.sh_col);
+    const unsigned char *vsrc = MIX ? (h16 ? (const unsigned char *)a.cv16 : (const unsigned char *)a.val32)
                                     : (const unsigned char *)a.val;
     b_add_range(st + SG::OFF_VAL, vsrc, vb * (z0 + e0), vb * (z0 + e1), &S.bar[k], h.sh_val);
 }
@@ -476,6 +482,29 @@ __device__ __forceinline__ double row_dot1_smem(int a, int e, const uint16_t *__
             const int c = (int)col[a + kk] & (PW - 1);
             const AT v = kk < n ? (AT)val[a + kk] : (AT)0;
             s = vfma(v, (AT)src(c), s);
+        }
+    }
+    double d = (double)s;
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o, L);
+    return d;
+}
+
+// The same for an FP16 pass: one 32-bit word per entry (FP16 value bits in
+// the high half, the column offset in the low half), so a slot costs one
+// shared-memory load besides its gather.
+template <int L, class Src>
+__device__ __forceinline__ double row_dot1_cv16(int a, int e, const uint32_t *__restrict__ cv, int lane, Src src)
+{
+    float s = 0.f;
+    const int n = e - a;
+    for (int k = lane; k < n; k += L * BU) {
+#pragma unroll
+        for (int u = 0; u < BU; u++) {
+            const int kk = k + u * L;
+            const uint32_t w = cv[a + kk];
+            const float v = kk < n ? __half2float(__ushort_as_half((unsigned short)(w >> 16))) : 0.f;
+            s = fmaf(v, (float)src((int)(w & (uint32_t)(PW - 1))), s);
         }
     }
     double d = (double)s;
@@ -905,8 +934,7 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                                 }
                             } else if constexpr (MIX) {
                                 if (h16)
-                                    y0 = row_dot1_smem<L, __half>(ra0 - h.e0, re0 - h.e0, scol, (const __half *)sval,
-                                                                  clane, psrc);
+                                    y0 = row_dot1_cv16<L>(ra0 - h.e0, re0 - h.e0, (const uint32_t *)sval, clane, psrc);
                                 else
                                     y0 = row_dot1_smem<L, float>(ra0 - h.e0, re0 - h.e0, scol, (const float *)sval,
                                                                  clane, psrc);
@@ -1278,8 +1306,8 @@ __global__ void k_batch_resid(BatchArgs a, const double *b, const double *x, dou
 // Row scale: 2^(e - 14) with e the exponent of the largest off-diagonal
 // magnitude; rows whose scale leaves FP32's normal range, or whose diagonal
 // does not fit FP32, are marked not FP16-capable.
-__global__ void k_batch_rows(BatchArgs a, float *val32, __half *val16, float *rscale, float *diag32, float4 *rowstat,
-                             unsigned char *rowflag)
+__global__ void k_batch_rows(BatchArgs a, float *val32, __half *val16, uint32_t *cv16, float *rscale, float *diag32,
+                             float4 *rowstat, unsigned char *rowflag)
 {
     for (int sys = blockIdx.x; sys < a.count; sys += gridDim.x) {
         const SysView V = sys_view(a, sys);
@@ -1313,6 +1341,7 @@ __global__ void k_batch_rows(BatchArgs a, float *val32, __half *val16, float *rs
                         if ((double)__half2float(h) * ldexp(1.0, e) != v) exact = false;
                     }
                     val16[eb + q] = h;
+                    cv16[eb + q] = ((uint32_t)__half_as_ushort(h) << 16) | (uint32_t)a.col[eb + q];
                 }
             }
             rscale[V.r0 + i] = ok ? ldexpf(1.f, e) : 0.f;
@@ -1558,6 +1587,7 @@ mf_status mf_batch_create(int count, const int *n, const int *const *rowptr, con
     BT_ALLOC(bt->d_val, sizeof(double) * (nz + 2));
     BT_ALLOC(bt->d_val32, sizeof(float) * (nz + 4));
     BT_ALLOC(bt->d_val16, sizeof(__half) * (nz + 16));
+    BT_ALLOC(bt->d_cv16, sizeof(uint32_t) * (nz + 8));
     BT_ALLOC(bt->d_rscale, sizeof(float) * (rows + 4));
     BT_ALLOC(bt->d_diag32, sizeof(float) * (rows + 4));
     BT_ALLOC(bt->d_ccls, (size_t)nch + 16);
@@ -1608,7 +1638,8 @@ mf_status mf_batch_create(int count, const int *n, const int *const *rowptr, con
         a.prow = bt->d_prow;
         a.col = bt->d_col;
         a.val = bt->d_val;
-        k_batch_rows<<<grid, 256>>>(a, bt->d_val32, bt->d_val16, bt->d_rscale, bt->d_diag32, rowstat, rowflag);
+        k_batch_rows<<<grid, 256>>>(a, bt->d_val32, bt->d_val16, bt->d_cv16, bt->d_rscale, bt->d_diag32, rowstat,
+                                    rowflag);
         note_launch();
         e = cudaGetLastError();
         if (e == cudaSuccess) {
@@ -1641,6 +1672,7 @@ mf_status mf_batch_destroy(mf_batch bt)
     void *bufs[] = {bt->d_order,  bt->d_n,      bt->d_pan0,   bt->d_npan,   bt->d_row0,   bt->d_prow0,
                     bt->d_pent0,  bt->d_prow,   bt->d_col,    bt->d_val,    bt->d_val32,  bt->d_val16,
                     bt->d_rscale, bt->d_diag32, bt->d_iters,  bt->d_refs,   bt->d_status, bt->d_relres,
+                    bt->d_cv16,
                     bt->work,     bt->d_queue,  bt->d_sc,     bt->d_crow,   bt->d_cent,   bt->d_ccls,
                     bt->d_ccls_static, bt->d_cstat, bt->d_cdyn, bt->d_sysstat};
     for (void *p : bufs)
@@ -1694,6 +1726,7 @@ static BatchArgs batch_args(mf_batch bt, const double *b, double *x, const mf_so
     a.val = bt->d_val;
     a.val32 = bt->d_val32;
     a.val16 = bt->d_val16;
+    a.cv16 = bt->d_cv16;
     a.rscale = bt->d_rscale;
     a.diag32 = bt->d_diag32;
     a.b = b;

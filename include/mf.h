@@ -107,7 +107,8 @@ mf_status mf_matrix_get_info(mf_matrix m, mf_matrix_info *info);
  * blockcsr_ptr_new (u8); Blockcsr_Val (f64); Blockcsr_Val_Low (f32);
  * nonzero_row_new, tile_rowidx, block_signal (int32); rowblkblock_rowidx
  * (u32), rowblkblock_colstart, rowblkblock_colstop (int32);
- * tile_class (u8, MF_CLASS_*); payload_f16 (u16 bits); payload_i8 (i8).
+ * tile_class (u8, MF_CLASS_*); tile_f16ok (u8: 1 when every FP16 payload
+ * value of the tile is finite); payload_f16 (u16 bits); payload_i8 (i8).
  * `bytes` must equal the array's size; mf_matrix_array_bytes tells it.
  */
 mf_status mf_matrix_array_bytes(mf_matrix m, const char *name, size_t *bytes);
@@ -200,6 +201,10 @@ typedef struct mf_solve_report {
     int layout;            /* execution layout of the solve: 0 tile chunks,
                               1 row slots, 2 staged row slots (the chunk's
                               vector entries copied to shared memory) */
+    int fallback_iteration;/* RULE / RULE_SCALED CG: the iteration
+                              at which the static classes took over because
+                              a refinement cycle under the policy's classes
+                              did not halve the FP64 residual; 0 if never */
 } mf_solve_report;
 
 /* The classes a rule policy gives every tile for the FP32 direction vectors
@@ -216,7 +221,9 @@ typedef struct mf_solve_report {
  * working (device, tilenum bytes, may be NULL) the class the mixed solver
  * runs each tile in: FP32 for FP64 and FP32 decisions, FP16 for FP16 and for
  * INT8 decisions on non-integer tiles, a narrower exact (value-range) class
- * kept.  Any other policy is MF_ERR_INVALID_ARG. */
+ * kept.  BYPASS drops the tile only under MF_POLICY_RULE_SCALED; under the
+ * absolute thresholds every segment is BYPASS once |p| falls below 1e-8, so
+ * there BYPASS runs like INT8.  Any other policy is MF_ERR_INVALID_ARG. */
 mf_status mf_rule_classes(mf_matrix m, int policy, const float *p_new, const float *p_old, unsigned char *decision,
                           unsigned char *working, void *stream);
 

@@ -56,7 +56,8 @@ class BatchReport(C.Structure):
 class SolveReport(C.Structure):
     _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("refinements", C.c_int), ("relres", C.c_double),
                 ("relres_true", C.c_double), ("kernel_ms", C.c_double), ("bytes_moved", C.c_longlong),
-                ("grid_ctas", C.c_int), ("phase_us", C.c_double * 9), ("layout", C.c_int)]
+                ("grid_ctas", C.c_int), ("phase_us", C.c_double * 9), ("layout", C.c_int),
+                ("fallback_iteration", C.c_int)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
@@ -71,7 +72,7 @@ ARRAY_DTYPES = {
     "Blockcsr_Ptr": np.uint8, "csr_compressedIdx": np.uint8, "nonzero_row_new": np.int32, "tile_rowidx": np.int32,
     "block_signal": np.int32, "blockrowid_new": np.uint8, "blockcsr_ptr_new": np.uint8,
     "rowblkblock_rowidx": np.uint32, "rowblkblock_colstart": np.int32, "rowblkblock_colstop": np.int32,
-    "tile_class": np.uint8, "payload_f16": np.uint16, "payload_i8": np.int8,
+    "tile_class": np.uint8, "tile_f16ok": np.uint8, "payload_f16": np.uint16, "payload_i8": np.int8,
 }
 
 _lib = None

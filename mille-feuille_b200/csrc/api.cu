@@ -168,8 +168,8 @@ mf_status mf_matrix_destroy(mf_matrix m)
 {
     if (!m) return MF_OK;
     void *bufs[] = {m->d_tile_ptr, m->d_tile_columnidx, m->d_tile_nnz, m->d_csrptr_offset, m->d_blknnznnz, m->d_val,
-                    m->d_val_low, m->d_col, m->d_ptr, m->d_cidx, m->d_f16, m->d_i8, m->d_class, m->d_nonzero_row_new,
-                    m->d_tile_rowidx, m->d_block_signal, m->d_blockrowid_new, m->d_blockcsr_ptr_new, m->d_rbb_rowidx,
+                    m->d_val_low, m->d_col, m->d_ptr, m->d_cidx, m->d_f16, m->d_i8, m->d_class, m->d_f16ok,
+                    m->d_nonzero_row_new, m->d_tile_rowidx, m->d_block_signal, m->d_blockrowid_new, m->d_blockcsr_ptr_new, m->d_rbb_rowidx,
                     m->d_rbb_colstart, m->d_rbb_colstop, m->d_part, m->d_cta_chunk, m->d_chunks, m->work, m->host_io,
                     m->d_wcls, m->d_poff, m->d_pay, m->d_resid, m->d_pol, m->d_sslot, m->d_smeta, m->d_sval,
                     m->d_shdr, m->d_spay, m->d_scta_chunk, m->d_schunks, m->d_spos, m->d_sdesc, m->mr_work,
@@ -231,6 +231,7 @@ static bool array_desc(mf_matrix m, const char *name, const void **ptr, size_t *
         {"rowblkblock_colstart", m->d_rbb_colstart, 4 * (size_t)m->rowblkblock},
         {"rowblkblock_colstop", m->d_rbb_colstop, 4 * (size_t)m->rowblkblock},
         {"tile_class", m->d_class, T},
+        {"tile_f16ok", m->d_f16ok, T},
         {"payload_f16", m->d_f16, 2 * nnz},
         {"payload_i8", m->d_i8, nnz},
     };
@@ -477,6 +478,12 @@ mf_status mf_cg_solve_multi_host(mf_matrix m, int k, const double *B_host, doubl
         return MF_ERR_CUDA;
     }
     const mf_status st = mf_cg_solve_multi(m, k, dB, (int)n, dX, (int)n, opts, reports, s);
+    // X is only written when the solve ran: a call rejected before its
+    // kernels (bad options, an unsupported policy) leaves X_host untouched.
+    if (st != MF_OK && st != MF_ERR_NOT_CONVERGED && st != MF_ERR_BREAKDOWN) {
+        cudaStreamSynchronize(s);
+        return st;
+    }
     e = cudaMemcpyAsync(X_host, dX, bytes, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {

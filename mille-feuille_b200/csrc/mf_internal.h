@@ -45,6 +45,7 @@ struct mf_matrix_s {
     uint16_t *d_f16 = nullptr;
     int8_t *d_i8 = nullptr;
     unsigned char *d_class = nullptr;
+    unsigned char *d_f16ok = nullptr;  // per tile: 1 when every FP16 payload value is finite
     // derived reference arrays (src/main-cg.cu:1231-1288, blockspmv_cpu.h:35-83)
     int *d_nonzero_row_new = nullptr, *d_tile_rowidx = nullptr, *d_block_signal = nullptr;
     unsigned char *d_blockrowid_new = nullptr, *d_blockcsr_ptr_new = nullptr;

@@ -181,29 +181,35 @@ __global__ void k_seg_rule(int nseg, int n, const VT *__restrict__ pn, const VT 
 // decisions (the inner solver's vectors and sums are FP32; FP64 accuracy
 // comes from the reliable updates), FP16 for FP16 and for INT8 decisions on
 // tiles that are not integers, and an exact class narrower than the decided
-// one is kept.
-__device__ __forceinline__ int exec_class(int d, int c)
+// one is kept.  A BYPASS decision drops the tile only under the scaled rule
+// (keep_bypass): the absolute thresholds call every segment converged once
+// |p| itself falls below 1e-8, which would empty the product, so there it
+// runs like an INT8 decision.  An inexact tile whose FP16 payload is not
+// finite (ok16 = 0) runs FP16 decisions in FP32.
+__device__ __forceinline__ int exec_class(int d, int c, bool keep_bypass, bool ok16)
 {
     int w;
     if (d == MF_CLASS_FP64 || d == MF_CLASS_FP32) w = MF_CLASS_FP32;
     else if (d == MF_CLASS_FP16) w = MF_CLASS_FP16;
-    else if (d == MF_CLASS_INT8) w = (c == MF_CLASS_INT8) ? MF_CLASS_INT8 : MF_CLASS_FP16;
+    else if (d == MF_CLASS_INT8 || !keep_bypass) w = (c == MF_CLASS_INT8) ? MF_CLASS_INT8 : MF_CLASS_FP16;
     else w = MF_CLASS_BYPASS;
     if (w == MF_CLASS_FP32 && (c == MF_CLASS_FP16 || c == MF_CLASS_INT8)) w = c;
     if (w == MF_CLASS_FP16 && c == MF_CLASS_INT8) w = c;
+    if (w == MF_CLASS_FP16 && c != MF_CLASS_FP16 && !ok16) w = MF_CLASS_FP32;
     return w;
 }
 
 // Tile t takes the decision of its column segment (the p segment it
 // multiplies), as the reference's SpMV reads d_vis[tile column].
 __global__ void k_rule_tiles(int T, const int *__restrict__ tile_col, const unsigned char *__restrict__ cls,
-                             const unsigned char *__restrict__ seg_cls, unsigned char *__restrict__ decision,
+                             const unsigned char *__restrict__ ok16, const unsigned char *__restrict__ seg_cls,
+                             unsigned char *__restrict__ decision,
                              unsigned char *__restrict__ w)
 {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
         const int d = seg_cls[tile_col[t]];
         if (decision) decision[t] = (unsigned char)d;
-        if (w) w[t] = (unsigned char)exec_class(d, cls[t]);
+        if (w) w[t] = (unsigned char)exec_class(d, cls[t], false, ok16[t] != 0);
     }
 }
 
@@ -213,7 +219,7 @@ __global__ void k_rule_tiles(int T, const int *__restrict__ tile_col, const unsi
 // 1e-7 < v <= 1e-6 -> FP16, 1e-8 < v <= 1e-7 -> INT8, else BYPASS (no FP64
 // decision: FP32 is the inner solver's widest class).
 __global__ void k_rule_scaled_classes(int T, const int *__restrict__ tile_col, const unsigned char *__restrict__ cls,
-                                      const float *__restrict__ seg_dp, const unsigned *__restrict__ pmax_bits,
+                                      const unsigned char *__restrict__ ok16, const float *__restrict__ seg_dp, const unsigned *__restrict__ pmax_bits,
                                       unsigned char *__restrict__ decision, unsigned char *__restrict__ w)
 {
     const float pmax = __uint_as_float(*pmax_bits);
@@ -225,7 +231,7 @@ __global__ void k_rule_scaled_classes(int T, const int *__restrict__ tile_col, c
         else if (v > 1e-8f) d = MF_CLASS_INT8;
         else d = MF_CLASS_BYPASS;
         if (decision) decision[t] = (unsigned char)d;
-        if (w) w[t] = (unsigned char)exec_class(d, cls[t]);
+        if (w) w[t] = (unsigned char)exec_class(d, cls[t], true, ok16[t] != 0);
     }
 }
 
@@ -254,7 +260,8 @@ mf_status rule_classes(mf_matrix m, int policy, const void *p_new, const void *p
             MF_CUDA(cudaGetLastError());
         }
         if (T > 0) {
-            k_rule_tiles<<<grid_for2(T, 256), 256, 0, s>>>(T, m->d_tile_columnidx, m->d_class, seg, d_decision, d_wcls);
+            k_rule_tiles<<<grid_for2(T, 256), 256, 0, s>>>(T, m->d_tile_columnidx, m->d_class, m->d_f16ok, seg, d_decision,
+                                                              d_wcls);
             note_launch();
             MF_CUDA(cudaGetLastError());
         }
@@ -272,7 +279,7 @@ mf_status rule_classes(mf_matrix m, int policy, const void *p_new, const void *p
         MF_CUDA(cudaGetLastError());
     }
     if (T > 0) {
-        k_rule_scaled_classes<<<grid_for2(T, 256), 256, 0, s>>>(T, m->d_tile_columnidx, m->d_class, seg, pmax,
+        k_rule_scaled_classes<<<grid_for2(T, 256), 256, 0, s>>>(T, m->d_tile_columnidx, m->d_class, m->d_f16ok, seg, pmax,
                                                                  d_decision, d_wcls);
         note_launch();
         MF_CUDA(cudaGetLastError());

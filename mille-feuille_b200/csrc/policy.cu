@@ -249,6 +249,8 @@ __global__ void k_mlp_classify(FeatIn f, const __nv_bfloat16 *__restrict__ wq, u
         if (best == 0) w = (c == MF_CLASS_INT8) ? MF_CLASS_INT8 : MF_CLASS_BYPASS;
         else if (best == 1) w = (c == MF_CLASS_INT8) ? MF_CLASS_INT8 : MF_CLASS_FP16;
         else w = (c == MF_CLASS_INT8 || c == MF_CLASS_FP16) ? c : MF_CLASS_FP32;
+        // an inexact tile beyond binary16's range stays FP32
+        if (w == MF_CLASS_FP16 && c != MF_CLASS_FP16 && !(f.vmax[t] <= 65504.f)) w = MF_CLASS_FP32;
         wcls[t] = (unsigned char)w;
     }
 }

@@ -33,13 +33,20 @@ double *g_part_ptr[MAX_DEVICES] = {nullptr};
 // Device address of the scratch array on the current device (set up once per
 // device, with that device current).  In host code the array's name is only
 // a host-side stand-in, so its device address must come from the runtime.
-mf_status scratch_address(double **out)
+// The matrix must live on the current device: its pointers are used by
+// kernels launched there.
+mf_status scratch_address(int matrix_device, double **out)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
         mf::set_last_error("mf_residual_norm_noalloc: no usable current device (%s)", cudaGetErrorString(e));
         return MF_ERR_NO_DEVICE;
+    }
+    if (dev != matrix_device) {
+        mf::set_last_error("mf_residual_norm_noalloc: the matrix lives on device %d but device %d is current",
+                           matrix_device, dev);
+        return MF_ERR_INVALID_ARG;
     }
     std::lock_guard<std::mutex> lk(g_setup_mu);
     if (!g_part_ptr[dev]) {
@@ -77,6 +84,6 @@ extern "C" mf_status mf_residual_norm_noalloc(mf_matrix m, const double *b, cons
         return MF_ERR_INVALID_ARG;
     }
     double *part = nullptr;
-    MF_TRY(scratch_address(&part));
+    MF_TRY(scratch_address(m->device, &part));
     return mf::residual_norm(m->v, b, x, part, out, (cudaStream_t)stream);
 }

@@ -156,6 +156,10 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
     MF_CUDA(cudaEventRecord(e0, s));
     double st[S_COUNT];
     int h_status = 0, launches = 0;
+    // stagnation guard of the dynamic policies: FP64 residual and
+    // refinement count at the last reliable update
+    double guard_relres = 1.0;
+    int guard_refs = 0;
     for (;;) {
         MF_CUDA(cudaMemsetAsync(w.bar, 0, 9 * 128, s));
         if (bicg) MF_TRY(launch_bicgstab(mixed, a, G, s));
@@ -172,9 +176,25 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
         const void *pnew = (it & 1) ? w.p1 : w.p0;  // written by the last iteration
         const void *pold = (it & 1) ? w.p0 : w.p1;
         if (hook) MF_TRY(hook->fn(hook->ctx, m, w, pnew, pold, it, st[S_RELRES], s));
-        if (o.policy == MF_POLICY_FP64 || o.policy == MF_POLICY_STATIC) {
+        if (o.policy == MF_POLICY_FP64 || o.policy == MF_POLICY_STATIC || rep.fallback_iteration > 0) {
             a.start = 0;
             continue;
+        }
+        const bool rule = o.policy == MF_POLICY_RULE || o.policy == MF_POLICY_RULE_SCALED;
+        if (rule && a.exit_on_refine && (int)st[S_REFS] > guard_refs) {
+            // a whole refinement cycle under the rule's classes that did not
+            // halve the FP64 residual (and did not end the solve): the static
+            // classes take over for the rest of it (no further checkpoints)
+            if (!(st[S_RELRES] <= 0.5 * guard_relres) && !(a.fixed == 0 && st[S_RELRES] <= o.tol)) {
+                MF_TRY(static_working_classes(m, m->d_wcls, s));
+                MF_TRY(repack(MF_POLICY_STATIC));
+                a.exit_on_refine = 0;
+                a.start = 0;
+                rep.fallback_iteration = (int)st[S_ITERS];
+                continue;
+            }
+            guard_relres = st[S_RELRES];
+            guard_refs = (int)st[S_REFS];
         }
         if (o.policy == MF_POLICY_RULE || o.policy == MF_POLICY_RULE_SCALED) {
             MF_TRY(rule_classes(m, o.policy, pnew, pold, nullptr, m->d_wcls, s));

@@ -305,13 +305,16 @@ __global__ void k_rbb_fill(int tilem, const int *__restrict__ tile_ptr, const in
 //   fp64 : otherwise
 // Payloads: fp16 = (half)(float)v, int8 = (int8_t)v (low byte of the
 // truncated 32-bit integer), as src/main-cg-mixed.cu:2333-2336 builds them.
+// f16ok: every FP16 payload value of the tile is finite (|v| within
+// binary16's range), the condition for running an inexact tile in FP16.
 __global__ void k_payloads(int T, const int *__restrict__ tile_nnz, const double *__restrict__ val,
                            const float *__restrict__ low, uint16_t *__restrict__ f16, int8_t *__restrict__ i8,
-                           unsigned char *__restrict__ cls, int *__restrict__ class_count, int *__restrict__ max_nz)
+                           unsigned char *__restrict__ cls, unsigned char *__restrict__ f16ok,
+                           int *__restrict__ class_count, int *__restrict__ max_nz)
 {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
         const int a = tile_nnz[t], b = tile_nnz[t + 1];
-        bool is_int8 = true, in16 = true, in32 = true;
+        bool is_int8 = true, in16 = true, in32 = true, fin16 = true;
         for (int k = a; k < b; k++) {
             const double v = val[k];
             const double av = fabs(v);
@@ -323,7 +326,9 @@ __global__ void k_payloads(int T, const int *__restrict__ tile_nnz, const double
             const float vf = (float)v;
             if ((double)vf != v) in32 = false;
             if ((double)__half2float(h) != v) in16 = false;
+            if (__hisinf(h) || __hisnan(h)) fin16 = false;
         }
+        f16ok[t] = fin16 ? 1 : 0;
         unsigned char c = is_int8 ? MF_CLASS_INT8 : in16 ? MF_CLASS_FP16 : in32 ? MF_CLASS_FP32 : MF_CLASS_FP64;
         cls[t] = c;
         atomicAdd(&class_count[c], 1);
@@ -540,9 +545,10 @@ mf_status build_tiles(mf_matrix m, int rowA, int colA, const int *d_rowptr, cons
     MF_TRY(dalloc(&m->d_f16, nnz, &acc));
     MF_TRY(dalloc(&m->d_i8, nnz, &acc));
     MF_TRY(dalloc(&m->d_class, T, &acc));
+    MF_TRY(dalloc(&m->d_f16ok, T, &acc));
     if (T > 0) {
         k_payloads<<<grid_for(T, 256), 256, 0, s>>>(T, m->d_tile_nnz, m->d_val, m->d_val_low, m->d_f16, m->d_i8,
-                                                    m->d_class, d_class_count, d_maxnz);
+                                                    m->d_class, m->d_f16ok, d_class_count, d_maxnz);
         note_launch();
         MF_CUDA(cudaGetLastError());
     }

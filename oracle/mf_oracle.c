@@ -426,10 +426,13 @@ int orc_rule_class(double v)
  * same thresholds (without the FP64 class) on max_seg |pn - po| / max |pn|
  * in FP32.  A tile takes its column segment's decision; the working class
  * maps FP64 / FP32 decisions to FP32, FP16 to FP16, INT8 to INT8 on integer
- * tiles (static class INT8) and FP16 otherwise, BYPASS to BYPASS, and keeps
- * a narrower exact static class (INT8, FP16). */
-void orc_rule_tiles(int n, int tilen, int T, const int *tile_col, const unsigned char *static_cls, const float *pn,
-                    const float *po, int scaled, unsigned char *decision, unsigned char *working)
+ * tiles (static class INT8) and FP16 otherwise, BYPASS to BYPASS under the
+ * scaled rule and like INT8 under the absolute one, and keeps a narrower
+ * exact static class (INT8, FP16); an inexact tile whose FP16 payload is not
+ * finite (f16ok[t] = 0; NULL: all finite) runs FP16 in FP32. */
+void orc_rule_tiles(int n, int tilen, int T, const int *tile_col, const unsigned char *static_cls,
+                    const unsigned char *f16ok, const float *pn, const float *po, int scaled, unsigned char *decision,
+                    unsigned char *working)
 {
     int *seg = (int *)malloc(sizeof(int) * (tilen > 0 ? tilen : 1));
     float pmax = 0.f;
@@ -459,10 +462,11 @@ void orc_rule_tiles(int n, int tilen, int T, const int *tile_col, const unsigned
         int d = seg[tile_col[t]], c = static_cls[t], w;
         if (d == 0 || d == 4) w = 4;
         else if (d == 3) w = 3;
-        else if (d == 2) w = (c == 2) ? 2 : 3;
+        else if (d == 2 || !scaled) w = (c == 2) ? 2 : 3;  /* absolute rule: BYPASS runs as INT8 */
         else w = 1;
         if (w == 4 && (c == 3 || c == 2)) w = c;
         if (w == 3 && c == 2) w = c;
+        if (w == 3 && c != 3 && f16ok && !f16ok[t]) w = 4;
         decision[t] = (unsigned char)d;
         working[t] = (unsigned char)w;
     }

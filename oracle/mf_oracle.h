@@ -84,8 +84,9 @@ void orc_batch_classify(int n, const int *rp, const int *ci, const double *val, 
                         double relres, int refs, int have_prev, float *prev, const float *w, float *feat,
                         unsigned char *cls, double *margin);
 /* Per-tile rule decision and working class for FP32 directions (see .c). */
-void orc_rule_tiles(int n, int tilen, int T, const int *tile_col, const unsigned char *static_cls, const float *pn,
-                    const float *po, int scaled, unsigned char *decision, unsigned char *working);
+void orc_rule_tiles(int n, int tilen, int T, const int *tile_col, const unsigned char *static_cls,
+                    const unsigned char *f16ok, const float *pn, const float *po, int scaled, unsigned char *decision,
+                    unsigned char *working);
 
 /* CSR SpMV and FP64 solvers (textbook order; sequential sums). */
 void orc_csr_spmv(int n, const int *rowptr, const int *colidx, const double *val,

@@ -17,6 +17,15 @@ ROOT = Path(__file__).resolve().parent.parent
 ORACLE_SO = ROOT / "oracle" / "liboracle.so"
 REF_SO = ROOT / "oracle" / "_ref" / "libmfref.so"
 
+
+def reference_root():
+    """The reference checkout: $MF_REFERENCE_ROOT, else a `reference`
+    directory beside this repository; None when neither exists (tests that
+    read its files then skip)."""
+    env = os.environ.get("MF_REFERENCE_ROOT")
+    cand = Path(env) if env else ROOT.parent / "reference"
+    return cand if cand.is_dir() else None
+
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -91,7 +100,8 @@ def oracle() -> C.CDLL:
         lib.orc_f32_to_f16_bits.restype = C.c_uint16
         lib.orc_payload_casts.argtypes = [_f64p, C.c_int, _f32p, _u16p, _i8p]
         lib.orc_rule_class.argtypes = [C.c_double]
-        lib.orc_rule_tiles.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _u8p, _f32p, _f32p, C.c_int, _u8p, _u8p]
+        lib.orc_rule_tiles.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _u8p, C.c_void_p, _f32p, _f32p, C.c_int, _u8p,
+                                       _u8p]
         lib.orc_rule_tiles.restype = None
         lib.orc_f64_to_f16_bits.argtypes = [C.c_double]
         lib.orc_f64_to_f16_bits.restype = C.c_uint16
@@ -274,14 +284,18 @@ def oracle_true_relres(csr: Csr, b, x) -> float:
                                     np.ascontiguousarray(b, np.float64), np.ascontiguousarray(x, np.float64))
 
 
-def oracle_rule_tiles(n, tilen, tile_col, static_cls, pn, po, scaled=False):
+def oracle_rule_tiles(n, tilen, tile_col, static_cls, pn, po, scaled=False, f16ok=None):
     """Per-tile rule decision and working class (the restatement of the
-    reference's partial-convergence rule, src/main-cg-mixed.cu:415-460)."""
+    reference's partial-convergence rule, src/main-cg-mixed.cu:415-460);
+    f16ok (u8 per tile, None: all finite) marks tiles whose FP16 payload is
+    finite."""
     T = len(tile_col)
     dec = np.zeros(max(T, 1), np.uint8)
     work = np.zeros(max(T, 1), np.uint8)
+    ok = None if f16ok is None else np.ascontiguousarray(f16ok, np.uint8)
     oracle().orc_rule_tiles(n, tilen, T, np.ascontiguousarray(tile_col, np.int32),
-                            np.ascontiguousarray(static_cls, np.uint8), np.ascontiguousarray(pn, np.float32),
+                            np.ascontiguousarray(static_cls, np.uint8), None if ok is None else ok.ctypes.data,
+                            np.ascontiguousarray(pn, np.float32),
                             np.ascontiguousarray(po, np.float32), 1 if scaled else 0, dec, work)
     return dec[:T], work[:T]
 

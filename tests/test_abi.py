@@ -65,6 +65,19 @@ def test_invalid_arguments_rejected_without_device(mf):
     assert b"null" in L.mf_last_error()
 
 
+def test_noalloc_residual_argument_checks_without_device(mf):
+    """mf_residual_norm_noalloc rejects a null matrix, vector or output
+    before it touches a device (the scratch lookup and the matrix's device
+    check come after these)."""
+    L = mf.lib()
+    buf = (ctypes.c_double * 3)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    for args in [(None, p, p, p), (p, None, p, p), (p, p, None, p), (p, p, p, None)]:
+        assert L.mf_residual_norm_noalloc(*args, None) == 1  # MF_ERR_INVALID_ARG
+        assert b"null argument" in L.mf_last_error()
+    assert list(buf) == [0.0, 0.0, 0.0]
+
+
 @pytest.mark.parametrize("libname", ["libmf_solvers.so", "libmf_solvers_mixed.so"])
 def test_solver_entry_libraries_export_reference_names(mf, libname):
     """cg_solve_inc/sync/reduce and bicgstab/_sync/_inc, as declared in
@@ -87,8 +100,11 @@ def test_tile_matrix_layout_matches_reference_field_order():
     names = [n for n, _ in f]
     assert names[:6] == ["tilem", "tilen", "tilenum", "tile_ptr", "tile_columnidx", "tile_nnz"]
     assert names.index("csrsize") == names.index("csr_compressedIdx") + 1
-    ref = ROOT.parent / "reference" / "src" / "format.h"
-    if ref.exists():
+    import oracle_lib
+
+    root = oracle_lib.reference_root()
+    ref = root / "src" / "format.h" if root is not None else None
+    if ref is not None and ref.exists():
         body = ref.read_text()
         body = body[body.index("typedef struct\n{"): body.index("} Tile_matrix;")]
         import re as _re

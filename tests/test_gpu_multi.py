@@ -164,9 +164,15 @@ def test_multi_rejects(mf):
     for k in (0, 17):
         o = mf.solve_opts()
         assert L.mf_cg_solve_multi_host(M.h, k, B.ctypes.data, X.ctypes.data, C.byref(o), reps) == 1
+    # a solve run first leaves the staging buffer holding a solution ...
+    o = mf.solve_opts()
+    assert L.mf_cg_solve_multi_host(M.h, 2, B.ctypes.data, X.ctypes.data, C.byref(o), reps) == 0
     for kw in (dict(policy="static"), dict(precond=1)):
+        # ... which an UNSUPPORTED call must not copy into the caller's X
+        X[:] = 7.25
         o = mf.solve_opts(**kw)
         assert L.mf_cg_solve_multi_host(M.h, 2, B.ctypes.data, X.ctypes.data, C.byref(o), reps) == 8
+        assert np.all(X == 7.25)
     o = mf.solve_opts()
     assert L.mf_cg_solve_multi(M.h, 2, None, n - 1, None, n, C.byref(o), reps, None) == 1
     assert L.mf_spmm(M.h, 0, None, n, None, n, None) == 1

@@ -54,8 +54,15 @@ def _run(mf, A, policy, seed):
     assert st == 0, lib.mf_last_error()
     tile_col = M.export("tile_columnidx")
     static_cls = M.export("tile_class")
+    f16ok = M.export("tile_f16ok")
+    # f16ok against the FP16 payload itself: 0 exactly where a value is inf
+    tnz = M.export("tile_nnz")
+    f16 = M.export("payload_f16")
+    inf = np.concatenate([[0], np.cumsum((f16 & 0x7C00) == 0x7C00)])
+    per_tile = inf[tnz[1:]] - inf[tnz[:-1]]
+    assert np.array_equal(f16ok, (per_tile == 0).astype(np.uint8))
     want_dec, want_wrk = ol.oracle_rule_tiles(A.n_cols, info.tilen, tile_col, static_cls, pn, po,
-                                              scaled=(policy == "rule_scaled"))
+                                              scaled=(policy == "rule_scaled"), f16ok=f16ok)
     got_dec, got_wrk = dec.cpu().numpy(), wrk.cpu().numpy()
     M.close()
     return got_dec, got_wrk, want_dec, want_wrk
@@ -65,6 +72,7 @@ CASES = [
     ("poisson3d_64", lambda mf: mf.synth_poisson3d_scaled(64, 1)),
     ("laplace2d_128", lambda mf: mf.synth_laplace2d(128, 128)),
     ("laplace2d_ragged", lambda mf: mf.synth_laplace2d(37, 29)),
+    ("aniso_64", lambda mf: mf.synth_aniso3d(64, 3)),  # values beyond binary16's range
 ]
 
 

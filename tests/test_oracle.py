@@ -13,7 +13,8 @@ import matrices
 import oracle_lib as ol
 
 GOLDEN = json.loads((Path(__file__).parent / "golden" / "tiles.json").read_text())
-ADD20 = Path("/root/reference/test/add20.mtx")
+_REF_ROOT = ol.reference_root()
+ADD20 = _REF_ROOT / "test" / "add20.mtx" if _REF_ROOT is not None else Path("add20.mtx.absent")
 
 
 def digest(a):
@@ -161,20 +162,26 @@ def test_rule_tiles_restatement():
     pn = (po.astype(np.float64) + d).astype(np.float32)
     tile_col = rng.integers(0, tilen, T).astype(np.int32)
     static = rng.choice([0, 2, 3, 4], T).astype(np.uint8)
-    dec, work = ol.oracle_rule_tiles(n, tilen, tile_col, static, pn, po)
+    ok16 = (rng.uniform(size=T) < 0.8).astype(np.uint8)
+    ok16[static == 3] = 1  # an exact FP16 tile is finite in FP16
+    dec, work = ol.oracle_rule_tiles(n, tilen, tile_col, static, pn, po, f16ok=ok16)
     v = np.zeros(tilen)
     np.maximum.at(v, np.arange(n) // 16, np.abs(pn.astype(np.float64) - po.astype(np.float64)))
     seg = np.select([v > 1e-5, v > 1e-6, v > 1e-7, v > 1e-8], [0, 4, 3, 2], 1)
     assert dec.tolist() == seg[tile_col].tolist()
     want = []
-    for dd, c in zip(seg[tile_col], static):
-        w = {0: 4, 4: 4, 3: 3, 2: 2 if c == 2 else 3, 1: 1}[int(dd)]
+    for dd, c, ok in zip(seg[tile_col], static, ok16):
+        # BYPASS runs like INT8 under the absolute thresholds
+        w = {0: 4, 4: 4, 3: 3, 2: 2 if c == 2 else 3, 1: 2 if c == 2 else 3}[int(dd)]
         if w == 4 and c in (2, 3):
             w = int(c)
         if w == 3 and c == 2:
             w = 2
+        if w == 3 and c != 3 and not ok:
+            w = 4
         want.append(w)
     assert work.tolist() == want
+    assert 1 in dec.tolist() and 4 in work.tolist()
 
 
 def test_oracle_cg_on_laplacian(mf):

@@ -96,7 +96,7 @@ def ncu_traffic(kernel, workload, policy):
     if not p.exists():
         return None
     e = json.loads(p.read_text()).get(kernel)
-    if e is None or e.get("workload") != workload or e.get("policy") != policy:
+    if e is None or e.get("workload") != workload or (e.get("policy") is not None and e.get("policy") != policy):
         return None
     return e
 
@@ -549,6 +549,74 @@ def workload_single(args, mf, world, local):
     return result, info
 
 
+def workload_spmv(args, mf, world, local):
+    """The standalone FP64 tiled SpMV (mf_spmv, k_spmv_fp64) on the
+    poisson3d matrix; value = SpMVs per second.  Algorithmic bytes of one
+    SpMV: nnz x (8-byte value + 1-byte in-tile column) + 24 bytes per tile
+    (tile column, entry offset, 16 row pointers) + x read once and y written
+    once (16 bytes per row)."""
+    import torch
+
+    L = mf.lib()
+    A = mf.synth_poisson3d_scaled(GRID, SEED)
+    M = mf.Matrix(A)
+    inf = M.info()
+    n, T = A.n_rows, inf.tilenum
+    xs = mf.synth_xstar(SEED, inf.tilen * 16)
+    dx = torch.from_numpy(xs).cuda()
+    dy = torch.zeros(n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    reps = 20  # SpMVs per step
+
+    def spmv():
+        for _ in range(reps):
+            st = L.mf_spmv(M.h, dx.data_ptr(), dy.data_ptr(), stream.cuda_stream)
+            if st != 0:
+                mf.check(st)
+
+    for _ in range(args.warmup):
+        spmv()
+    torch.cuda.synchronize()
+    _barrier(world)
+    launches0 = L.mf_kernel_launches()
+    with ClockSampler(local) as clk:
+        ms = _timed(stream, spmv, args.steps)
+    launches = L.mf_kernel_launches() - launches0
+    ms = _max_over_ranks(ms, world)
+    value = reps * args.steps * world / (ms * 1e-3)
+    result = {"ms": ms, "value": value, "launches": launches, "clocks": clk.summary(),
+              "metric": "FP64 tiled SpMV/s (mf_spmv, bit-identical to the reference's blockspmv_cpu), 1 B200",
+              "unit": "spmv/s"}
+    if args.profile:
+        return result, None
+    y = dy.cpu().numpy()
+    err = float(np.max(np.abs(y - A.matvec(xs[:n]))) / max(1e-300, np.max(np.abs(y))))
+    bytes_spmv = A.nnz * 9 + 24 * T + 16 * n
+    info = {"workload": f"poisson3d_scaled_{GRID}^3 mf_spmv", "n": n, "nnz": A.nnz, "tiles": T,
+            "spmv_per_step": reps, "rel_diff_vs_scipy": err, "parallelism": f"replicas x{world}",
+            "l2": "matrix (186 MB) larger than L2; no flush between SpMVs"}
+    # e2e: x from pinned host memory, one SpMV, y back, every step
+    x_pin = torch.from_numpy(xs).pin_memory()
+    y_pin = torch.zeros(n, dtype=torch.float64).pin_memory()
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dx.copy_(x_pin, non_blocking=True)
+        L.mf_spmv(M.h, dx.data_ptr(), dy.data_ptr(), stream.cuda_stream)
+        y_pin.copy_(dy, non_blocking=True)
+        torch.cuda.synchronize()
+        e2e_s += time.perf_counter() - t0
+    e2e_s = _max_over_ranks(e2e_s, world)
+    result["e2e"] = {"value": args.steps * world / e2e_s, "unit": "spmv/s", "h2d_bytes_per_step": 8 * len(xs),
+                     "d2h_bytes_per_step": 8 * n}
+    result["roofline_in"] = (bytes_spmv, ms / (reps * args.steps), "k_spmv_fp64", None)
+    result["dtype"] = "f64"
+    result["cpu"] = None
+    M.close()
+    return result, info
+
+
 BATCH_NAME = ("batched random SPD x512 (n ~ log-uniform[1k,64k], seeds 100-611, 8-32 draws per row, "
               "row scale 10^U[-4,4]) CG to 1e-10")
 
@@ -818,6 +886,8 @@ def run_mf(args):
         res, info = workload_batched(args, mf, world, local)
     elif args.workload == "multirhs":
         res, info = workload_multi(args, mf, world, local)
+    elif args.workload == "spmv":
+        res, info = workload_spmv(args, mf, world, local)
     else:
         res, info = workload_single(args, mf, world, local)
     if args.profile:
@@ -832,13 +902,16 @@ def run_mf(args):
     achieved = per_launch / (mean_ms * 1e-3) / 1e9
     tr = ncu_traffic(kname, args.workload, args.policy)
     traffic = None
-    if tr is not None and mean_iters is not None:
+    if tr is not None and "dram_bytes_per_launch" in tr:
+        traffic = tr["dram_bytes_per_launch"]
+    elif tr is not None and mean_iters is not None:
         traffic = tr["dram_bytes_per_iteration"] * mean_iters
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_kind": peak_kind, "kernel": kname,
                 "algorithmic_bytes_per_launch": per_launch, "launch_ms": mean_ms}
     line = {
-        "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": res.get("metric", METRIC), "value": res["value"], "unit": res.get("unit", UNIT), "n_gpus": world,
+        "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": res["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": res["dtype"], "data": "synthetic", "config": info, "roofline": roofline,
         "e2e": res["e2e"], "gpu_launches": int(res["launches"]), "clocks": res["clocks"],
@@ -881,7 +954,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mf", "reference"], default="mf")
     ap.add_argument("--workload", default="batched",
-                    choices=["batched", "poisson3d", "lap2d", "convdiff", "aniso", "multirhs"])
+                    choices=["batched", "poisson3d", "lap2d", "convdiff", "aniso", "multirhs", "spmv"])
     ap.add_argument("--rhs", type=int, default=16, help="multirhs workload: right-hand sides (1-16)")
     ap.add_argument("--policy", default=None, choices=["fp64", "static", "rule", "learned"],
                     help="precision policy (default: learned for batched, static otherwise)")

@@ -169,6 +169,8 @@ struct BatchArgs {
     double tol;
     double delta;
     unsigned long long budget_ns;  // bound of every shared-memory stage wait
+    unsigned backoff_ns;           // sleep between retries of a stage wait
+    int rowsum;                    // mixed passes: 0 two-phase row sums, 1 lane groups per row
     int policy;
     const __nv_bfloat16 *mlp_w;    // LEARNED: the network's BF16 weights
     // trace collection (FP64 solves): samples every collect_every iterations
@@ -701,7 +703,7 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
     if (threadIdx.x == 0) {
         for (int k = 0; k < NS; k++) {
             mbar_init(&S.bar[k], 1);
-            mbar_init(&S.empty[k], BNW - 1);
+            mbar_init(&S.empty[k], MIX ? (BNW - 1) / NS : BNW - 1);  // the stage's consumer warps
         }
         mbar_init(&S.pbar, 1);
         mbar_init(&S.wempty, BNW - 1);
@@ -856,7 +858,9 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                             int ok = 1;
                             if (wl == 0) {
                                 if (MIX && j % nchl == 0) {
-                                    if (wstarted) ok = mbar_wait_sleep_bounded(&S.wempty, wpar ^ 1u, a.queue + 1, a.budget_ns);
+                                    if (wstarted)
+                                        ok = mbar_wait_sleep_bounded(&S.wempty, wpar ^ 1u, a.queue + 1, a.budget_ns,
+                                                                     a.backoff_ns);
                                     if (ok) {
                                         issue_pwin(&S.pbar, s_win, (const float *)pnew, V.n, j / nchl, s_pshift);
                                         wpar ^= 1u;
@@ -865,7 +869,7 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                                 }
                                 if (ok && ((pstarted >> k) & 1u))
                                     ok = mbar_wait_sleep_bounded(&S.empty[k], ((pfill >> k) & 1u) ^ 1u, a.queue + 1,
-                                                           a.budget_ns);
+                                                           a.budget_ns, a.backoff_ns);
                                 if (ok) {
                                     b_issue<MIX>(a, S, ch, k);
                                     pfill ^= 1u << k;
@@ -883,93 +887,156 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                         }
                     }
                 } else {
-                    const int ct = tid - 32;            // consumer thread (warp-aligned)
+                    // consumer warps in NS groups: group g consumes stage g,
+                    // i.e. passes j with j % NS == g, its CWS warps splitting
+                    // each pass's rows; every consumer warp waits for each
+                    // panel's window and releases it after its own passes
+                    // of that panel
+                    // (mixed kernel; the FP64 kernel's consumer warps all
+                    // take every pass, so that a row's panels are added in
+                    // panel order without a window to order them)
+                    constexpr int NCW = BNW - 1;
+                    constexpr int CWS = MIX ? NCW / NS : NCW;   // consumer warps per stage
+                    static_assert(NCW % NS == 0, "consumer warps split evenly over the stages");
+                    const int cw = wid - 1;
+                    const int kg = MIX ? cw / CWS : 0;          // this warp's stage (mixed kernel)
+                    const int gr = cw % CWS;                    // warp within the stage's group
+                    const int ct = gr * 32 + wl;                // thread within the stage's group
                     const int clane = ct % L, cgrp = ct / L;
-                    constexpr int GPC = (BNT - 32) / L;  // consumer row groups
-                    for (int j = 0; j < J; j++) {
-                        const int k = j % NS;
-                        const int jp = j % nchl;
-                        bool w = true;
-                        if (MIX && jp == 0) {
-                            w = mbar_wait_sleep_bounded(&S.pbar, cwpar, a.queue + 1, a.budget_ns);
+                    constexpr int GPC = CWS * 32 / L;           // row groups per stage
+                    const int nwin = MIX ? npan : 1;
+                    for (int pw = 0; pw < nwin && !fail; pw++) {
+                        const int j0 = MIX ? pw * nchl : 0, j1 = MIX ? j0 + nchl : J;
+                        if (MIX) {
+                            const bool ww =
+                                mbar_wait_sleep_bounded(&S.pbar, cwpar, a.queue + 1, a.budget_ns, a.backoff_ns);
                             cwpar ^= 1u;
-                        }
-                        w = mbar_wait_sleep_bounded(&S.bar[k], (cfull >> k) & 1u, a.queue + 1, a.budget_ns) && w;
-                        cfull ^= 1u << k;
-                        if (!__all_sync(0xffffffffu, w)) {
-                            fail = true;
-                            break;
-                        }
-                        const BHdr &h = S.hdr[k];
-                        const unsigned char *st = S.stage[k];
-                        const int *rps = (const int *)(st + SG::OFF_RP + h.sh_rp);  // panel row pointers of h.r0 ..
-                        const int nr = h.r1 - h.r0;
-                        const bool h16 = MIX && h.cls == 1;
-                        const bool firstp = h.panel == 0;
-                        const VT *pwin = MIX ? (const VT *)s_win + s_pshift : (const VT *)pnew + (long long)h.panel * PW;
-                        auto psrc = [=](int c) -> VT { return pwin[c]; };
-                        const uint16_t *scol = (const uint16_t *)(st + SG::OFF_COL + h.sh_col);
-                        const unsigned char *sval = st + SG::OFF_VAL + h.sh_val;
-                        // one row per lane group; the trip count is the same
-                        // for every lane of a warp (shuffles inside)
-                        for (int qb = 0; qb < nr; qb += GPC) {
-                            const int q0 = qb + cgrp;
-                            const bool in = q0 < nr;
-                            const int ra0 = in ? rps[q0] : 0, re0 = in ? rps[q0 + 1] : 0;
-                            double y0;
-                            if (h.direct) {
-                                RowPair rr{ra0, re0, 0, 0};
-                                const uint16_t *gcol = a.col + h.ebase;
-                                double y1;
-                                if constexpr (MIX) {
-                                    if (h16)
-                                        row_dot2<L, __half, decltype(psrc), true>(rr, gcol, a.val16 + h.ebase, clane,
-                                                                                   psrc, y0, y1);
-                                    else
-                                        row_dot2<L, float, decltype(psrc), true>(rr, gcol, a.val32 + h.ebase, clane,
-                                                                                  psrc, y0, y1);
-                                } else {
-                                    row_dot2<L, double, decltype(psrc), true>(rr, gcol, a.val + h.ebase, clane, psrc,
-                                                                               y0, y1);
-                                }
-                            } else if constexpr (MIX) {
-                                if (h16)
-                                    y0 = row_dot1_cv16<L>(ra0 - h.e0, re0 - h.e0, (const uint32_t *)sval, clane, psrc);
-                                else
-                                    y0 = row_dot1_smem<L, float>(ra0 - h.e0, re0 - h.e0, scol, (const float *)sval,
-                                                                 clane, psrc);
-                            } else {
-                                y0 = row_dot1_smem<L, double>(ra0 - h.e0, re0 - h.e0, scol, (const double *)sval,
-                                                              clane, psrc);
+                            if (!__all_sync(0xffffffffu, ww)) {
+                                fail = true;
+                                break;
                             }
-                            if (clane == 0 && in) {
-                                // no global load on this path: FP16 rows take
-                                // their scale and FP32 diagonal from the stage,
-                                // the diagonal's p from the window of the panel
-                                // that holds the diagonal column
+                        }
+                        const int jfirst = MIX ? j0 + (kg - j0 % NS + NS) % NS : j0;
+                        for (int j = jfirst; j < j1; j += (MIX ? NS : 1)) {
+                            const int k = j % NS;
+                            bool w = mbar_wait_sleep_bounded(&S.bar[k], (cfull >> k) & 1u, a.queue + 1, a.budget_ns,
+                                                             a.backoff_ns);
+                            cfull ^= 1u << k;
+                            if (!__all_sync(0xffffffffu, w)) {
+                                fail = true;
+                                break;
+                            }
+                            const BHdr &h = S.hdr[k];
+                            const unsigned char *st = S.stage[k];
+                            const int *rps = (const int *)(st + SG::OFF_RP + h.sh_rp);  // panel row pointers of h.r0 ..
+                            const int nr = h.r1 - h.r0;
+                            const bool h16 = MIX && h.cls == 1;
+                            const bool firstp = h.panel == 0;
+                            const VT *pwin = MIX ? (const VT *)s_win + s_pshift : (const VT *)pnew + (long long)h.panel * PW;
+                            auto psrc = [=](int c) -> VT { return pwin[c]; };
+                            const uint16_t *scol = (const uint16_t *)(st + SG::OFF_COL + h.sh_col);
+                            const unsigned char *sval = st + SG::OFF_VAL + h.sh_val;
+                            // the row sum of row q0 of this pass goes to q (FP16
+                            // rows: scaled, plus the FP32 diagonal times the
+                            // diagonal's p from the window of the panel that
+                            // holds the diagonal column).  One panel: the row
+                            // sum is q; two panels: both partial sums are added
+                            // to q (zeroed by the p update; two additions onto
+                            // zero give the same bits in either order); more
+                            // panels: added in panel order (the mixed kernel's
+                            // window barrier orders the panels; the FP64
+                            // kernel's warps take every pass in order).
+                            auto row_out = [&](int q0, double y0) {
                                 const int i0 = h.r0 + q0;
                                 if (h16) {
                                     const float *srs = (const float *)(st + SG::OFF_RS + h.sh_rs);
                                     const float *sdg = (const float *)(st + SG::OFF_DG + h.sh_dg);
-                                    const float dt = (i0 / PW == h.panel) ? sdg[q0] * (float)pwin[i0 - h.panel * PW] : 0.f;
+                                    const float dt =
+                                        (i0 / PW == h.panel) ? sdg[q0] * (float)pwin[i0 - h.panel * PW] : 0.f;
                                     y0 = (double)fmaf(srs[q0], (float)y0, dt);
                                 }
-                                // one panel: the row sum is q; two panels: both
-                                // partial sums are added to q (zeroed by the p
-                                // update; two additions onto zero give the same
-                                // bits in either order); more panels: the same
-                                // thread handles a row in every panel and adds
-                                // in panel order
                                 VT *qi = q + i0;
                                 if (npan == 1) *qi = (VT)y0;
                                 else if (npan == 2) atomicAdd(qi, (VT)y0);
                                 else *qi = firstp ? (VT)y0 : (VT)((double)*qi + y0);
+                            };
+                            if (MIX && !h.direct && a.rowsum == 0) {
+                                // two phases over this warp's share of the
+                                // pass's rows: (1) the products of its entries,
+                                // consecutive entries to consecutive lanes,
+                                // written over the staged values in place;
+                                // (2) one lane per row adds its products in
+                                // entry order
+                                const int qa = (int)((long long)nr * gr / CWS);
+                                const int qe = (int)((long long)nr * (gr + 1) / CWS);
+                                uint32_t *pv = (uint32_t *)(st + SG::OFF_VAL + h.sh_val);
+                                if (qa < qe) {
+                                    const int ea = rps[qa] - h.e0, eb = rps[qe] - h.e0;
+                                    if (h16) {
+#pragma unroll 4
+                                        for (int e = ea + wl; e < eb; e += 32) {
+                                            const uint32_t wv = pv[e];
+                                            const float v = __half2float(__ushort_as_half((unsigned short)(wv >> 16)));
+                                            pv[e] = __float_as_uint(v * (float)pwin[wv & (uint32_t)(PW - 1)]);
+                                        }
+                                    } else {
+#pragma unroll 4
+                                        for (int e = ea + wl; e < eb; e += 32)
+                                            pv[e] = __float_as_uint(__uint_as_float(pv[e]) * (float)pwin[scol[e]]);
+                                    }
+                                    __syncwarp();
+                                    for (int q0 = qa + wl; q0 < qe; q0 += 32) {
+                                        const int s0 = rps[q0] - h.e0, s1 = rps[q0 + 1] - h.e0;
+                                        float acc = 0.f;
+                                        for (int e = s0; e < s1; e++) acc += __uint_as_float(pv[e]);
+                                        row_out(q0, (double)acc);
+                                    }
+                                }
+                                // the products written here precede the next
+                                // bulk copy into this stage
+                                fence_proxy_async_smem();
+                            } else
+                            // one row per lane group; the trip count is the same
+                            // for every lane of a warp (shuffles inside)
+                            for (int qb = 0; qb < nr; qb += GPC) {
+                                const int q0 = qb + cgrp;
+                                const bool in = q0 < nr;
+                                const int ra0 = in ? rps[q0] : 0, re0 = in ? rps[q0 + 1] : 0;
+                                double y0;
+                                if (h.direct) {
+                                    RowPair rr{ra0, re0, 0, 0};
+                                    const uint16_t *gcol = a.col + h.ebase;
+                                    double y1;
+                                    if constexpr (MIX) {
+                                        if (h16)
+                                            row_dot2<L, __half, decltype(psrc), true>(rr, gcol, a.val16 + h.ebase, clane,
+                                                                                       psrc, y0, y1);
+                                        else
+                                            row_dot2<L, float, decltype(psrc), true>(rr, gcol, a.val32 + h.ebase, clane,
+                                                                                      psrc, y0, y1);
+                                    } else {
+                                        row_dot2<L, double, decltype(psrc), true>(rr, gcol, a.val + h.ebase, clane, psrc,
+                                                                                   y0, y1);
+                                    }
+                                } else if constexpr (MIX) {
+                                    if (h16)
+                                        y0 = row_dot1_cv16<L>(ra0 - h.e0, re0 - h.e0, (const uint32_t *)sval, clane, psrc);
+                                    else
+                                        y0 = row_dot1_smem<L, float>(ra0 - h.e0, re0 - h.e0, scol, (const float *)sval,
+                                                                     clane, psrc);
+                                } else {
+                                    y0 = row_dot1_smem<L, double>(ra0 - h.e0, re0 - h.e0, scol, (const double *)sval,
+                                                                  clane, psrc);
+                                }
+                                if (clane == 0 && in) row_out(q0, y0);
                             }
+                            __syncwarp();
+                            if (wl == 0) mbar_arrive(&S.empty[k]);
                         }
-                        __syncwarp();
-                        if (wl == 0) {
-                            mbar_arrive(&S.empty[k]);
-                            if (MIX && jp == nchl - 1) mbar_arrive(&S.wempty);
+                        if (fail) break;
+                        if (MIX) {
+                            __syncwarp();
+                            if (wl == 0) mbar_arrive(&S.wempty);
                         }
                     }
                 }
@@ -1753,6 +1820,12 @@ static BatchArgs batch_args(mf_batch bt, const double *b, double *x, const mf_so
     a.tol = o.tol;
     a.delta = (o.refine_delta > 0 && o.refine_delta < 1) ? o.refine_delta : 0.1;
     a.budget_ns = (unsigned long long)(o.wait_budget_s * 1e9);
+    {
+        const char *e = getenv("MF_BATCH_BACKOFF_NS");
+        a.backoff_ns = e ? (unsigned)atoi(e) : 0u;
+        const char *rs = getenv("MF_BATCH_ROWSUM");
+        a.rowsum = (rs && !strcmp(rs, "lanes")) ? 1 : 0;
+    }
     a.policy = o.policy;
     a.mlp_w = (o.policy == MF_POLICY_LEARNED && bt->policy) ? policy_weights(bt->policy) : nullptr;
     return a;

@@ -85,14 +85,16 @@ __device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, unsigned pari
     return ok != 0;
 }
 
-// Bounded wait that sleeps between tries (mbar_try_wait_sleep); false (and
+// Bounded wait that sleeps between tries (mbar_try_wait_sleep, then
+// __nanosleep(backoff_ns) before each retry when backoff_ns > 0); false (and
 // status set) when the budget ran out.
 __device__ __forceinline__ bool mbar_wait_sleep_bounded(uint64_t *bar, unsigned parity, int *status,
-                                                        unsigned long long budget_ns)
+                                                        unsigned long long budget_ns, unsigned backoff_ns = 0)
 {
     if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
     const unsigned long long t0 = globaltimer_ns();
     for (;;) {
+        if (backoff_ns) __nanosleep(backoff_ns);
         if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
         if (globaltimer_ns() - t0 > budget_ns) {
             atomicCAS(status, DEV_OK, DEV_TIMEOUT);

@@ -393,6 +393,13 @@ __device__ void b_issue(const BatchArgs &a, BSmem<MIX> &S, const BChunk &ch, int
 #endif
 constexpr int BU = MF_BATCH_BU;
 
+// product loads in flight per lane in the two-phase row sums
+#ifndef MF_BATCH_P1U
+#define MF_BATCH_P1U 8
+#endif
+#define MF_PRAGMA(x) _Pragma(#x)
+#define MF_UNROLL(n) MF_PRAGMA(unroll n)
+
 struct RowPair {
     int a0, e0, a1, e1;
 };
@@ -973,14 +980,14 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                                 if (qa < qe) {
                                     const int ea = rps[qa] - h.e0, eb = rps[qe] - h.e0;
                                     if (h16) {
-#pragma unroll 4
+                                        MF_UNROLL(MF_BATCH_P1U)
                                         for (int e = ea + wl; e < eb; e += 32) {
                                             const uint32_t wv = pv[e];
                                             const float v = __half2float(__ushort_as_half((unsigned short)(wv >> 16)));
                                             pv[e] = __float_as_uint(v * (float)pwin[wv & (uint32_t)(PW - 1)]);
                                         }
                                     } else {
-#pragma unroll 4
+                                        MF_UNROLL(MF_BATCH_P1U)
                                         for (int e = ea + wl; e < eb; e += 32)
                                             pv[e] = __float_as_uint(__uint_as_float(pv[e]) * (float)pwin[scol[e]]);
                                     }

@@ -956,7 +956,7 @@ def main():
     ap.add_argument("--workload", default="batched",
                     choices=["batched", "poisson3d", "lap2d", "convdiff", "aniso", "multirhs", "spmv"])
     ap.add_argument("--rhs", type=int, default=16, help="multirhs workload: right-hand sides (1-16)")
-    ap.add_argument("--policy", default=None, choices=["fp64", "static", "rule", "learned"],
+    ap.add_argument("--policy", default=None, choices=["fp64", "static", "rule", "learned", "static_fp16"],
                     help="precision policy (default: learned for batched, static otherwise)")
     ap.add_argument("--policy-file", default=None,
                     help="learned policy (mf_policy_save format; batched default: "

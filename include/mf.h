@@ -107,8 +107,9 @@ mf_status mf_matrix_get_info(mf_matrix m, mf_matrix_info *info);
  * blockcsr_ptr_new (u8); Blockcsr_Val (f64); Blockcsr_Val_Low (f32);
  * nonzero_row_new, tile_rowidx, block_signal (int32); rowblkblock_rowidx
  * (u32), rowblkblock_colstart, rowblkblock_colstop (int32);
- * tile_class (u8, MF_CLASS_*); tile_f16ok (u8: 1 when every FP16 payload
- * value of the tile is finite); payload_f16 (u16 bits); payload_i8 (i8).
+ * tile_class (u8, MF_CLASS_*); tile_f16ok (u8: bit 0 every FP16 payload
+ * value of the tile is finite, bit 1 every nonzero one is also a normal
+ * binary16 number); payload_f16 (u16 bits); payload_i8 (i8).
  * `bytes` must equal the array's size; mf_matrix_array_bytes tells it.
  */
 mf_status mf_matrix_array_bytes(mf_matrix m, const char *name, size_t *bytes);
@@ -156,9 +157,14 @@ typedef enum mf_policy {
                               rule per segment (absolute thresholds on
                               |p_new - p_old|, src/main-cg-mixed.cu:415-460) */
     MF_POLICY_LEARNED = 3, /* STATIC + the learned per-tile policy */
-    MF_POLICY_RULE_SCALED = 4 /* the rule's thresholds on the change relative
+    MF_POLICY_RULE_SCALED = 4, /* the rule's thresholds on the change relative
                               to max |p| (no reference counterpart: does not
                               depend on the scale of b) */
+    MF_POLICY_STATIC_FP16 = 5 /* STATIC, plus every inexact tile whose nonzero
+                              values all lie in binary16's normal range
+                              [2^-14, 65504] runs from its FP16 payload (the
+                              rounding, <= 2^-11 relative, is corrected by the
+                              FP64 reliable updates); CG and BiCGSTAB */
 } mf_policy;
 
 typedef struct mf_solve_opts {

@@ -21,7 +21,7 @@ STATUS_NAMES = {
     5: "MF_ERR_BREAKDOWN", 6: "MF_ERR_NOT_CONVERGED", 7: "MF_ERR_IO", 8: "MF_ERR_UNSUPPORTED",
     9: "MF_ERR_NO_DEVICE",
 }
-POLICY = {"fp64": 0, "static": 1, "rule": 2, "learned": 3, "rule_scaled": 4}
+POLICY = {"fp64": 0, "static": 1, "rule": 2, "learned": 3, "rule_scaled": 4, "static_fp16": 5}
 CLASS_NAMES = {0: "fp64", 1: "bypass", 2: "int8", 3: "fp16", 4: "fp32"}
 
 

@@ -323,7 +323,7 @@ static mf_status solve_common(bool bicg, mf_matrix m, const double *b, double *x
     mf_solve_opts o;
     mf_solve_opts_default(&o);
     if (opts) o = *opts;
-    if (o.maxiter < 0 || o.wait_budget_s <= 0 || o.policy < 0 || o.policy > MF_POLICY_RULE_SCALED || o.precond < 0 ||
+    if (o.maxiter < 0 || o.wait_budget_s <= 0 || o.policy < 0 || o.policy > MF_POLICY_STATIC_FP16 || o.precond < 0 ||
         o.precond > 1) {
         set_last_error("solve: maxiter < 0, wait budget <= 0, unknown policy or unknown preconditioner");
         return MF_ERR_INVALID_ARG;
@@ -432,7 +432,7 @@ mf_status mf_cg_solve_multi(mf_matrix m, int k, const double *B, int ldb, double
     mf_solve_opts o;
     mf_solve_opts_default(&o);
     if (opts) o = *opts;
-    if (o.maxiter < 0 || o.policy < 0 || o.policy > MF_POLICY_RULE_SCALED || o.precond < 0 || o.precond > 1) {
+    if (o.maxiter < 0 || o.policy < 0 || o.policy > MF_POLICY_STATIC_FP16 || o.precond < 0 || o.precond > 1) {
         set_last_error("multi-RHS solve: maxiter < 0, unknown policy or unknown preconditioner");
         return MF_ERR_INVALID_ARG;
     }

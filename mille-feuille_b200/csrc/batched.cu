@@ -1863,7 +1863,7 @@ static mf_status batch_check_opts(mf_batch bt, const mf_solve_opts &o)
         set_last_error("batched CG needs tol > 0, maxiter > 0 and a positive wait budget");
         return MF_ERR_INVALID_ARG;
     }
-    if (o.policy < MF_POLICY_FP64 || o.policy > MF_POLICY_RULE_SCALED) {
+    if (o.policy < MF_POLICY_FP64 || o.policy > MF_POLICY_STATIC_FP16) {
         set_last_error("batched CG: unknown policy %d", o.policy);
         return MF_ERR_INVALID_ARG;
     }
@@ -1871,8 +1871,9 @@ static mf_status batch_check_opts(mf_batch bt, const mf_solve_opts &o)
         set_last_error("batched CG: no preconditioner");
         return MF_ERR_UNSUPPORTED;
     }
-    if (o.policy == MF_POLICY_RULE_SCALED) {
-        set_last_error("batched CG: the scaled rule is not available (RULE, LEARNED, STATIC, FP64 are)");
+    if (o.policy == MF_POLICY_RULE_SCALED || o.policy == MF_POLICY_STATIC_FP16) {
+        set_last_error("batched CG: the scaled rule and STATIC_FP16 are not available (RULE, LEARNED, STATIC, FP64 are;"
+                       " its FP16 chunks are row-scaled)");
         return MF_ERR_UNSUPPORTED;
     }
     if (o.policy == MF_POLICY_LEARNED && !bt->policy) {

@@ -53,12 +53,17 @@ __global__ void k_pack_fill(int T, const int *__restrict__ tile_nnz, const unsig
 }
 
 // Static policy: the stored (value-range) class; tiles that need FP64 run
-// their inner products from the FP32 payload.
-__global__ void k_static_classes(int T, const unsigned char *__restrict__ cls, unsigned char *__restrict__ w)
+// their inner products from the FP32 payload.  range16 (MF_POLICY_STATIC_FP16):
+// an inexact tile whose nonzero values are all normal binary16 numbers
+// (f16ok bit 1) runs from its FP16 payload instead.
+__global__ void k_static_classes(int T, const unsigned char *__restrict__ cls, const unsigned char *__restrict__ ok16,
+                                 int range16, unsigned char *__restrict__ w)
 {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
         const int c = cls[t];
-        w[t] = (c == MF_CLASS_FP64) ? MF_CLASS_FP32 : c;
+        int v = (c == MF_CLASS_FP64) ? MF_CLASS_FP32 : c;
+        if (range16 && v == MF_CLASS_FP32 && (ok16[t] & 2)) v = MF_CLASS_FP16;
+        w[t] = (unsigned char)v;
     }
 }
 
@@ -72,11 +77,11 @@ int grid_for(long long work, int nt)
 
 }  // namespace
 
-mf_status static_working_classes(mf_matrix m, unsigned char *d_wcls, cudaStream_t s)
+mf_status static_working_classes(mf_matrix m, unsigned char *d_wcls, cudaStream_t s, bool range16)
 {
     const int T = m->v.tilenum;
     if (T == 0) return MF_OK;
-    k_static_classes<<<grid_for(T, 256), 256, 0, s>>>(T, m->d_class, d_wcls);
+    k_static_classes<<<grid_for(T, 256), 256, 0, s>>>(T, m->d_class, m->d_f16ok, range16 ? 1 : 0, d_wcls);
     note_launch();
     MF_CUDA(cudaGetLastError());
     return MF_OK;
@@ -209,7 +214,7 @@ __global__ void k_rule_tiles(int T, const int *__restrict__ tile_col, const unsi
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
         const int d = seg_cls[tile_col[t]];
         if (decision) decision[t] = (unsigned char)d;
-        if (w) w[t] = (unsigned char)exec_class(d, cls[t], false, ok16[t] != 0);
+        if (w) w[t] = (unsigned char)exec_class(d, cls[t], false, (ok16[t] & 1) != 0);
     }
 }
 
@@ -231,7 +236,7 @@ __global__ void k_rule_scaled_classes(int T, const int *__restrict__ tile_col, c
         else if (v > 1e-8f) d = MF_CLASS_INT8;
         else d = MF_CLASS_BYPASS;
         if (decision) decision[t] = (unsigned char)d;
-        if (w) w[t] = (unsigned char)exec_class(d, cls[t], true, ok16[t] != 0);
+        if (w) w[t] = (unsigned char)exec_class(d, cls[t], true, (ok16[t] & 1) != 0);
     }
 }
 

@@ -80,11 +80,14 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
         }
         return MF_OK;
     };
+    // the classes a solve starts from: STATIC_FP16's, or STATIC's for every
+    // other mixed policy
+    const int base_policy = o.policy == MF_POLICY_STATIC_FP16 ? MF_POLICY_STATIC_FP16 : MF_POLICY_STATIC;
     if (mixed) {
         if (!m->d_wcls) MF_CUDA(cudaMalloc(&m->d_wcls, (size_t)T + 16));
-        if ((slots ? m->slot_policy : m->packed_policy) != MF_POLICY_STATIC) {
-            MF_TRY(static_working_classes(m, m->d_wcls, s));
-            MF_TRY(repack(MF_POLICY_STATIC));
+        if ((slots ? m->slot_policy : m->packed_policy) != base_policy) {
+            MF_TRY(static_working_classes(m, m->d_wcls, s, base_policy == MF_POLICY_STATIC_FP16));
+            MF_TRY(repack(base_policy));
         }
     }
     if (o.policy == MF_POLICY_LEARNED) m->pol_have_prev = 0;  // no history from an earlier solve
@@ -136,7 +139,7 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
     a.fixed = o.tol < 0 ? 1 : 0;
     a.delta = o.refine_delta > 0 && o.refine_delta < 1 ? o.refine_delta : 0.1;
     // checkpoints (policy updates between launches) for CG's dynamic policies
-    a.exit_on_refine = (!bicg && mixed && o.policy != MF_POLICY_STATIC) ? 1 : 0;
+    a.exit_on_refine = (!bicg && mixed && o.policy != MF_POLICY_STATIC && o.policy != MF_POLICY_STATIC_FP16) ? 1 : 0;
     a.checkpoint_every = (hook && !bicg) ? hook->every : 0;
     a.one_reduction = (one_reduction && a.checkpoint_every == 0) ? 1 : 0;
     if (!bicg && o.precond == 1) {
@@ -176,7 +179,8 @@ static mf_status persistent_solve(bool bicg, mf_matrix m, const double *b, doubl
         const void *pnew = (it & 1) ? w.p1 : w.p0;  // written by the last iteration
         const void *pold = (it & 1) ? w.p0 : w.p1;
         if (hook) MF_TRY(hook->fn(hook->ctx, m, w, pnew, pold, it, st[S_RELRES], s));
-        if (o.policy == MF_POLICY_FP64 || o.policy == MF_POLICY_STATIC || rep.fallback_iteration > 0) {
+        if (o.policy == MF_POLICY_FP64 || o.policy == MF_POLICY_STATIC || o.policy == MF_POLICY_STATIC_FP16 ||
+            rep.fallback_iteration > 0) {
             a.start = 0;
             continue;
         }

@@ -155,7 +155,8 @@ mf_status true_residual(mf_matrix m, const double *b, const double *x, SolverWor
 mf_status jacobi_dinv(mf_matrix m, double *dinv, cudaStream_t s);
 // payload.cu
 mf_status pack_payload(mf_matrix m, const unsigned char *d_wcls, cudaStream_t s);
-mf_status static_working_classes(mf_matrix m, unsigned char *d_wcls, cudaStream_t s);
+// STATIC classes; range16: MF_POLICY_STATIC_FP16's FP16 class for inexact tiles in binary16's normal range
+mf_status static_working_classes(mf_matrix m, unsigned char *d_wcls, cudaStream_t s, bool range16 = false);
 mf_status learned_working_classes(mf_matrix m, SolverWork &w, const void *p_new, const void *p_old,
                                   unsigned char *d_wcls, cudaStream_t s);
 // RULE / RULE_SCALED classes for the FP32 directions p_new / p_old: the

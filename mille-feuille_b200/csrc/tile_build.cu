@@ -305,8 +305,9 @@ __global__ void k_rbb_fill(int tilem, const int *__restrict__ tile_ptr, const in
 //   fp64 : otherwise
 // Payloads: fp16 = (half)(float)v, int8 = (int8_t)v (low byte of the
 // truncated 32-bit integer), as src/main-cg-mixed.cu:2333-2336 builds them.
-// f16ok: every FP16 payload value of the tile is finite (|v| within
-// binary16's range), the condition for running an inexact tile in FP16.
+// f16ok: bit 0 every FP16 payload value of the tile is finite (|v| within
+// binary16's range), the condition for running an inexact tile in FP16;
+// bit 1 every nonzero one is also normal (|v| >= 2^-14: no subnormal loss).
 __global__ void k_payloads(int T, const int *__restrict__ tile_nnz, const double *__restrict__ val,
                            const float *__restrict__ low, uint16_t *__restrict__ f16, int8_t *__restrict__ i8,
                            unsigned char *__restrict__ cls, unsigned char *__restrict__ f16ok,
@@ -314,7 +315,7 @@ __global__ void k_payloads(int T, const int *__restrict__ tile_nnz, const double
 {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
         const int a = tile_nnz[t], b = tile_nnz[t + 1];
-        bool is_int8 = true, in16 = true, in32 = true, fin16 = true;
+        bool is_int8 = true, in16 = true, in32 = true, fin16 = true, norm16 = true;
         for (int k = a; k < b; k++) {
             const double v = val[k];
             const double av = fabs(v);
@@ -327,8 +328,10 @@ __global__ void k_payloads(int T, const int *__restrict__ tile_nnz, const double
             if ((double)vf != v) in32 = false;
             if ((double)__half2float(h) != v) in16 = false;
             if (__hisinf(h) || __hisnan(h)) fin16 = false;
+            const unsigned short hb = __half_as_ushort(h);
+            if (v != 0.0 && (hb & 0x7C00u) == 0) norm16 = false;  // zero or subnormal from a nonzero value
         }
-        f16ok[t] = fin16 ? 1 : 0;
+        f16ok[t] = (unsigned char)((fin16 ? 1 : 0) | (fin16 && norm16 ? 2 : 0));
         unsigned char c = is_int8 ? MF_CLASS_INT8 : in16 ? MF_CLASS_FP16 : in32 ? MF_CLASS_FP32 : MF_CLASS_FP64;
         cls[t] = c;
         atomicAdd(&class_count[c], 1);

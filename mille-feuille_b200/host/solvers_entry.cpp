@@ -77,6 +77,7 @@ void configure(mf_solve_opts &o, int fixed_iters, bool bicg)
         if (p && !strcmp(p, "static")) o.policy = MF_POLICY_STATIC;
         if (p && !strcmp(p, "rule")) o.policy = MF_POLICY_RULE;
         if (p && !strcmp(p, "rule_scaled")) o.policy = MF_POLICY_RULE_SCALED;
+        if (p && !strcmp(p, "static_fp16")) o.policy = MF_POLICY_STATIC_FP16;
         if (p && !strcmp(p, "learned")) o.policy = MF_POLICY_LEARNED;
     }
 }

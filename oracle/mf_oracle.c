@@ -429,7 +429,7 @@ int orc_rule_class(double v)
  * tiles (static class INT8) and FP16 otherwise, BYPASS to BYPASS under the
  * scaled rule and like INT8 under the absolute one, and keeps a narrower
  * exact static class (INT8, FP16); an inexact tile whose FP16 payload is not
- * finite (f16ok[t] = 0; NULL: all finite) runs FP16 in FP32. */
+ * finite (bit 0 of f16ok[t] clear; NULL: all finite) runs FP16 in FP32. */
 void orc_rule_tiles(int n, int tilen, int T, const int *tile_col, const unsigned char *static_cls,
                     const unsigned char *f16ok, const float *pn, const float *po, int scaled, unsigned char *decision,
                     unsigned char *working)
@@ -466,7 +466,7 @@ void orc_rule_tiles(int n, int tilen, int T, const int *tile_col, const unsigned
         else w = 1;
         if (w == 4 && (c == 3 || c == 2)) w = c;
         if (w == 3 && c == 2) w = c;
-        if (w == 3 && c != 3 && f16ok && !f16ok[t]) w = 4;
+        if (w == 3 && c != 3 && f16ok && !(f16ok[t] & 1)) w = 4;
         decision[t] = (unsigned char)d;
         working[t] = (unsigned char)w;
     }

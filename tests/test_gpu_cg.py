@@ -91,7 +91,7 @@ def test_cg_zero_rhs(mf):
     M.close()
 
 
-@pytest.mark.parametrize("policy", ["static", "rule"])
+@pytest.mark.parametrize("policy", ["static", "rule", "static_fp16"])
 @pytest.mark.parametrize("name,make,seed", [
     ("laplace2d_128", lambda mf: mf.synth_laplace2d(128, 128), 0),
     ("poisson3d_32", lambda mf: mf.synth_poisson3d_scaled(32, 1), 1),

@@ -55,12 +55,17 @@ def _run(mf, A, policy, seed):
     tile_col = M.export("tile_columnidx")
     static_cls = M.export("tile_class")
     f16ok = M.export("tile_f16ok")
-    # f16ok against the FP16 payload itself: 0 exactly where a value is inf
+    # f16ok against the FP16 payload itself: bit 0 clear exactly where a
+    # value is inf, bit 1 set where also no nonzero value became zero or
+    # subnormal
     tnz = M.export("tile_nnz")
     f16 = M.export("payload_f16")
-    inf = np.concatenate([[0], np.cumsum((f16 & 0x7C00) == 0x7C00)])
-    per_tile = inf[tnz[1:]] - inf[tnz[:-1]]
-    assert np.array_equal(f16ok, (per_tile == 0).astype(np.uint8))
+    val = M.export("Blockcsr_Val")
+    per_tile = lambda bad: np.diff(np.concatenate([[0], np.cumsum(bad)])[tnz])
+    n_inf = per_tile((f16 & 0x7C00) == 0x7C00)
+    n_sub = per_tile(((f16 & 0x7C00) == 0) & (val != 0))
+    want_ok = (n_inf == 0).astype(np.uint8) | (((n_inf == 0) & (n_sub == 0)).astype(np.uint8) << 1)
+    assert np.array_equal(f16ok, want_ok)
     want_dec, want_wrk = ol.oracle_rule_tiles(A.n_cols, info.tilen, tile_col, static_cls, pn, po,
                                               scaled=(policy == "rule_scaled"), f16ok=f16ok)
     got_dec, got_wrk = dec.cpu().numpy(), wrk.cpu().numpy()

@@ -349,11 +349,12 @@ typedef struct mf_batch_report {
 } mf_batch_report;
 
 /* count systems; system s has n[s] rows, CSR rowptr[s] (rowptr[s][0] = 0),
- * colidx[s] in [0, n[s]), val[s] (host pointers).  Storage: column indices
- * as 16-bit words when every system has at most 65,536 rows (32-bit
- * otherwise); values in FP64, FP32 and FP16 scaled per row by a power of two
- * (diagonal kept apart in FP32); rows cut into chunks of at most 256 rows
- * and 2048 entries, each with a precision class. */
+ * colidx[s] in [0, n[s]), val[s] (host pointers).  Storage: each system in
+ * column panels of 32,768 columns (a 16-bit column offset within the panel
+ * per entry, the panel's rows in CSR); values in FP64, FP32 and FP16 scaled
+ * per row by a power of two (diagonal kept apart in FP32; the FP16 value and
+ * its column packed in one 32-bit word); rows cut into chunks of at most 256
+ * rows and 4,096 entries in every panel, each with a precision class. */
 mf_status mf_batch_create(int count, const int *n, const int *const *rowptr, const int *const *colidx,
                           const double *const *val, mf_batch *out);
 mf_status mf_batch_destroy(mf_batch bt);
@@ -387,8 +388,8 @@ mf_status mf_batch_chunk_count(mf_batch bt, int *chunks, int *static_fp16, int *
  * (6 floats per chunk: features 0-4 and the chunk's max |a|), chunk_start
  * (int32, count+1: first chunk of each system), chunk_rows (int32: per
  * system its chunks' first rows and the row count), chunk_ends (int32: the
- * same chunks' first entries and the entry count), val16 (FP16 bits), val32, row_scale, diag32 (float), col (u16 or
- * int32 as stored).  `bytes` must equal the array's size. */
+ * same chunks' first entries and the entry count), val16 (FP16 bits), val32, row_scale, diag32 (float), col (u16:
+ * the column offset within its panel).  `bytes` must equal the array's size. */
 mf_status mf_batch_export(mf_batch bt, const char *name, void *host_dst, size_t bytes);
 /* MF_POLICY_LEARNED batched solves use p (NULL detaches). */
 mf_status mf_batch_attach_policy(mf_batch bt, mf_learned p);

@@ -19,6 +19,8 @@
  *                           mixed persistent CG      src/main-cg-mixed.cu:99,998
  *   mf_read_matrix_market   read_Dmatrix_32 (.mtx)   src/biio2.0/src/biio.h:153
  *   mf_read_matrix          read_Dmatrix_32          src/biio2.0/src/biio.h:153
+ *   mf_matrix_create_mtx    read_Dmatrix_32 +        src/biio2.0/src/biio.h:153,
+ *                           Tile_create              src/csr2block.h:267
  *   mf_read_cbd / _write_cbd binary_read_csr /       src/biio2.0/src/biio.h:22, 72
  *                           binary_write_csr
  * The reference's own solve entry points (cg_solve_*, bicgstab*) keep their
@@ -439,6 +441,15 @@ mf_status mf_selftest_bounded_waits(double budget_s, int *results);
  * file placed right after its original (mmio_highlevel.h:151-321). */
 mf_status mf_read_matrix_market(const char *path, int *m, int *n, int *nnz, int **rowptr,
                                 int **colidx, double **val, int *is_symmetric);
+
+/* A Matrix Market file straight to a device-resident matrix: the entries
+ * are parsed on the host threads as mf_read_matrix_market parses them, the
+ * CSR (the same arrays, bit for bit) is built on the GPU -- the symmetric
+ * mirrors expanded in place, a stable radix sort by row -- and handed to
+ * the tile build without a host round trip (read_Dmatrix_32 + Tile_create,
+ * src/biio2.0/src/biio.h:153, src/csr2block.h:267).  Stream-ordered on
+ * `stream`; returns after the matrix is built. */
+mf_status mf_matrix_create_mtx(const char *path, void *stream, mf_matrix *out, int *is_symmetric);
 
 /* Binary CSR files (".cbd"), the reference's cache of a parsed matrix
  * (binary_read_csr / binary_write_csr, src/biio2.0/src/biio.h:22-94):

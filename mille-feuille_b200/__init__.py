@@ -110,6 +110,7 @@ def lib() -> C.CDLL:
                                         C.POINTER(SolveReport), vp]
         L.mf_cg_solve_multi_host.argtypes = [vp, C.c_int, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]
         L.mf_read_matrix_market.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
+        L.mf_matrix_create_mtx.argtypes = [C.c_char_p, vp, C.POINTER(vp), ip]
         L.mf_read_matrix.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
         L.mf_read_cbd.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp)]
         L.mf_write_cbd.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, vp]
@@ -240,6 +241,15 @@ def read_matrix_market(path):
     return _take_csr(m.value, nnz.value, rp, ci, v, n_cols=n.value)
 
 
+def matrix_from_mtx(path, stream=None):
+    """A Matrix from a Matrix Market file, the CSR built on the GPU
+    (mf_matrix_create_mtx); returns (Matrix, is_symmetric)."""
+    h = C.c_void_p()
+    sym = C.c_int()
+    check(lib().mf_matrix_create_mtx(str(path).encode(), stream, C.byref(h), C.byref(sym)))
+    return Matrix(None, _handle=h), sym.value
+
+
 def read_matrix(path):
     """.mtx or .cbd by extension (mf_read_matrix); returns (HostCsr, is_symmetric)."""
     L = lib()
@@ -281,7 +291,11 @@ def solve_opts(**kw):
 class Matrix:
     """A device-resident tiled matrix (mf_matrix handle)."""
 
-    def __init__(self, csr: HostCsr, rows=None, cols=None, val_low=None):
+    def __init__(self, csr: HostCsr, rows=None, cols=None, val_low=None, _handle=None):
+        if _handle is not None:  # a handle made by another entry point (matrix_from_mtx)
+            self._keep = None
+            self.h = _handle
+            return
         L = lib()
         rows = csr.n_rows if rows is None else rows
         cols = csr.n_cols if cols is None else cols

@@ -199,10 +199,16 @@ bool parse_entries_parallel(const char *p, const char *e, long long NZ, long lon
 
 }  // namespace
 
-extern "C" mf_status mf_read_matrix_market(const char *path, int *m_out, int *n_out, int *nnz_out, int **rowptr,
-                                           int **colidx, double **val, int *is_symmetric)
+namespace mf {
+
+// The entries of a Matrix Market coordinate file in file order (0-based
+// row, column, value), its sizes and whether it is symmetric (or
+// hermitian); a symmetric file's off-diagonal entries are checked to mirror
+// inside the rows.  The CSR is built from these by mf_read_matrix_market
+// (host) or mf_matrix_create_mtx (device).
+mf_status mtx_read_coo(const char *path, long long &M, long long &N, long long &NZ, bool &sym, std::vector<int> &ri,
+                       std::vector<int> &ci, std::vector<double> &vv)
 {
-    if (!path || !m_out || !n_out || !nnz_out || !rowptr || !colidx || !val) return MF_ERR_INVALID_ARG;
     FILE *f = fopen(path, "rb");
     if (!f) {
         mf::set_last_error("cannot open %s: %s", path, strerror(errno));
@@ -228,7 +234,7 @@ extern "C" mf_status mf_read_matrix_market(const char *path, int *m_out, int *n_
     const bool pattern = bl.find("pattern") != std::string::npos;
     const bool complex_ = bl.find("complex") != std::string::npos;
     const bool integer = bl.find("integer") != std::string::npos;
-    const bool sym = bl.find("symmetric") != std::string::npos || bl.find("hermitian") != std::string::npos;
+    sym = bl.find("symmetric") != std::string::npos || bl.find("hermitian") != std::string::npos;
     p = nl ? nl + 1 : e;
     // skip comments / blank lines
     while (p < e) {
@@ -242,14 +248,14 @@ extern "C" mf_status mf_read_matrix_market(const char *path, int *m_out, int *n_
         break;
     }
     Reader rd{p, e};
-    long long M, N, NZ;
     if (!rd.next_long(M) || !rd.next_long(N) || !rd.next_long(NZ) || M < 0 || N < 0 || NZ < 0 || M > 0x7fffffff ||
         N > 0x7fffffff) {
         mf::set_last_error("%s: bad size line", path);
         return MF_ERR_IO;
     }
-    std::vector<int> ri((size_t)NZ), ci((size_t)NZ);
-    std::vector<double> vv((size_t)NZ);
+    ri.assign((size_t)NZ, 0);
+    ci.assign((size_t)NZ, 0);
+    vv.assign((size_t)NZ, 0.0);
     // entries in parallel on files of 200,000 entries or more, serially
     // otherwise or when the file is not one entry per line;
     // MF_MTX_THREADS=<t> sets the threads for every file (1: serial)
@@ -290,16 +296,33 @@ extern "C" mf_status mf_read_matrix_market(const char *path, int *m_out, int *n_
         ci[k] = (int)(j - 1);
         vv[k] = v;
     }
-    std::vector<long long> cnt((size_t)M + 1, 0);
-    for (long long k = 0; k < NZ; k++) {
-        cnt[ri[k]]++;
-        if (sym && ri[k] != ci[k]) {
-            if (ci[k] >= M) {
+    if (sym)
+        for (long long k = 0; k < NZ; k++)
+            if (ri[k] != ci[k] && ci[k] >= M) {
                 mf::set_last_error("%s: symmetric entry mirrors outside the rows", path);
                 return MF_ERR_IO;
             }
-            cnt[ci[k]]++;
-        }
+    return MF_OK;
+}
+
+}  // namespace mf
+
+extern "C" mf_status mf_read_matrix_market(const char *path, int *m_out, int *n_out, int *nnz_out, int **rowptr,
+                                           int **colidx, double **val, int *is_symmetric)
+{
+    if (!path || !m_out || !n_out || !nnz_out || !rowptr || !colidx || !val) return MF_ERR_INVALID_ARG;
+    long long M, N, NZ;
+    bool sym = false;
+    std::vector<int> ri, ci;
+    std::vector<double> vv;
+    const mf_status st = mf::mtx_read_coo(path, M, N, NZ, sym, ri, ci, vv);
+    if (st != MF_OK) return st;
+    // CSR: a row's entries in file order, a symmetric entry's mirror placed
+    // when the entry is read
+    std::vector<long long> cnt((size_t)M + 1, 0);
+    for (long long k = 0; k < NZ; k++) {
+        cnt[ri[k]]++;
+        if (sym && ri[k] != ci[k]) cnt[ci[k]]++;
     }
     // exclusive scan
     long long run = 0;

@@ -78,6 +78,20 @@ def test_noalloc_residual_argument_checks_without_device(mf):
     assert list(buf) == [0.0, 0.0, 0.0]
 
 
+def test_device_mtx_reader_rejects_before_device(mf, tmp_path):
+    """mf_matrix_create_mtx: a null path or handle pointer, a missing file
+    and a malformed one are reported before any device work."""
+    L = mf.lib()
+    h = ctypes.c_void_p()
+    assert L.mf_matrix_create_mtx(None, None, ctypes.byref(h), None) == 1
+    assert L.mf_matrix_create_mtx(b"x.mtx", None, None, None) == 1
+    assert L.mf_matrix_create_mtx(str(tmp_path / "missing.mtx").encode(), None, ctypes.byref(h), None) == 7
+    bad = tmp_path / "bad.mtx"
+    bad.write_text("%%MatrixMarket matrix coordinate real general\n3 3 2\n1 1 1.0\n")  # truncated
+    assert L.mf_matrix_create_mtx(str(bad).encode(), None, ctypes.byref(h), None) == 7
+    assert h.value is None
+
+
 @pytest.mark.parametrize("libname", ["libmf_solvers.so", "libmf_solvers_mixed.so"])
 def test_solver_entry_libraries_export_reference_names(mf, libname):
     """cg_solve_inc/sync/reduce and bicgstab/_sync/_inc, as declared in

@@ -17,20 +17,25 @@
 // panel in CSR), and the mixed-precision kernel copies the panel's slice of p
 // (FP32, 128 KB) into shared memory before it streams the panel's chunks:
 // the gathers hit shared memory (about 8 lanes per cycle for random
-// addresses) and the kernel is bound by the bytes it streams.  A chunk is a
-// range of rows with at most BCE entries in every panel; for each (chunk,
-// panel) pair its row pointers, columns and values arrive by bulk copies in
-// one of four shared-memory stages, and the row sums of the panels are added
-// in panel order (partial sums kept in q).  The FP64 kernel (the FP64
-// policy and trace collection) gathers p from global memory.
+// addresses).  A chunk is a range of rows with at most BCE entries in every
+// panel; for each (chunk, panel) pair its row pointers, columns and values
+// arrive by bulk copies in one of NS = 3 shared-memory stages, produced by
+// warp 0 and consumed, in the mixed kernel, by a group of five warps per
+// stage (the FP64 kernel's fifteen consumer warps all take every pass).  A
+// mixed pass sums its rows in two phases: the products of consecutive
+// entries on consecutive lanes, written over the staged values, then one
+// lane per row adding its products in entry order.  The row sums of the
+// panels are added in panel order (partial sums kept in q).  The FP64 kernel
+// (the FP64 policy and trace collection) gathers p from global memory.
 //
 // Values are held three times: FP64 (reliable updates, FP64 policy), FP32,
 // and FP16 scaled per row by a power of two (the row's largest
 // off-diagonal magnitude maps into [2^14, 2^15)) with the diagonal taken out
 // and kept in FP32 beside the row scale.  A mixed-precision solve reads each
-// chunk in its working class -- FP32 (4 + 2 bytes per entry) or FP16
-// (2 + 2) -- and accumulates in FP32; FP64 dot products, FP64 reliable
-// updates r = b - A x from the FP64 values, convergence judged on that FP64
+// chunk in its working class -- FP32 (4 + 2 bytes per entry) or FP16 (one
+// 4-byte word per entry: the value bits and the column offset) -- and
+// accumulates in FP32; FP64 dot products, FP64 reliable updates
+// r = b - A x from the FP64 values, convergence judged on that FP64
 // residual.
 //
 // Classes per chunk, decided inside the persistent kernel by the CTA that

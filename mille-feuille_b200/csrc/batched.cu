@@ -80,8 +80,14 @@ namespace cg = cooperative_groups;
 namespace mf {
 namespace {
 constexpr int PW = 32768;   // columns per storage panel (16-bit offsets)
-constexpr int BCE = 4096;   // entries of a (chunk, panel) stage
-constexpr int BCR = 256;    // rows of a chunk
+#ifndef MF_BATCH_BCE
+#define MF_BATCH_BCE 4096
+#endif
+#ifndef MF_BATCH_BCR
+#define MF_BATCH_BCR 256
+#endif
+constexpr int BCE = MF_BATCH_BCE;   // entries of a (chunk, panel) stage
+constexpr int BCR = MF_BATCH_BCR;   // rows of a chunk
 }  // namespace
 }  // namespace mf
 
@@ -258,9 +264,13 @@ struct BHdr {
 };
 
 // Stages in flight per CTA.  The mixed kernels stage at most 4 + 2 bytes
-// per entry (FP32 values, 16-bit columns).
+// per entry (FP32 values, 16-bit columns); their consumer warps form
+// MF_BATCH_GROUPS groups, group g consuming the stages k with k % groups = g.
 #ifndef MF_BATCH_STAGES_MIX
 #define MF_BATCH_STAGES_MIX 3
+#endif
+#ifndef MF_BATCH_GROUPS
+#define MF_BATCH_GROUPS 3
 #endif
 #ifndef MF_BATCH_STAGES_FP64
 #define MF_BATCH_STAGES_FP64 3
@@ -273,7 +283,7 @@ struct Stage {
     static constexpr int NS = MIX ? MF_BATCH_STAGES_MIX : MF_BATCH_STAGES_FP64;
     static constexpr int VB = MIX ? 4 : 8;  // widest stored value
     static constexpr int OFF_RP = 0;
-    static constexpr int OFF_COL = 1072;
+    static constexpr int OFF_COL = ((BCR + 1) * 4 + 32 + 15) & ~15;
     static constexpr int OFF_VAL = OFF_COL + ((BCE * 2 + 32 + 15) & ~15);
     static constexpr int OFF_RS = OFF_VAL + ((BCE * VB + 32 + 15) & ~15);  // FP16 passes: row scales
     static constexpr int OFF_DG = OFF_RS + ((BCR * 4 + 32 + 15) & ~15);    // FP16 passes: FP32 diagonals
@@ -715,7 +725,7 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
     if (threadIdx.x == 0) {
         for (int k = 0; k < NS; k++) {
             mbar_init(&S.bar[k], 1);
-            mbar_init(&S.empty[k], MIX ? (BNW - 1) / NS : BNW - 1);  // the stage's consumer warps
+            mbar_init(&S.empty[k], MIX ? (BNW - 1) / MF_BATCH_GROUPS : BNW - 1);  // the stage's consumer warps
         }
         mbar_init(&S.pbar, 1);
         mbar_init(&S.wempty, BNW - 1);
@@ -899,19 +909,20 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                         }
                     }
                 } else {
-                    // consumer warps in NS groups: group g consumes stage g,
-                    // i.e. passes j with j % NS == g, its CWS warps splitting
-                    // each pass's rows; every consumer warp waits for each
-                    // panel's window and releases it after its own passes
-                    // of that panel
+                    // consumer warps in NGRP groups: group g consumes the
+                    // passes j with j % NGRP == g (stages j % NS, two per
+                    // group), its CWS warps splitting each pass's rows;
+                    // every consumer warp waits for each panel's window and
+                    // releases it after its own passes of that panel
                     // (mixed kernel; the FP64 kernel's consumer warps all
                     // take every pass, so that a row's panels are added in
                     // panel order without a window to order them)
                     constexpr int NCW = BNW - 1;
-                    constexpr int CWS = MIX ? NCW / NS : NCW;   // consumer warps per stage
-                    static_assert(NCW % NS == 0, "consumer warps split evenly over the stages");
+                    constexpr int NGRP = MIX ? MF_BATCH_GROUPS : 1;
+                    constexpr int CWS = NCW / NGRP;             // consumer warps per group
+                    static_assert(NCW % NGRP == 0 && NS % NGRP == 0, "groups split the warps and stages evenly");
                     const int cw = wid - 1;
-                    const int kg = MIX ? cw / CWS : 0;          // this warp's stage (mixed kernel)
+                    const int kg = cw / CWS;                    // this warp's group
                     const int gr = cw % CWS;                    // warp within the stage's group
                     const int ct = gr * 32 + wl;                // thread within the stage's group
                     const int clane = ct % L, cgrp = ct / L;
@@ -928,8 +939,8 @@ __global__ void __launch_bounds__(BNT, MF_BATCH_MINB) k_batched_cg(BatchArgs a)
                                 break;
                             }
                         }
-                        const int jfirst = MIX ? j0 + (kg - j0 % NS + NS) % NS : j0;
-                        for (int j = jfirst; j < j1; j += (MIX ? NS : 1)) {
+                        const int jfirst = j0 + (kg - j0 % NGRP + NGRP) % NGRP;
+                        for (int j = jfirst; j < j1; j += NGRP) {
                             const int k = j % NS;
                             bool w = mbar_wait_sleep_bounded(&S.bar[k], (cfull >> k) & 1u, a.queue + 1, a.budget_ns,
                                                              a.backoff_ns);

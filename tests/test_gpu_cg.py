@@ -116,8 +116,13 @@ def test_mixed_precision_reaches_fp64_accuracy(mf, policy, name, make, seed):
     # bounded by the error the oracle itself has against x*
     err_o = np.max(np.abs(x_o - xs))
     assert np.max(np.abs(x - x_o)) <= 10 * err_o + 1e-12
-    # the iteration count stays near the FP64 one
-    assert rep.iterations <= 2 * it_o + 50, (rep.iterations, it_o)
+    # the iteration count stays near the FP64 one: FP32 payloads and inner
+    # sums within 10 %; FP16 payloads of inexact values (STATIC_FP16) cost
+    # more on ill-conditioned systems
+    if policy == "static_fp16":
+        assert rep.iterations <= 2 * it_o + 50, (rep.iterations, it_o)
+    else:
+        assert rep.iterations <= int(1.1 * it_o) + 10, (rep.iterations, it_o)
     M.close()
 
 

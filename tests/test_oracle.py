@@ -262,3 +262,36 @@ def test_pn_forward_restatement():
     h2 = np.maximum(W2 @ h1 + b2, 0)
     o = W3 @ h2 + b3
     assert np.allclose(out, o, rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.skipif(ol.reference() is None, reason="reference code not compiled")
+@pytest.mark.parametrize("name,make,seed", [
+    ("laplace2d_48", lambda mf: mf.synth_laplace2d(48, 48), 0),
+    ("poisson3d_12", lambda mf: mf.synth_poisson3d_scaled(12, 1), 1),
+])
+def test_oracle_cg_iterates_match_reference_spmv_cg(mf, name, make, seed):
+    """Fixed-count CG iterates of the oracle (CSR SpMV, sequential sums)
+    against a CG around the reference's own blockspmv_cpu (one thread,
+    sequential dot products): the same method; only each row's summation
+    order differs (tile order against CSR order), so after 1, 5 and 20
+    iterations the iterates agree to 1e-12 relative."""
+    import ctypes as C
+
+    A = make(mf)
+    b = A.matvec(mf.synth_xstar(seed, A.n_rows))
+    csr = ol.Csr(A.n_rows, A.n_cols, A.rowptr, A.colidx, A.val)
+    ref = ol.reference()
+    ref.ref_cg_iterations.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    ref.ref_cg_iterations.restype = C.c_double
+    sizes, _ = ol.reference_tiles(csr)
+    ref.ref_encode_last()
+    nx = sizes["tilen"] * 16
+    for k in (1, 5, 20):
+        x, r, p, q, bb = (np.zeros(nx) for _ in range(5))
+        bb[: A.n_rows] = b
+        rho = C.c_double(0.0)
+        ref.ref_cg_iterations(A.n_rows, A.n_cols, A.nnz, bb.ctypes.data, x.ctypes.data, r.ctypes.data,
+                              p.ctypes.data, q.ctypes.data, k, 1, 1, C.byref(rho))
+        _, x_o, _ = ol.oracle_cg(csr, b, k, -1.0)
+        assert np.max(np.abs(x[: A.n_rows] - x_o)) <= 1e-12 * np.max(np.abs(x_o)), (name, k)

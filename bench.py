@@ -617,6 +617,92 @@ def workload_spmv(args, mf, world, local):
     return result, info
 
 
+def workload_spmm_f16(args, mf, world, local):
+    """mf_spmm_f16 (16 right-hand sides, the dense 16x16 tiles on the tensor
+    cores) on a block-structured matrix of 32,768 block rows (a dense
+    diagonal block and 3 random dense blocks per block row, 2 random sparse
+    entries per row); value = SpMMs per second, the FP64 mf_spmm of the same
+    product beside it.  Algorithmic bytes per launch: 512 per dense tile
+    (FP16) + 5 per sparse entry (FP32 value, in-tile column) + 24 per tile +
+    X read (FP64, 128 B per row) and packed (FP16, 32 B per row written and
+    read) + Y written (FP64, 128 B per row)."""
+    import torch
+
+    L = mf.lib()
+    H = mf.synth_block_dense(32768, 3, 2, 7)
+    M = mf.Matrix(H)
+    inf = M.info()
+    n, k = H.n_rows, 16
+    X = torch.from_numpy(np.random.default_rng(7).normal(size=(k, n))).cuda()
+    Y = torch.zeros(k, n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    nd = C.c_int()
+    reps = 20
+
+    def f16():
+        for _ in range(reps):
+            st = L.mf_spmm_f16(M.h, k, X.data_ptr(), n, Y.data_ptr(), n, 0, C.byref(nd), stream.cuda_stream)
+            if st != 0:
+                mf.check(st)
+
+    def f64():
+        for _ in range(reps):
+            st = L.mf_spmm(M.h, k, X.data_ptr(), n, Y.data_ptr(), n, stream.cuda_stream)
+            if st != 0:
+                mf.check(st)
+
+    for _ in range(args.warmup):
+        f16()
+    torch.cuda.synchronize()
+    _barrier(world)
+    launches0 = L.mf_kernel_launches()
+    with ClockSampler(local) as clk:
+        ms = _timed(stream, f16, args.steps)
+    launches = L.mf_kernel_launches() - launches0
+    ms = _max_over_ranks(ms, world)
+    result = {"ms": ms, "value": reps * args.steps * world / (ms * 1e-3), "launches": launches,
+              "clocks": clk.summary(), "unit": "spmm/s",
+              "metric": "SpMM/s, 16 right-hand sides, dense tiles on tensor cores (mf_spmm_f16), 1 B200"}
+    if args.profile:
+        return result, None
+    y16 = Y.cpu().numpy().copy()
+    f64()
+    torch.cuda.synchronize()
+    ms64 = _max_over_ranks(_timed(stream, f64, max(3, args.steps // 2)), world)
+    y64 = Y.cpu().numpy()
+    dense_entries = 256 * nd.value
+    sparse_entries = H.nnz - dense_entries
+    npad = inf.tilen * 16
+    bytes_launch = 512 * nd.value + 5 * sparse_entries + 24 * inf.tilenum + 128 * n + 64 * npad + 128 * n
+    info = {"workload": "block-dense 32768 x (16x16 diagonal + 3 dense blocks) + 2 sparse per row, k = 16",
+            "n": n, "nnz": H.nnz, "tiles": inf.tilenum, "dense_tiles": nd.value,
+            "max_rel_diff_vs_fp64_spmm": float(np.max(np.abs(y16 - y64)) / np.max(np.abs(y64))),
+            "fp64_spmm": {"value": reps * max(3, args.steps // 2) * world / (ms64 * 1e-3), "unit": "spmm/s",
+                          "what": "mf_spmm of the same product (FP64, SIMT)"},
+            "tensor_tflops": 2 * 16 * 16 * 16 * nd.value / (ms / (reps * args.steps) * 1e-3) / 1e12,
+            "parallelism": f"replicas x{world}", "l2": "matrix larger than L2; no flush between SpMMs"}
+    # e2e: X from pinned host memory, one SpMM, Y back, every step
+    x_pin = X.cpu().pin_memory()
+    y_pin = torch.zeros_like(x_pin).pin_memory()
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        X.copy_(x_pin, non_blocking=True)
+        L.mf_spmm_f16(M.h, k, X.data_ptr(), n, Y.data_ptr(), n, 0, None, stream.cuda_stream)
+        y_pin.copy_(Y, non_blocking=True)
+        torch.cuda.synchronize()
+        e2e_s += time.perf_counter() - t0
+    e2e_s = _max_over_ranks(e2e_s, world)
+    result["e2e"] = {"value": args.steps * world / e2e_s, "unit": "spmm/s", "h2d_bytes_per_step": 8 * k * n,
+                     "d2h_bytes_per_step": 8 * k * n}
+    result["roofline_in"] = (bytes_launch, ms / (reps * args.steps), "k_spmm_tc", None)
+    result["dtype"] = "mixed(f16 dense tiles and x on tensor cores, f32 sparse tiles, f32 accumulate)"
+    result["cpu"] = None
+    M.close()
+    return result, info
+
+
 BATCH_NAME = ("batched random SPD x512 (n ~ log-uniform[1k,64k], seeds 100-611, 8-32 draws per row, "
               "row scale 10^U[-4,4]) CG to 1e-10")
 
@@ -888,6 +974,8 @@ def run_mf(args):
         res, info = workload_multi(args, mf, world, local)
     elif args.workload == "spmv":
         res, info = workload_spmv(args, mf, world, local)
+    elif args.workload == "spmm_f16":
+        res, info = workload_spmm_f16(args, mf, world, local)
     else:
         res, info = workload_single(args, mf, world, local)
     if args.profile:
@@ -954,7 +1042,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mf", "reference"], default="mf")
     ap.add_argument("--workload", default="batched",
-                    choices=["batched", "poisson3d", "lap2d", "convdiff", "aniso", "multirhs", "spmv"])
+                    choices=["batched", "poisson3d", "lap2d", "convdiff", "aniso", "multirhs", "spmv", "spmm_f16"])
     ap.add_argument("--rhs", type=int, default=16, help="multirhs workload: right-hand sides (1-16)")
     ap.add_argument("--policy", default=None, choices=["fp64", "static", "rule", "learned", "static_fp16"],
                     help="precision policy (default: learned for batched, static otherwise)")

@@ -270,6 +270,20 @@ mf_status mf_bicgstab_solve_host(mf_matrix m, const double *b_host, double *x_ho
  * MF_ERR_INVALID_ARG. */
 mf_status mf_spmm(mf_matrix m, int k, const double *X, int ldx, double *Y, int ldy, void *stream);
 
+/* Y = A X as mf_spmm, with the dense tiles on the tensor cores: every tile
+ * with at least dense_fill entries (<= 0: 64; at most 256) whose FP16
+ * payload is finite is kept as a dense FP16 block (built on the first call
+ * and kept on the handle) and multiplied by warp-level MMA (m16n8k16, FP16
+ * inputs, FP32 accumulation); the other tiles use their FP32 values.  X is
+ * scaled per column by a power of two and rounded to FP16; Y is written in
+ * FP64.  Accuracy: FP16 rounding of the dense tiles and of X (2^-11
+ * relative each) with FP32 sums -- the form for mixed-precision multi-RHS
+ * work, not a replacement for the exact mf_spmm.  dense_tiles (may be NULL)
+ * receives the number of dense tiles.  No reference counterpart (it runs
+ * one SpMV per vector). */
+mf_status mf_spmm_f16(mf_matrix m, int k, const double *X, int ldx, double *Y, int ldy, int dense_fill,
+                      int *dense_tiles, void *stream);
+
 /* Solves A X = B for k right-hand sides (1 <= k <= 16) with k independent
  * FP64 CG recurrences that share every SpMM (the matrix is read once per
  * iteration for all columns).  B and X are device arrays, column-major,

@@ -111,6 +111,7 @@ def lib() -> C.CDLL:
         L.mf_cg_solve_multi_host.argtypes = [vp, C.c_int, vp, vp, C.POINTER(SolveOpts), C.POINTER(SolveReport)]
         L.mf_read_matrix_market.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
         L.mf_matrix_create_mtx.argtypes = [C.c_char_p, vp, C.POINTER(vp), ip]
+        L.mf_spmm_f16.argtypes = [vp, C.c_int, vp, C.c_int, vp, C.c_int, C.c_int, ip, vp]
         L.mf_read_matrix.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
         L.mf_read_cbd.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp)]
         L.mf_write_cbd.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, vp]
@@ -223,6 +224,37 @@ def synth_random_spd(seed, n=0):
 
 def synth_aniso3d(g, seed, log_sigma=2.0, corr_len=8.0, aniso=100.0):
     return _gen(lib().mf_synth_aniso3d, g, seed, log_sigma, corr_len, aniso)
+
+
+def synth_block_dense(nb, dense_per_row, sparse_per_row, seed, ragged=0):
+    """A block-structured matrix (HostCsr) for the tensor-core SpMM: nb block
+    rows of 16 (the last one `ragged` rows short); per block row a dense
+    diagonal 16x16 block and `dense_per_row` dense blocks at random block
+    columns (values N(0,1) x 10^U[-2,2] per block), plus `sparse_per_row`
+    random N(0,1) entries per row; duplicates summed, columns sorted (NumPy
+    PCG64 seeded with `seed`)."""
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(seed)
+    n = 16 * nb - ragged
+    rows, cols, vals = [], [], []
+    base = np.arange(16)
+    for b in range(nb):
+        for bc in sorted({b} | set(rng.integers(0, nb, dense_per_row).tolist())):
+            rows.append(np.repeat(base + 16 * b, 16))
+            cols.append(np.tile(base + 16 * bc, 16))
+            vals.append(rng.normal(size=256) * 10.0 ** rng.uniform(-2, 2))
+    r = rng.integers(0, 16 * nb, 16 * nb * sparse_per_row)
+    c = rng.integers(0, 16 * nb, 16 * nb * sparse_per_row)
+    rows.append(r)
+    cols.append(c)
+    vals.append(rng.normal(size=r.size))
+    rows, cols, vals = np.concatenate(rows), np.concatenate(cols), np.concatenate(vals)
+    keep = (rows < n) & (cols < n)
+    A = sp.coo_matrix((vals[keep], (rows[keep], cols[keep])), shape=(n, n)).tocsr()
+    A.sum_duplicates()
+    A.sort_indices()
+    return HostCsr(n, n, A.indptr, A.indices, A.data)
 
 
 def synth_xstar(seed, n):

@@ -173,7 +173,7 @@ mf_status mf_matrix_destroy(mf_matrix m)
                     m->d_rbb_colstart, m->d_rbb_colstop, m->d_part, m->d_cta_chunk, m->d_chunks, m->work, m->host_io,
                     m->d_wcls, m->d_poff, m->d_pay, m->d_resid, m->d_pol, m->d_sslot, m->d_smeta, m->d_sval,
                     m->d_shdr, m->d_spay, m->d_scta_chunk, m->d_schunks, m->d_spos, m->d_sdesc, m->mr_work,
-                    m->mr_io};
+                    m->mr_io, m->d_tc_index, m->d_tc_dense};
     for (void *p : bufs)
         if (p) cudaFree(p);
     delete m;

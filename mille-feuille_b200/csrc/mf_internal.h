@@ -102,6 +102,12 @@ struct mf_matrix_s {
     size_t mr_work_bytes = 0;
     void *mr_io = nullptr;
     size_t mr_io_bytes = 0;
+    // tensor-core SpMM (spmm_tc.cu): dense FP16 copies of the tiles with at
+    // least tc_fill entries, and each tile's index among them (-1: sparse)
+    int tc_fill = 0;
+    int tc_ndense = 0;
+    int *d_tc_index = nullptr;
+    void *d_tc_dense = nullptr;
 };
 
 namespace mf {

@@ -78,6 +78,10 @@ def test_noalloc_residual_argument_checks_without_device(mf):
     assert list(buf) == [0.0, 0.0, 0.0]
 
 
+def test_tensor_core_spmm_rejects_null_without_device(mf):
+    assert mf.lib().mf_spmm_f16(None, 4, None, 8, None, 8, 0, None, None) == 1
+
+
 def test_device_mtx_reader_rejects_before_device(mf, tmp_path):
     """mf_matrix_create_mtx: a null path or handle pointer, a missing file
     and a malformed one are reported before any device work."""

@@ -21,6 +21,8 @@
 // tcgen05 with TMEM accumulators would idle most of each instruction here.
 #include <cuda_fp16.h>
 
+#include <algorithm>
+
 #include "mf_internal.h"
 #include "spmv_core.cuh"
 
@@ -81,9 +83,12 @@ __global__ void __launch_bounds__(TC_NT) k_tc_fill(MfTiles A, int T, const int *
 
 // Per column j < k: the largest |X[:, j]| (float bits; atomicMax on
 // non-negative floats orders like the values).  Each thread keeps the
-// maxima of its rows, a warp combines them, one atomic per warp and column.
-__global__ void k_tc_colmax(int n, int k, const double *__restrict__ X, int ldx, unsigned *__restrict__ mx)
+// maxima of its rows, the block combines them (warp shuffles, then shared
+// memory), one atomic per block and column.
+__global__ void __launch_bounds__(256) k_tc_colmax(int n, int k, const double *__restrict__ X, int ldx,
+                                                   unsigned *__restrict__ mx)
 {
+    __shared__ float s_m[8][16];
     float m[16];
 #pragma unroll
     for (int j = 0; j < 16; j++) m[j] = 0.f;
@@ -91,11 +96,18 @@ __global__ void k_tc_colmax(int n, int k, const double *__restrict__ X, int ldx,
 #pragma unroll
         for (int j = 0; j < 16; j++)
             if (j < k) m[j] = fmaxf(m[j], (float)fabs(X[(size_t)j * ldx + r]));
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
     for (int j = 0; j < 16; j++) {
         float v = m[j];
         for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if ((threadIdx.x & 31) == 0 && j < k) atomicMax(&mx[j], __float_as_uint(v));
+        if (lane == 0) s_m[w][j] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 16 && (int)threadIdx.x < k) {
+        float v = 0.f;
+        for (int ww = 0; ww < 8; ww++) v = fmaxf(v, s_m[ww][threadIdx.x]);
+        atomicMax(&mx[threadIdx.x], __float_as_uint(v));
     }
 }
 
@@ -166,9 +178,17 @@ __global__ void __launch_bounds__(TC_NT) k_spmm_tc(MfTiles A, const int *__restr
         const int rowlen = (bi == A.tilem - 1) ? A.rows - bi * MF_TILE : MF_TILE;
         float d0[4] = {0.f, 0.f, 0.f, 0.f}, d1[4] = {0.f, 0.f, 0.f, 0.f};
         const int t0 = A.tile_ptr[bi], t1 = A.tile_ptr[bi + 1];
+        // the next tile's metadata (dense index, column, entry offsets) is
+        // loaded before the current tile is computed
+        int di = t0 < t1 ? index[t0] : -1, xo = t0 < t1 ? A.tile_columnidx[t0] * MF_TILE : 0;
+        int off = A.tile_nnz[t0], nxt = t0 < t1 ? A.tile_nnz[t0 + 1] : off;
         for (int t = t0; t < t1; t++) {  // uniform over the warp
-            const int di = index[t];
-            const int xo = A.tile_columnidx[t] * MF_TILE;
+            int di2 = -1, xo2 = 0, nxt2 = nxt;
+            if (t + 1 < t1) {
+                di2 = index[t + 1];
+                xo2 = A.tile_columnidx[t + 1] * MF_TILE;
+                nxt2 = A.tile_nnz[t + 2];
+            }
             const __half *xb = x16 + (size_t)xo * 16;
             if (di >= 0) {
                 const __half *a = dense + (size_t)di * 256;
@@ -188,7 +208,7 @@ __global__ void __launch_bounds__(TC_NT) k_spmm_tc(MfTiles A, const int *__restr
                 }
             } else {
                 // sparse tile: rows gid and gid + 8, this thread's columns
-                const int off = A.tile_nnz[t], nz = A.tile_nnz[t + 1] - off;
+                const int nz = nxt - off;
                 for (int h = 0; h < 2; h++) {
                     const int r = gid + 8 * h;
                     if (r >= rowlen) continue;
@@ -206,6 +226,10 @@ __global__ void __launch_bounds__(TC_NT) k_spmm_tc(MfTiles A, const int *__restr
                     }
                 }
             }
+            di = di2;
+            xo = xo2;
+            off = nxt;
+            nxt = nxt2;
         }
         for (int h = 0; h < 2; h++) {
             const int r = gid + 8 * h;
@@ -284,7 +308,8 @@ extern "C" mf_status mf_spmm_f16(mf_matrix m, int k, const double *X, int ldx, d
     float *scale = (float *)(mx + 16), *inv = scale + 16;
     MF_CUDA(cudaMemsetAsync(mx, 0, sizeof(unsigned) * 16, s));
     if (m->v.cols > 0) {
-        k_tc_colmax<<<tc_grid(m->v.cols, 256), 256, 0, s>>>(m->v.cols, k, X, ldx, mx);
+        // a resident wave of blocks, each striding over the rows
+        k_tc_colmax<<<std::min(tc_grid(m->v.cols, 256), 148 * 4), 256, 0, s>>>(m->v.cols, k, X, ldx, mx);
         note_launch();
     }
     k_tc_scale<<<1, 32, 0, s>>>(k, mx, scale, inv);

@@ -40,8 +40,11 @@ Workloads (--workload):
                  per host core at once, scaled by the FP64 oracle's
                  iteration counts of all 512 systems)
 
-N > 1 runs independent replicas, one per GPU (a single system does not
-shard), timed with CUDA events and reported as the max over ranks.
+N > 1: the batched workload is sharded -- rank r solves its own 512
+systems (seeds 100 + 512 r ...), no collective on the data path -- and the
+single-system workloads run independent replicas (a single system does not
+shard); timed with CUDA events and reported as the max over ranks, value =
+the systems of all ranks / that time (weak scaling).
 """
 from __future__ import annotations
 
@@ -707,16 +710,26 @@ BATCH_NAME = ("batched random SPD x512 (n ~ log-uniform[1k,64k], seeds 100-611, 
               "row scale 10^U[-4,4]) CG to 1e-10")
 
 
+def batch_seeds(rank, count):
+    """The seeds of rank `rank`'s shard of the batched workload: rank 0 has
+    the benchmark's 100 .. 100 + count - 1, rank r the next `count` after
+    rank r - 1's (disjoint shards of one larger batch)."""
+    return [100 + rank * count + k for k in range(count)]
+
+
 def workload_batched(args, mf, world, local):
-    """512 random SPD systems in one graph-captured batched launch."""
+    """512 random SPD systems per GPU in one graph-captured batched launch
+    (rank r: its own shard of systems, batch_seeds)."""
     import torch
     from concurrent.futures import ThreadPoolExecutor
 
     L = mf.lib()
     N = args.systems
+    rank = int(os.environ.get("RANK", "0"))
+    seeds = batch_seeds(rank, N)
     with ThreadPoolExecutor(16) as ex:
-        systems = list(ex.map(lambda k: mf.synth_random_spd(100 + k), range(N)))
-        xs = list(ex.map(lambda k: mf.synth_xstar(100 + k, systems[k].n_rows), range(N)))
+        systems = list(ex.map(lambda k: mf.synth_random_spd(seeds[k]), range(N)))
+        xs = list(ex.map(lambda k: mf.synth_xstar(seeds[k], systems[k].n_rows), range(N)))
     bs = [A.matvec(x) for A, x in zip(systems, xs)]
     t0 = time.perf_counter()
     B = mf.Batch(systems)
@@ -786,8 +799,8 @@ def workload_batched(args, mf, world, local):
             "fp16_share": float(rep.fp16_share), "max_abs_err_vs_xstar": err_xs,
             "max_abs_err_vs_fp64_oracle_4_smallest": err_or, "setup_ms": setup_ms,
             "lanes_per_row": int(rep.lanes_per_row), "cluster_ctas": int(rep.cluster_ctas),
-            "parallelism": f"replicas x{world}", "l2": L2_NOTE}
-    if fixture is not None and N == len(fixture):
+            "parallelism": f"sharded x{world} (disjoint systems per GPU)", "l2": L2_NOTE}
+    if fixture is not None and N == len(fixture) and rank == 0:
         it_o = np.array([s["iterations"] for s in fixture])
         info["iterations_vs_fp64_oracle"] = float(its.sum() / it_o.sum())
         info["oracle_max_abs_err_vs_xstar"] = max(s["max_abs_err_vs_xstar"] for s in fixture)

@@ -51,3 +51,11 @@ def test_batched_reference_baseline_runs_on_host():
     assert t > 0 and len(cpu.systems) == 512 and cpu.cores == 2
     assert all(nnz > 0 and s > 0 for _, _, nnz, s in cpu.last)
     assert "512 systems" in cpu.describe() or "of the 512" in cpu.describe()
+
+
+def test_batch_shards_are_disjoint_and_rank0_is_the_benchmark():
+    n = 512
+    shards = [bench.batch_seeds(r, n) for r in range(8)]
+    assert shards[0] == list(range(100, 612))
+    flat = [s for sh in shards for s in sh]
+    assert len(set(flat)) == len(flat) == 8 * n

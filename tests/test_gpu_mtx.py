@@ -33,6 +33,8 @@ def random_entries(rng, m, n, count, fmt, lower):
             out.append(f"{a} {b} {rng.normal() * 10.0 ** rng.integers(-6, 6):.17g}")
         elif fmt == "integer":
             out.append(f"{a} {b} {int(rng.integers(-100, 100))}")
+        elif fmt == "complex":
+            out.append(f"{a} {b} {rng.normal():.17g} {rng.normal():.6g}")
         else:
             out.append(f"{a} {b}")
     return out
@@ -61,6 +63,7 @@ def same_matrix(mf, path):
     ("real", "symmetric", 2500, 2500, 30000),
     ("pattern", "symmetric", 1000, 1000, 8000),
     ("integer", "general", 777, 777, 9000),
+    ("complex", "hermitian", 900, 900, 7000),  # real parts
     ("real", "general", 1200, 900, 15000),   # rectangular
 ])
 def test_device_csr_equals_host_csr(mf, tmp_path, fmt, sym, m, n, count):

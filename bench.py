@@ -286,6 +286,50 @@ class CpuBatchReference:
                 f"iteration counts) / {self.cores} cores; reference Tile_create not timed")
 
 
+def run_reference_spmv(args):
+    """The reference arm of --workload spmv: the reference's own
+    blockspmv_cpu (serial, as the reference runs it, its schedule arrays
+    allocated per call) on the same matrix and x, timed per call."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as ol  # reference arm: the reference's own CPU code
+
+    ref = ol.reference()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU code not built (oracle/_ref)"}))
+        return 0
+    import __graft_entry__ as ge
+
+    mf = ge.load_package()
+    A = mf.synth_poisson3d_scaled(GRID, SEED)
+    csr = ol.Csr(A.n_rows, A.n_cols, A.rowptr, A.colidx, A.val)
+    sizes, _ = ol.reference_tiles(csr)
+    ref.ref_encode_last()
+    nx = sizes["tilen"] * 16
+    x = np.ascontiguousarray(mf.synth_xstar(SEED, nx))
+    y = np.zeros(nx)
+    p1 = np.zeros(sizes["tilenum"] + 1, np.int32)
+    p2 = np.zeros(sizes["tilenum"] + 1, np.int32)
+    vals = []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        ref.ref_blockspmv(A.n_rows, A.n_cols, A.nnz, x, y, p1, p2, None, None, None)
+        t = time.perf_counter() - t0
+        if s >= args.warmup:
+            vals.append(1.0 / t)
+    v = statistics.median(vals)
+    line = {"impl": "reference",
+            "metric": "FP64 tiled SpMV/s (mf_spmv, bit-identical to the reference's blockspmv_cpu), 1 B200",
+            "value": v, "unit": "spmv/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"poisson3d_scaled_{GRID}^3 mf_spmv", "n": A.n_rows, "nnz": A.nnz},
+            "cpu_baseline": {"value": v, "unit": "spmv/s", "cores": 1, "kind": "reference",
+                             "sample": "one reference blockspmv_cpu call per step (serial), schedule included"},
+            "e2e": {"value": v, "unit": "spmv/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -319,6 +363,12 @@ def run_reference(args):
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
         print(json.dumps(line))
+        return 0
+    if args.workload == "spmv":
+        return run_reference_spmv(args)
+    if args.workload not in ("poisson3d",):
+        print(json.dumps({"impl": "reference", "unavailable": f"no reference arm for --workload {args.workload} "
+                                                              "(the reference arm measures batched, poisson3d, spmv)"}))
         return 0
     import __graft_entry__ as ge
 

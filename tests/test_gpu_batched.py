@@ -236,3 +236,38 @@ def test_batched_rejects_bad_input(mf):
     A.colidx[3] = 10**6
     with pytest.raises(mf.MfError):
         mf.Batch([A])
+
+
+def test_batched_edge_systems(mf):
+    """Systems the benchmark batch never holds: one of 100,000 rows (four
+    column panels: the panel-ordered row sums), a 1x1 and a 5-row system, a
+    system whose right-hand side is zero (0 iterations, x = 0), next to a
+    Laplacian; every policy against the FP64 oracle."""
+    big = mf.synth_random_spd(4242, 100000)
+    one = mf.HostCsr(1, 1, np.array([0, 1], np.int32), np.array([0], np.int32), np.array([4.0]))
+    five = mf.synth_random_spd(77, 5)
+    zero = mf.synth_random_spd(78, 900)
+    lap = mf.synth_laplace2d(30, 30)
+    systems = [big, one, five, zero, lap]
+    xs, bs = _rhs(mf, systems, [4242, 1, 77, 78, 5])
+    bs[3] = np.zeros(zero.n_rows)
+    B = mf.Batch(systems)
+    db = torch.from_numpy(B.stack(bs)).cuda()
+    oracle = {}
+    for k in (0, 1, 2, 4):
+        Ac = _csr(systems[k])
+        it_o, x_o, _ = ol.oracle_cg(Ac, bs[k], 50000, 1e-10)
+        oracle[k] = (Ac, it_o, x_o, np.max(np.abs(x_o - xs[k])))
+    for pol in ("fp64", "static", "rule"):
+        dx = torch.full_like(db, 7.0)  # overwritten: the solve starts from x = 0
+        st, rep = B.solve_device(db.data_ptr(), dx.data_ptr(), use_graph=0, tol=1e-10, maxiter=50000, policy=pol)
+        assert st == 0 and rep.failed == 0, (pol, rep.as_dict())
+        its, rr = B.results()
+        x = B.split(dx.cpu().numpy())
+        assert its[3] == 0 and np.all(x[3] == 0.0)
+        for k, (Ac, it_o, x_o, err_o) in oracle.items():
+            assert ol.oracle_true_relres(Ac, bs[k], x[k]) <= 1.2e-10, (pol, k)
+            assert np.max(np.abs(x[k] - x_o)) <= 100 * err_o + 1e-9, (pol, k)
+            if pol == "fp64":
+                assert abs(int(its[k]) - it_o) <= max(3, it_o // 50), (k, its[k], it_o)
+    B.close()
